@@ -1,0 +1,185 @@
+/*
+ * plegma2pt — C ABI of the B200 hadron two-point contraction + momentum
+ * projection library.
+ *
+ * One call replaces the reference's contraction path
+ *   PLEGMA_Correlator<Float>::contract{Baryons,MesonsAll,MesonsNew,Mesons}
+ *     -> contract_{baryons,mesons_all,mesons_new,mesons}        (lib/kernels)
+ *     -> fourier_transform_3D inside the kernel, host block sum,
+ *        MPI_Allreduce over the spatial communicator
+ * and the generic projection PLEGMA_FT<Float>::apply.  Plain pointers and
+ * sizes only; every entry point returns a p2_status and never exits.
+ *
+ * Data formats
+ *  - Propagator (PLEGMA_Propagator storage, lib/PLEGMA_Propagator.cu:33-49,
+ *    lib/kernels/PLEGMA_kernel_getSet.cuh:791-851): structure of arrays,
+ *    component i = ((mu*4 + nu)*3 + c1)*3 + c2 (144 components) major, the
+ *    site index x + Lx*(y + Ly*(z + Lz*j)) fastest, each element a complex
+ *    (re, im) pair of double (P2_FP64) or float (P2_FP32).  j counts the
+ *    stored time slices: slice j holds global time (t_first + j) mod Lt.
+ *  - Momenta: integer triples n, p = 2*pi*n/L; the list of
+ *    PLEGMA_FT::createMom (lib/PLEGMA_FT.cu:50-72) when built from Q^2_max.
+ *  - Result of a request: for every contraction block in bit order below,
+ *    [group][dataset][tau][mom][component] complex double, tau = 0..totalT-1
+ *    the time measured from the source (the order in which the reference's
+ *    HDF5 writer stores it, lib/PLEGMA_Correlator.cu:810-950).
+ *    p2_block_info() gives each block's shape and offset.
+ */
+#ifndef PLEGMA2PT_H
+#define PLEGMA2PT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define P2_ABI_VERSION 1
+
+typedef enum {
+  P2_OK = 0,
+  P2_ERR_INVALID_ARG = 1,
+  P2_ERR_OOM = 2,
+  P2_ERR_CUDA = 3,
+  P2_ERR_DEVICE_TIMEOUT = 4,
+  P2_ERR_UNSUPPORTED = 5
+} p2_status;
+
+typedef enum { P2_FP64 = 0, P2_FP32 = 1 } p2_precision;
+
+/* Arithmetic of a request.
+ * P2_PLAIN_FP64: FP64 site contraction, FP64 direct phase sum.
+ * P2_SPLIT_FP16: FP32 site contraction with power-of-two scaling per time
+ *   slice; projection on the tensor cores as hi+lo FP16 products with FP32
+ *   accumulation; FP64 cross-block sums and normalisation. */
+typedef enum { P2_PLAIN_FP64 = 0, P2_SPLIT_FP16 = 1 } p2_mode;
+
+typedef enum { P2_DEVICE = 0, P2_HOST = 1 } p2_location;
+
+/* Contraction blocks (bit order = order in the result).
+ *   groups x datasets x components per site                     reference
+ *   NUCLEON_CG5   1 x 2 x 16  nucl_nucl: proton (u,u,d), neutron   PLEGMA_baryons_NtoN.cu:6-46
+ *                 16 = (mu, mu') open spin, mu*4 + mu'
+ *   DELTA_ISO12   3 x 2 x 16  deltap_deltaz_kk, k = 1..3          PLEGMA_baryons_deltas.cu:7-59
+ *   DELTA_ISO32   3 x 2 x 16  deltapp_deltamm_kk, k = 1..3        PLEGMA_baryons_deltas.cu:62-110
+ *   MESON_G16     1 x 1 x 256 all (G_sink, G_src) pairs of the 16 PLEGMA_mesonsAll.cuh:52-76
+ *                 structures, component g_sink*16 + g_src, G_sink u G_src d^dagger
+ *   MESON_ALL34   1 x 1 x 34  contractMesonsAll subset              PLEGMA_mesonsAll.cuh:8-95
+ *   MESON_NEW10   1 x 1 x 10  contractMesonsNew (u . d^dagger)      PLEGMA_mesonsNew.cuh:5-56
+ *   MESON_DIAG10  1 x 2 x 10  contractMesons (u u^dag, d d^dag)     PLEGMA_mesons.cuh:10-65
+ */
+enum {
+  P2_NUCLEON_CG5 = 1u << 0,
+  P2_DELTA_ISO12 = 1u << 1,
+  P2_DELTA_ISO32 = 1u << 2,
+  P2_MESON_G16 = 1u << 3,
+  P2_MESON_ALL34 = 1u << 4,
+  P2_MESON_NEW10 = 1u << 5,
+  P2_MESON_DIAG10 = 1u << 6
+};
+
+typedef struct p2_ctx p2_ctx;
+
+/* Lattice and process geometry; replaces PLEGMA_init's globals
+ * (lib/PLEGMA.cu:19-212, include/global/PLEGMA_global_constants.h:64-110).
+ * L is the global extent; procs/coords the process grid and this rank's
+ * position in it (all 1 / 0 for one GPU).  device < 0 creates a host-only
+ * context: argument checks, shapes and the host generator work, every
+ * device entry point returns P2_ERR_UNSUPPORTED. */
+typedef struct {
+  int L[4];
+  int procs[4];
+  int coords[4];
+  int device;
+} p2_geom;
+
+/* Non-owning view of one propagator (PLEGMA_Propagator<Float>::D_elem()/H_elem()). */
+typedef struct {
+  const void* data;
+  int precision; /* p2_precision */
+  int location;  /* p2_location; host views are streamed through the device */
+  int t_first;   /* global time of stored slice 0 */
+  int nt;        /* stored slices (the local time extent for a full field) */
+} p2_prop;
+
+/* One two-point request: one source, one time window, one contraction set. */
+typedef struct {
+  int source[4];       /* x, y, z, t (PLEGMA's `site`) */
+  int totalT;          /* window from the source (PLEGMA_Correlator totalT) */
+  const int* moms;     /* int[nmom][3]; NULL: build from q2max */
+  int nmom;
+  int q2max;
+  unsigned contractions;
+  int mode;            /* p2_mode */
+  int prop_u, prop_d;  /* indices into the props array of the call */
+  double* out;         /* result, layout in the file header */
+  int out_location;    /* p2_location */
+} p2_request;
+
+/* Shape of one block of a request's result. */
+typedef struct {
+  unsigned bit;
+  int groups, datasets, comps;
+  size_t offset; /* in complex elements from the start of the result */
+} p2_block;
+
+/* ---- context ---------------------------------------------------------- */
+/* Replaces PLEGMA_init's geometry setup for this path; the context owns the
+ * stream-ordered workspaces, momentum tables and tuned launch shapes. */
+p2_status p2_ctx_create(const p2_geom* geom, p2_ctx** ctx);
+p2_status p2_ctx_destroy(p2_ctx* ctx);
+/* Text of the last error on this context (never NULL). */
+const char* p2_last_error(const p2_ctx* ctx);
+/* Block until all work issued on the context's stream is done. */
+p2_status p2_sync(p2_ctx* ctx);
+/* Work is issued on `stream` (a cudaStream_t; NULL = the context's own). */
+p2_status p2_set_stream(p2_ctx* ctx, void* stream);
+
+/* ---- shapes ----------------------------------------------------------- */
+/* Components per site of a contraction set (sum over blocks of groups*datasets*comps). */
+int p2_components(unsigned contractions);
+/* Number of momenta with |n|^2 <= q2max; fills moms[n][3] in createMom order
+ * when moms is not NULL (PLEGMA_FT::createMom, lib/PLEGMA_FT.cu:50-72). */
+int p2_mom_list(int q2max, int* moms);
+/* Block layout of a result: writes up to max_blocks entries, returns count;
+ * *total gets the result size in complex elements for (totalT, nmom). */
+int p2_block_info(unsigned contractions, int totalT, int nmom, p2_block* blocks, int max_blocks, size_t* total);
+
+/* ---- the hot path ------------------------------------------------------ */
+/* Contraction + projection of nreq requests over the given propagators.
+ * Replaces contract_baryons / contract_mesons_all / contract_mesons_new /
+ * contract_mesons (lib/kernels/PLEGMA_baryons.cuh:169-206,
+ * PLEGMA_mesonsAll.cuh:161-192, PLEGMA_mesonsNew.cuh:140-157,
+ * PLEGMA_mesons.cuh:134-165) including their host block sums and spatial
+ * all-reduce (one GPU holds the full spatial volume).  Asynchronous on the
+ * context's stream when all outputs are on the device; synchronous when a
+ * result or a propagator lives on the host. */
+p2_status p2_contract_project(p2_ctx* ctx, const p2_prop* props, int nprops, const p2_request* reqs, int nreq);
+
+/* Position-space contraction (the reference's POSITION_SPACE correlator):
+ * out[tau][k][x3] complex double, k over p2_components(contractions),
+ * x3 the spatial site index; the request's moms/mode are ignored (FP64). */
+p2_status p2_contract_position(p2_ctx* ctx, const p2_prop* props, int nprops, const p2_request* req);
+
+/* Generic momentum projection of a field, PLEGMA_FT<Float>::apply with
+ * FT_NAIVE/FT_GEMV (lib/PLEGMA_FT.cu:122-162): field SoA [dof][V3*nt]
+ * complex double on the device, out [nt][dof][nmom] complex double
+ * (host or device per out_location), phase exp(sign * i p.x) with the
+ * origin at x = 0. */
+p2_status p2_ft_apply(p2_ctx* ctx, const double* field, int dof, int nt, const int* moms, int nmom, int sign,
+                      double* out, int out_location);
+
+/* ---- synthetic inputs (benchmarks and tests) --------------------------- */
+/* Fill a propagator with entries Re, Im ~ N(0,1) scaled by exp(-a*|t - t0|),
+ * drawn from a counter-based SplitMix64 + Box-Muller stream keyed by
+ * (seed, flavour, global site, component).  `dst` is a device pointer
+ * (on_device = 1, fast, device libm) or a host pointer (on_device = 0,
+ * host libm, OpenMP).  Layout as p2_prop with the given t_first/nt. */
+p2_status p2_synth_propagator(p2_ctx* ctx, void* dst, int on_device, int precision, uint64_t seed, int flavour,
+                              int t0, double decay, int t_first, int nt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PLEGMA2PT_H */

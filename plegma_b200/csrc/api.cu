@@ -1,0 +1,558 @@
+// C ABI (include/plegma2pt.h): argument checks, workspaces, phase tables and
+// the launch sequence of the hot path.  Every failure is returned as a
+// p2_status with a message in the context; nothing here exits.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/plegma2pt.h"
+#include "kernels.cuh"
+#include "ctx.h"
+#include "synth_host.h"
+
+using namespace p2host;
+
+namespace p2host {
+
+int components_of(unsigned what) {
+  int k = 0;
+  for (const auto& b : kBlocks)
+    if (what & b.bit) k += b.groups * b.datasets * b.comps;
+  return k;
+}
+
+p2::CompOffsets offsets_of(unsigned what) {
+  p2::CompOffsets o{-1, -1, -1, -1, -1, -1, -1};
+  int k = 0;
+  int* slot[] = {&o.nuc, &o.diso12, &o.diso32, &o.g16, &o.all34, &o.new10, &o.diag10};
+  for (int i = 0; i < 7; i++)
+    if (what & kBlocks[i].bit) {
+      *slot[i] = k;
+      k += kBlocks[i].groups * kBlocks[i].datasets * kBlocks[i].comps;
+    }
+  return o;
+}
+
+std::vector<int> createMom(int q2max) {
+  std::vector<int> m;
+  for (int iq = 0; iq <= q2max; iq++)
+    for (int nx = iq; nx >= -iq; nx--)
+      for (int ny = iq; ny >= -iq; ny--)
+        for (int nz = iq; nz >= -iq; nz--)
+          if (nx * nx + ny * ny + nz * nz == iq) {
+            m.push_back(nx);
+            m.push_back(ny);
+            m.push_back(nz);
+          }
+  return m;
+}
+
+// Per-dimension phase tables [3][nmom][Lmax] complex double:
+// exp(sign * i * 2 pi * n_d * (x_d - src_d) / L_d) for the local coordinates x_d.
+std::vector<double> phase_tables(const p2_ctx* c, const int* moms, int nmom, const int* src, int sign, int Lmax) {
+  std::vector<double> t((size_t)3 * nmom * Lmax * 2, 0.0);
+  for (int d = 0; d < 3; d++)
+    for (int p = 0; p < nmom; p++)
+      for (int xl = 0; xl < c->Ll[d]; xl++) {
+        const long long xg = (long long)xl + (long long)c->g.coords[d] * c->Ll[d];
+        // reduce n*(x - x0) mod L exactly in integers before the division
+        long long num = ((long long)moms[3 * p + d] * (xg - src[d])) % c->g.L[d];
+        if (num < 0) num += c->g.L[d];
+        const double ph = 2.0 * M_PI * (double)num / (double)c->g.L[d];
+        const size_t i = ((size_t)(d * nmom + p) * Lmax + xl) * 2;
+        t[i] = std::cos(ph);
+        t[i + 1] = sign * std::sin(ph);
+      }
+  return t;
+}
+
+std::vector<TauRun> local_runs(const p2_ctx* c, const p2_prop& u, const p2_prop& d, const int* src, int totalT) {
+  std::vector<TauRun> runs;
+  const int T = c->T;
+  const int tl0 = c->g.coords[3] * c->Ll[3];
+  int prev_ju = -2, prev_jd = -2;
+  for (int tau = 0; tau < totalT; tau++) {
+    const int t = (src[3] + tau) % T;
+    if (t < tl0 || t >= tl0 + c->Ll[3]) {
+      prev_ju = prev_jd = -2;
+      continue;
+    }
+    const int ju = ((t - u.t_first) % T + T) % T, jd = ((t - d.t_first) % T + T) % T;
+    if (ju >= u.nt || jd >= d.nt) {
+      prev_ju = prev_jd = -2;
+      continue;
+    }
+    if (!runs.empty() && ju == prev_ju + 1 && jd == prev_jd + 1 && runs.back().tau0 + runs.back().n == tau)
+      runs.back().n++;
+    else
+      runs.push_back({tau, 1});
+    prev_ju = ju;
+    prev_jd = jd;
+  }
+  return runs;
+}
+
+p2_status check_prop(p2_ctx* c, const p2_prop& p, const char* name) {
+  if (!p.data) return c->fail(P2_ERR_INVALID_ARG, std::string(name) + ": null data");
+  if (p.nt < 1 || p.nt > c->T) return c->fail(P2_ERR_INVALID_ARG, std::string(name) + ": nt out of range");
+  if (p.t_first < 0 || p.t_first >= c->T)
+    return c->fail(P2_ERR_INVALID_ARG, std::string(name) + ": t_first out of range");
+  if (p.precision != P2_FP64 && p.precision != P2_FP32)
+    return c->fail(P2_ERR_INVALID_ARG, std::string(name) + ": bad precision");
+  if (p.location != P2_DEVICE && p.location != P2_HOST)
+    return c->fail(P2_ERR_INVALID_ARG, std::string(name) + ": bad location");
+  return P2_OK;
+}
+
+// Device views for one chunk of time slices: device propagators are used in
+// place; host propagators are copied slice-range by slice-range into the
+// context's staging buffers (2-D copies over the 144 component rows).
+p2_status chunk_view(p2_ctx* c, const p2_prop& p, DevBuf& stage, int t_begin, int n, p2::ContractArgs& a, bool is_u) {
+  const size_t esz = p.precision == P2_FP64 ? 16 : 8;
+  const int T = c->T;
+  if (p.location == P2_DEVICE) {
+    if (is_u) {
+      a.u = p.data;
+      a.vol_u = c->V3 * p.nt;
+      a.t_first_u = p.t_first;
+    } else {
+      a.d = p.data;
+      a.vol_d = c->V3 * p.nt;
+      a.t_first_d = p.t_first;
+    }
+    return P2_OK;
+  }
+  const int j0 = ((t_begin - p.t_first) % T + T) % T;
+  P2_TRY(c, stage.ensure((size_t)144 * n * c->V3 * esz), "staging alloc");
+  const size_t width = (size_t)n * c->V3 * esz;
+  P2_TRY(c,
+         cudaMemcpy2DAsync(stage.p, width, (const char*)p.data + (size_t)j0 * c->V3 * esz,
+                           (size_t)p.nt * c->V3 * esz, width, 144, cudaMemcpyHostToDevice, c->stream),
+         "host propagator upload");
+  if (is_u) {
+    a.u = stage.p;
+    a.vol_u = c->V3 * n;
+    a.t_first_u = t_begin;
+  } else {
+    a.d = stage.p;
+    a.vol_d = c->V3 * n;
+    a.t_first_d = t_begin;
+  }
+  return P2_OK;
+}
+
+p2_status make_plan(p2_ctx* c, const p2_request& r, Plan& pl) {
+  if (r.contractions == 0 || (r.contractions & ~kAllBits))
+    return c->fail(P2_ERR_INVALID_ARG, "contractions: empty or unknown bits");
+  if (r.totalT < 1 || r.totalT > c->T) return c->fail(P2_ERR_INVALID_ARG, "totalT out of range");
+  for (int d = 0; d < 4; d++)
+    if (r.source[d] < 0 || r.source[d] >= c->g.L[d]) return c->fail(P2_ERR_INVALID_ARG, "source outside the lattice");
+  if (r.moms) {
+    if (r.nmom < 1) return c->fail(P2_ERR_INVALID_ARG, "nmom < 1 with an explicit momentum list");
+    pl.moms.assign(r.moms, r.moms + 3 * r.nmom);
+  } else {
+    if (r.q2max < 0) return c->fail(P2_ERR_INVALID_ARG, "q2max < 0");
+    pl.moms = createMom(r.q2max);
+  }
+  pl.nmom = (int)pl.moms.size() / 3;
+  pl.K = components_of(r.contractions);
+  pl.Lmax = std::max(c->Ll[0], std::max(c->Ll[1], c->Ll[2]));
+  pl.totalT = r.totalT;
+  pl.blocks.clear();
+  size_t off = 0;
+  int k = 0;
+  for (const auto& b : kBlocks)
+    if (r.contractions & b.bit) {
+      p2::ScatterBlock sb;
+      sb.k0 = k;
+      sb.groups = b.groups;
+      sb.datasets = b.datasets;
+      sb.comps = b.comps;
+      sb.base = (long long)off;
+      pl.blocks.push_back(sb);
+      k += b.groups * b.datasets * b.comps;
+      off += (size_t)b.groups * b.datasets * b.comps * r.totalT * pl.nmom;
+    }
+  pl.total = off;
+  return P2_OK;
+}
+
+int chunk_slices(p2_ctx* c, int K) {
+  const size_t per = (size_t)K * c->V3 * 16;
+  size_t n = c->ws_budget / std::max<size_t>(per, 1);
+  return (int)std::max<size_t>(1, std::min<size_t>(n, (size_t)c->T));
+}
+
+p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request& r, const Plan& pl, double* dres) {
+  const p2_prop& u = props[r.prop_u];
+  const p2_prop& d = props[r.prop_d];
+  if (u.precision != P2_FP64 || d.precision != P2_FP64)
+    return c->fail(P2_ERR_UNSUPPORTED, "the plain FP64 form needs FP64 propagators");
+  if (r.contractions & (P2_DELTA_ISO12 | P2_DELTA_ISO32))
+    return c->fail(P2_ERR_UNSUPPORTED, "Delta contractions are not available in the plain FP64 form yet");
+
+  std::vector<double> tabh = phase_tables(c, pl.moms.data(), pl.nmom, r.source, -1, pl.Lmax);
+  P2_TRY(c, c->tab.ensure(tabh.size() * sizeof(double)), "phase table alloc");
+  P2_TRY(c, cudaMemcpyAsync(c->tab.p, tabh.data(), tabh.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream),
+         "phase table upload");
+
+  const int tc = chunk_slices(c, pl.K);
+  P2_TRY(c, c->cbuf.ensure((size_t)tc * pl.K * c->V3 * 16), "position buffer alloc");
+
+  const int ptiles = (pl.nmom + 63) / 64;
+  const int ktiles = (pl.K + 95) / 96;
+  for (const TauRun& run : local_runs(c, u, d, r.source, r.totalT)) {
+    for (int off = 0; off < run.n; off += tc) {
+      const int n = std::min(tc, run.n - off);
+      const int tau0 = run.tau0 + off;
+      p2::ContractArgs a{};
+      const int t_begin = (r.source[3] + tau0) % c->T;
+      p2_status s = chunk_view(c, u, c->stage_u, t_begin, n, a, true);
+      if (s != P2_OK) return s;
+      s = chunk_view(c, d, c->stage_d, t_begin, n, a, false);
+      if (s != P2_OK) return s;
+      a.V3 = (int)c->V3;
+      a.T = c->T;
+      a.t0 = r.source[3];
+      a.tau0 = tau0;
+      a.ntau = n;
+      a.what = r.contractions;
+      a.K = pl.K;
+      a.k = offsets_of(r.contractions);
+      a.out = c->cbuf.p;
+      P2_TRY(c, p2::launch_contract_plain(a, c->nsm, c->stream), "contract kernel");
+
+      p2::ProjArgs pa{};
+      pa.c = c->cbuf.p;
+      pa.sT = (long long)pl.K * c->V3;
+      pa.sK = c->V3;
+      pa.ntau = n;
+      pa.K = pl.K;
+      pa.V3 = (int)c->V3;
+      pa.nmom = pl.nmom;
+      pa.Lx = c->Ll[0];
+      pa.Ly = c->Ll[1];
+      pa.Lz = c->Ll[2];
+      pa.Lmax = pl.Lmax;
+      pa.tab = (const double*)c->tab.p;
+      int nsplit = (2 * c->nsm + ptiles * ktiles * n - 1) / (ptiles * ktiles * n);
+      nsplit = std::max(1, std::min(nsplit, (int)((c->V3 + 255) / 256)));
+      pa.chunk = (int)((((c->V3 + nsplit - 1) / nsplit) + 15) / 16 * 16);
+      pa.nsplit = (int)((c->V3 + pa.chunk - 1) / pa.chunk);
+      P2_TRY(c, c->part.ensure((size_t)n * pa.nsplit * pl.nmom * pl.K * 16), "partials alloc");
+      pa.part = (double*)c->part.p;
+      P2_TRY(c, p2::launch_project_fp64(pa, c->stream), "projection kernel");
+
+      p2::ScatterArgs sa{};
+      sa.part = (const double*)c->part.p;
+      sa.ntau = n;
+      sa.nsplit = pa.nsplit;
+      sa.nmom = pl.nmom;
+      sa.K = pl.K;
+      sa.tau0 = tau0;
+      sa.totalT = r.totalT;
+      sa.nblocks = (int)pl.blocks.size();
+      for (size_t b = 0; b < pl.blocks.size(); b++) sa.blk[b] = pl.blocks[b];
+      sa.out = dres;
+      P2_TRY(c, p2::launch_scatter(sa, c->stream), "reduction kernel");
+      if (u.location == P2_HOST || d.location == P2_HOST)
+        P2_TRY(c, cudaStreamSynchronize(c->stream), "staging reuse");
+    }
+  }
+  return P2_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+p2_status p2_ctx_create(const p2_geom* g, p2_ctx** out) {
+  if (!g || !out) return P2_ERR_INVALID_ARG;
+  *out = nullptr;
+  for (int d = 0; d < 4; d++) {
+    if (g->L[d] < 1 || g->procs[d] < 1 || g->L[d] % g->procs[d] != 0) return P2_ERR_INVALID_ARG;
+    if (g->coords[d] < 0 || g->coords[d] >= g->procs[d]) return P2_ERR_INVALID_ARG;
+  }
+  p2_ctx* c = new p2_ctx();
+  c->g = *g;
+  for (int d = 0; d < 4; d++) c->Ll[d] = g->L[d] / g->procs[d];
+  c->V3 = (long long)c->Ll[0] * c->Ll[1] * c->Ll[2];
+  c->T = g->L[3];
+  if (g->device < 0) {  // host-only context: argument checks and host helpers, no device work
+    c->host_only = true;
+    *out = c;
+    return P2_OK;
+  }
+  if (cudaSetDevice(g->device) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return P2_ERR_CUDA;
+  }
+  int nsm = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g->device) == cudaSuccess && nsm > 0) c->nsm = nsm;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return P2_ERR_CUDA;
+  }
+  c->own_stream = true;
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  c->ws_budget = std::min<size_t>((size_t)8 << 30, fr / 4);
+  if (c->ws_budget < ((size_t)64 << 20)) c->ws_budget = (size_t)64 << 20;
+  *out = c;
+  return P2_OK;
+}
+
+p2_status p2_ctx_destroy(p2_ctx* c) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  if (c->host_only) {
+    delete c;
+    return P2_OK;
+  }
+  cudaStreamSynchronize(c->stream);
+  for (DevBuf* b : {&c->cbuf, &c->part, &c->tab, &c->res, &c->stage_u, &c->stage_d, &c->scratch}) b->release();
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  p2::precision_release(c);
+  delete c;
+  return P2_OK;
+}
+
+const char* p2_last_error(const p2_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+p2_status p2_sync(p2_ctx* c) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
+  return c->cuda(cudaStreamSynchronize(c->stream), "p2_sync");
+}
+
+p2_status p2_set_stream(p2_ctx* c, void* s) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
+  if (c->own_stream) {
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+    c->own_stream = false;
+  }
+  if (s) {
+    c->stream = (cudaStream_t)s;
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return c->fail(P2_ERR_CUDA, "stream create");
+    c->own_stream = true;
+  }
+  return P2_OK;
+}
+
+int p2_components(unsigned what) { return (what & ~kAllBits) ? -1 : components_of(what); }
+
+int p2_mom_list(int q2max, int* moms) {
+  if (q2max < 0) return -1;
+  std::vector<int> m = createMom(q2max);
+  if (moms) std::memcpy(moms, m.data(), m.size() * sizeof(int));
+  return (int)m.size() / 3;
+}
+
+int p2_block_info(unsigned what, int totalT, int nmom, p2_block* blocks, int max_blocks, size_t* total) {
+  if (what & ~kAllBits) return -1;
+  int n = 0;
+  size_t off = 0;
+  for (const auto& b : kBlocks)
+    if (what & b.bit) {
+      if (blocks && n < max_blocks) {
+        blocks[n].bit = b.bit;
+        blocks[n].groups = b.groups;
+        blocks[n].datasets = b.datasets;
+        blocks[n].comps = b.comps;
+        blocks[n].offset = off;
+      }
+      n++;
+      off += (size_t)b.groups * b.datasets * b.comps * totalT * nmom;
+    }
+  if (total) *total = off;
+  return n;
+}
+
+p2_status p2_contract_project(p2_ctx* c, const p2_prop* props, int nprops, const p2_request* reqs, int nreq) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  if (!props || nprops < 1 || !reqs || nreq < 1) return c->fail(P2_ERR_INVALID_ARG, "empty props or requests");
+  for (int i = 0; i < nprops; i++) {
+    p2_status s = check_prop(c, props[i], "prop");
+    if (s != P2_OK) return s;
+  }
+  std::vector<Plan> plans(nreq);
+  for (int i = 0; i < nreq; i++) {
+    const p2_request& r = reqs[i];
+    if (r.prop_u < 0 || r.prop_u >= nprops || r.prop_d < 0 || r.prop_d >= nprops)
+      return c->fail(P2_ERR_INVALID_ARG, "prop index out of range");
+    if (!r.out) return c->fail(P2_ERR_INVALID_ARG, "null output");
+    if (r.mode != P2_PLAIN_FP64 && r.mode != P2_SPLIT_FP16) return c->fail(P2_ERR_INVALID_ARG, "bad mode");
+    if (r.out_location != P2_DEVICE && r.out_location != P2_HOST)
+      return c->fail(P2_ERR_INVALID_ARG, "bad out_location");
+    p2_status s = make_plan(c, r, plans[i]);
+    if (s != P2_OK) return s;
+  }
+  if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
+  if (nreq > 1 && reqs[0].mode == P2_SPLIT_FP16) {
+    bool all = true;
+    for (int i = 0; i < nreq; i++) all &= reqs[i].mode == P2_SPLIT_FP16;
+    if (all) return p2::precision_run_batch(c, props, nprops, reqs, nreq);
+  }
+  for (int i = 0; i < nreq; i++) {
+    const p2_request& r = reqs[i];
+    const Plan& pl = plans[i];
+    double* dres = r.out;
+    if (r.out_location == P2_HOST) {
+      P2_TRY(c, c->res.ensure(pl.total * 16), "result alloc");
+      P2_TRY(c, cudaMemsetAsync(c->res.p, 0, pl.total * 16, c->stream), "result clear");
+      dres = (double*)c->res.p;
+    }
+    p2_status s = r.mode == P2_PLAIN_FP64 ? run_plain(c, props, r, pl, dres)
+                                          : p2::precision_run_batch(c, props, nprops, &r, 1);
+    if (s != P2_OK) return s;
+    if (r.out_location == P2_HOST && r.mode == P2_PLAIN_FP64) {
+      P2_TRY(c, cudaMemcpyAsync(r.out, dres, pl.total * 16, cudaMemcpyDeviceToHost, c->stream), "result download");
+      P2_TRY(c, cudaStreamSynchronize(c->stream), "result download");
+    }
+  }
+  return P2_OK;
+}
+
+p2_status p2_contract_position(p2_ctx* c, const p2_prop* props, int nprops, const p2_request* r) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  if (!props || !r || nprops < 1) return c->fail(P2_ERR_INVALID_ARG, "empty props or request");
+  for (int i = 0; i < nprops; i++) {
+    p2_status s = check_prop(c, props[i], "prop");
+    if (s != P2_OK) return s;
+  }
+  if (r->prop_u < 0 || r->prop_u >= nprops || r->prop_d < 0 || r->prop_d >= nprops)
+    return c->fail(P2_ERR_INVALID_ARG, "prop index out of range");
+  if (!r->out) return c->fail(P2_ERR_INVALID_ARG, "null output");
+  if (r->contractions == 0 || (r->contractions & ~kAllBits))
+    return c->fail(P2_ERR_INVALID_ARG, "contractions: empty or unknown bits");
+  if (r->contractions & (P2_DELTA_ISO12 | P2_DELTA_ISO32))
+    return c->fail(P2_ERR_UNSUPPORTED, "Delta contractions are not available in the plain FP64 form yet");
+  if (r->totalT < 1 || r->totalT > c->T) return c->fail(P2_ERR_INVALID_ARG, "totalT out of range");
+  const p2_prop& u = props[r->prop_u];
+  const p2_prop& d = props[r->prop_d];
+  if (u.precision != P2_FP64 || d.precision != P2_FP64)
+    return c->fail(P2_ERR_UNSUPPORTED, "position-space output needs FP64 propagators");
+  if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
+  const int K = components_of(r->contractions);
+  const size_t slice = (size_t)K * c->V3;
+  for (const TauRun& run : local_runs(c, u, d, r->source, r->totalT)) {
+    p2::ContractArgs a{};
+    const int t_begin = (r->source[3] + run.tau0) % c->T;
+    p2_status s = chunk_view(c, u, c->stage_u, t_begin, run.n, a, true);
+    if (s != P2_OK) return s;
+    s = chunk_view(c, d, c->stage_d, t_begin, run.n, a, false);
+    if (s != P2_OK) return s;
+    a.V3 = (int)c->V3;
+    a.T = c->T;
+    a.t0 = r->source[3];
+    a.tau0 = run.tau0;
+    a.ntau = run.n;
+    a.what = r->contractions;
+    a.K = K;
+    a.k = offsets_of(r->contractions);
+    double* dst = r->out + 2 * slice * run.tau0;
+    if (r->out_location == P2_HOST) {
+      P2_TRY(c, c->cbuf.ensure(slice * run.n * 16), "position buffer alloc");
+      a.out = c->cbuf.p;
+    } else {
+      a.out = dst;
+    }
+    P2_TRY(c, p2::launch_contract_plain(a, c->nsm, c->stream), "contract kernel");
+    if (r->out_location == P2_HOST) {
+      P2_TRY(c, cudaMemcpyAsync(dst, c->cbuf.p, slice * run.n * 16, cudaMemcpyDeviceToHost, c->stream),
+             "position download");
+      P2_TRY(c, cudaStreamSynchronize(c->stream), "position download");
+    } else if (u.location == P2_HOST || d.location == P2_HOST) {
+      P2_TRY(c, cudaStreamSynchronize(c->stream), "staging reuse");
+    }
+  }
+  return P2_OK;
+}
+
+p2_status p2_ft_apply(p2_ctx* c, const double* field, int dof, int nt, const int* moms, int nmom, int sign,
+                      double* out, int out_location) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  if (!field || !out || dof < 1 || nt < 1 || nt > c->Ll[3] || !moms || nmom < 1)
+    return c->fail(P2_ERR_INVALID_ARG, "p2_ft_apply: bad arguments");
+  if (sign != 1 && sign != -1) return c->fail(P2_ERR_INVALID_ARG, "p2_ft_apply: sign must be +1 or -1");
+  if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
+  const int Lmax = std::max(c->Ll[0], std::max(c->Ll[1], c->Ll[2]));
+  const int origin[4] = {0, 0, 0, 0};
+  std::vector<double> tabh = phase_tables(c, moms, nmom, origin, sign, Lmax);
+  P2_TRY(c, c->tab.ensure(tabh.size() * sizeof(double)), "phase table alloc");
+  P2_TRY(c, cudaMemcpyAsync(c->tab.p, tabh.data(), tabh.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream),
+         "phase table upload");
+  p2::ProjArgs pa{};
+  pa.c = field;
+  pa.sT = c->V3;
+  pa.sK = c->V3 * nt;
+  pa.ntau = nt;
+  pa.K = dof;
+  pa.V3 = (int)c->V3;
+  pa.nmom = nmom;
+  pa.Lx = c->Ll[0];
+  pa.Ly = c->Ll[1];
+  pa.Lz = c->Ll[2];
+  pa.Lmax = Lmax;
+  pa.tab = (const double*)c->tab.p;
+  const int ptiles = (nmom + 63) / 64, ktiles = (dof + 31) / 32;
+  int nsplit = (2 * c->nsm + ptiles * ktiles * nt - 1) / (ptiles * ktiles * nt);
+  nsplit = std::max(1, std::min(nsplit, (int)((c->V3 + 255) / 256)));
+  pa.chunk = (int)((((c->V3 + nsplit - 1) / nsplit) + 15) / 16 * 16);
+  pa.nsplit = (int)((c->V3 + pa.chunk - 1) / pa.chunk);
+  P2_TRY(c, c->part.ensure((size_t)nt * pa.nsplit * nmom * dof * 16), "partials alloc");
+  pa.part = (double*)c->part.p;
+  P2_TRY(c, p2::launch_project_fp64(pa, c->stream), "projection kernel");
+  const size_t total = (size_t)nt * dof * nmom;
+  double* dst = out;
+  if (out_location == P2_HOST) {
+    P2_TRY(c, c->res.ensure(total * 16), "result alloc");
+    dst = (double*)c->res.p;
+  }
+  p2::ScatterArgs sa{};
+  sa.part = (const double*)c->part.p;
+  sa.ntau = nt;
+  sa.nsplit = pa.nsplit;
+  sa.nmom = nmom;
+  sa.K = dof;
+  sa.tau0 = 0;
+  sa.totalT = nt;
+  sa.nblocks = 0;
+  sa.oT = (long long)dof * nmom;
+  sa.oK = nmom;
+  sa.out = dst;
+  P2_TRY(c, p2::launch_scatter(sa, c->stream), "reduction kernel");
+  if (out_location == P2_HOST) {
+    P2_TRY(c, cudaMemcpyAsync(out, dst, total * 16, cudaMemcpyDeviceToHost, c->stream), "result download");
+    P2_TRY(c, cudaStreamSynchronize(c->stream), "result download");
+  }
+  return P2_OK;
+}
+
+p2_status p2_synth_propagator(p2_ctx* c, void* dst, int on_device, int precision, uint64_t seed, int flavour, int t0,
+                              double decay, int t_first, int nt) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  if (!dst || nt < 1 || nt > c->T || t_first < 0 || t_first >= c->T || t0 < 0 || t0 >= c->T)
+    return c->fail(P2_ERR_INVALID_ARG, "p2_synth_propagator: bad arguments");
+  if (precision != P2_FP64 && precision != P2_FP32) return c->fail(P2_ERR_INVALID_ARG, "bad precision");
+  if (on_device) {
+    if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
+    P2_TRY(c,
+           p2::launch_synth(dst, precision == P2_FP32, seed, flavour, t0, decay, t_first, nt, c->g.L, c->Ll,
+                            c->g.coords, c->stream),
+           "synth kernel");
+    return P2_OK;
+  }
+  p2::synth_host(dst, precision == P2_FP32, seed, flavour, t0, decay, t_first, nt, c->g.L, c->Ll, c->g.coords);
+  return P2_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,104 @@
+// Shared device helpers: complex arithmetic in registers, the propagator
+// index map, cp.async staging and half-warp shuffles.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "spin_tables.h"
+
+namespace p2 {
+
+template <typename R>
+struct alignas(2 * sizeof(R)) Cx {
+  R x, y;
+};
+
+template <typename R>
+__device__ __forceinline__ Cx<R> cx(R x, R y) {
+  Cx<R> c;
+  c.x = x;
+  c.y = y;
+  return c;
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> czero() {
+  return cx<R>(R(0), R(0));
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> operator+(Cx<R> a, Cx<R> b) {
+  return cx<R>(a.x + b.x, a.y + b.y);
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> operator-(Cx<R> a, Cx<R> b) {
+  return cx<R>(a.x - b.x, a.y - b.y);
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> cscale(Cx<R> a, R s) {
+  return cx<R>(a.x * s, a.y * s);
+}
+// acc += a * b
+template <typename R>
+__device__ __forceinline__ void cmac(Cx<R>& acc, Cx<R> a, Cx<R> b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+}
+// acc -= a * b
+template <typename R>
+__device__ __forceinline__ void cmsub(Cx<R>& acc, Cx<R> a, Cx<R> b) {
+  acc.x = fma(-a.x, b.x, acc.x);
+  acc.x = fma(a.y, b.y, acc.x);
+  acc.y = fma(-a.x, b.y, acc.y);
+  acc.y = fma(-a.y, b.x, acc.y);
+}
+// acc += a * conj(b)
+template <typename R>
+__device__ __forceinline__ void cmac_conj(Cx<R>& acc, Cx<R> a, Cx<R> b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(a.y, b.y, acc.x);
+  acc.y = fma(a.y, b.x, acc.y);
+  acc.y = fma(-a.x, b.y, acc.y);
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
+  return cx<R>(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// a * (re + i im) for re, im in {-1, 0, 1}
+template <typename R>
+__device__ __forceinline__ Cx<R> cunit(Cx<R> a, int re, int im) {
+  return cx<R>(R(re) * a.x - R(im) * a.y, R(re) * a.y + R(im) * a.x);
+}
+
+// Index of spin block (mu, nu) in a site's 144 components; colour (a, b) adds a*3 + b.
+__host__ __device__ constexpr int sblk(int mu, int nu) { return (mu * 4 + nu) * 9; }
+
+// Half-warp shuffles: lanes 0..15 of each half of a warp exchange among themselves.
+__device__ __forceinline__ unsigned halfwarp_mask() {
+  return (threadIdx.x & 16) ? 0xFFFF0000u : 0x0000FFFFu;
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> shfl_xor16(Cx<R> v, int m, unsigned mask) {
+  return cx<R>(__shfl_xor_sync(mask, v.x, m, 16), __shfl_xor_sync(mask, v.y, m, 16));
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> shfl_idx16(Cx<R> v, int src, unsigned mask) {
+  return cx<R>(__shfl_sync(mask, v.x, src, 16), __shfl_sync(mask, v.y, src, 16));
+}
+
+// Asynchronous global -> shared copies (LDGSTS).  Bytes beyond src_bytes are zero-filled.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int src_bytes) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+}  // namespace p2

@@ -1,0 +1,167 @@
+// Direct FP64 phase sum and the deterministic cross-block reduction.
+//
+// C(t, p, k) = sum_x c_k(x, t) exp(sign * i p.(x - x0)), the reference's
+// fourier_transform_3D (lib/kernels/PLEGMA_kernel_utils.cuh:820-860) and the
+// host block sum after it (PLEGMA_baryons.cuh:197-206, PLEGMA_mesons*.cuh).
+// Per time slice this is a complex [nmom x V3] . [V3 x K] product; the phase
+// matrix is never stored: each entry is the product of three per-dimension
+// phase tables (p.x = sum_d n_d x_d), built on the host in double precision.
+//
+// CTA tile 64 momenta x (16*TK) components, 256 threads, each thread a
+// 4 x TK register tile; sites are consumed 16 at a time from shared memory.
+// The site range of a slice is split over `nsplit` CTAs whose partial sums
+// go to `part`; k_scatter adds them in a fixed order (bitwise reproducible)
+// and writes the result layout.
+#include "kernels.cuh"
+#include "p2_common.cuh"
+
+namespace p2 {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kXS = 16;  // sites per step
+constexpr int kTP = 4;   // momenta per thread
+constexpr int kPT = 16 * kTP;
+
+template <int TK>
+__global__ void __launch_bounds__(kThreads, 1) k_project_fp64(const ProjArgs a) {
+  constexpr int KT = 16 * TK;
+  __shared__ Cx<double> sE[kXS][kPT];
+  __shared__ Cx<double> sC[kXS][KT];
+  const int tid = threadIdx.x;
+  const int tp = tid >> 4, tk = tid & 15;
+  const int ktiles = (a.K + KT - 1) / KT;
+  const int p0 = (blockIdx.x / ktiles) * kPT;
+  const int k0 = (blockIdx.x % ktiles) * KT;
+  const int split = blockIdx.y;
+  const int tau = blockIdx.z;
+  const int xb = split * a.chunk;
+  const int xe = min(a.V3, xb + a.chunk);
+  const Cx<double>* c = (const Cx<double>*)a.c + (long long)tau * a.sT;
+  const Cx<double>* tab = (const Cx<double>*)a.tab;
+  const int LxLy = a.Lx * a.Ly;
+
+  Cx<double> acc[kTP][TK];
+#pragma unroll
+  for (int i = 0; i < kTP; i++)
+#pragma unroll
+    for (int j = 0; j < TK; j++) acc[i][j] = czero<double>();
+
+  for (int xs0 = xb; xs0 < xe; xs0 += kXS) {
+    // phases for 16 sites x 64 momenta
+#pragma unroll
+    for (int r = 0; r < (kXS * kPT) / kThreads; r++) {
+      const int e = tid + r * kThreads;
+      const int xs = e / kPT, pp = e % kPT;
+      const int p = p0 + pp, x = xs0 + xs;
+      Cx<double> v = czero<double>();
+      if (p < a.nmom && x < xe) {
+        const int xx = x % a.Lx, yy = (x / a.Lx) % a.Ly, zz = x / LxLy;
+        const Cx<double> ex = tab[(0 * a.nmom + p) * a.Lmax + xx];
+        const Cx<double> ey = tab[(1 * a.nmom + p) * a.Lmax + yy];
+        const Cx<double> ez = tab[(2 * a.nmom + p) * a.Lmax + zz];
+        v = cmul(cmul(ex, ey), ez);
+      }
+      sE[xs][pp] = v;
+    }
+    // site values for 16 sites x KT components (coalesced along x)
+#pragma unroll
+    for (int r = 0; r < (kXS * KT) / kThreads; r++) {
+      const int e = tid + r * kThreads;
+      const int xs = e % kXS, kk = e / kXS;
+      const int k = k0 + kk, x = xs0 + xs;
+      Cx<double> v = czero<double>();
+      if (k < a.K && x < xe) v = c[(long long)k * a.sK + x];
+      sC[xs][kk] = v;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int xs = 0; xs < kXS; xs++) {
+      Cx<double> ev[kTP], cv[TK];
+#pragma unroll
+      for (int i = 0; i < kTP; i++) ev[i] = sE[xs][tp + 16 * i];
+#pragma unroll
+      for (int j = 0; j < TK; j++) cv[j] = sC[xs][tk + 16 * j];
+#pragma unroll
+      for (int i = 0; i < kTP; i++)
+#pragma unroll
+        for (int j = 0; j < TK; j++) cmac(acc[i][j], ev[i], cv[j]);
+    }
+    __syncthreads();
+  }
+  Cx<double>* part = (Cx<double>*)a.part + ((long long)tau * a.nsplit + split) * a.nmom * a.K;
+#pragma unroll
+  for (int i = 0; i < kTP; i++) {
+    const int p = p0 + tp + 16 * i;
+    if (p >= a.nmom) continue;
+#pragma unroll
+    for (int j = 0; j < TK; j++) {
+      const int k = k0 + tk + 16 * j;
+      if (k < a.K) part[(long long)p * a.K + k] = acc[i][j];
+    }
+  }
+}
+
+__global__ void k_scatter(const ScatterArgs a) {
+  const long long n = (long long)a.ntau * a.nmom * a.K;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i % a.K);
+    const int p = (int)((i / a.K) % a.nmom);
+    const int tau = (int)(i / ((long long)a.K * a.nmom));
+    const Cx<double>* src = (const Cx<double>*)a.part + ((long long)tau * a.nsplit * a.nmom + p) * a.K + k;
+    Cx<double> s = czero<double>();
+    for (int sp = 0; sp < a.nsplit; sp++) s = s + src[(long long)sp * a.nmom * a.K];
+    long long o = -1;
+    if (a.nblocks == 0) {
+      o = (long long)(a.tau0 + tau) * a.oT + (long long)k * a.oK + p;
+    } else {
+      for (int b = 0; b < a.nblocks; b++) {
+        const ScatterBlock& B = a.blk[b];
+        const int rel = k - B.k0;
+        if (rel >= 0 && rel < B.groups * B.datasets * B.comps) {
+          const int comp = rel % B.comps;
+          const int gd = rel / B.comps;  // group * datasets + dataset
+          o = B.base + (((long long)gd * a.totalT + a.tau0 + tau) * a.nmom + p) * B.comps + comp;
+        }
+      }
+    }
+    if (o >= 0) ((Cx<double>*)a.out)[o] = s;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_project_fp64(const ProjArgs& a, cudaStream_t s) {
+  int tk = 8;
+  // pick the component tile (16*TK) that wastes least
+  int best = 1 << 30;
+  for (int cand : {8, 6, 4, 2}) {
+    const int kt = 16 * cand;
+    const int waste = ((a.K + kt - 1) / kt) * kt - a.K;
+    if (waste < best) {
+      best = waste;
+      tk = cand;
+    }
+  }
+  const int ptiles = (a.nmom + kPT - 1) / kPT;
+  const int ktiles = (a.K + 16 * tk - 1) / (16 * tk);
+  dim3 grid(ptiles * ktiles, a.nsplit, a.ntau);
+  switch (tk) {
+    case 2: k_project_fp64<2><<<grid, kThreads, 0, s>>>(a); break;
+    case 4: k_project_fp64<4><<<grid, kThreads, 0, s>>>(a); break;
+    case 6: k_project_fp64<6><<<grid, kThreads, 0, s>>>(a); break;
+    default: k_project_fp64<8><<<grid, kThreads, 0, s>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(const ScatterArgs& a, cudaStream_t s) {
+  const long long n = (long long)a.ntau * a.nmom * a.K;
+  int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+  if (blocks < 1) blocks = 1;
+  k_scatter<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace p2

@@ -1,0 +1,235 @@
+"""Spin/colour algebra for the hadron two-point contractions, derived from the
+gamma-matrix definitions (no tables are copied from the reference).
+
+Basis
+-----
+PLEGMA works in the Euclidean Dirac--Pauli basis (lib/kernels/PLEGMA_gammas.cuh:6-41,
+python/baryons.py:36-54):
+
+    gamma_k = i * [[0, sigma_k], [-sigma_k, 0]]   (k = 1, 2, 3)
+    gamma_4 = diag(1, 1, -1, -1)
+    gamma_5 = gamma_1 gamma_2 gamma_3 gamma_4
+    C       = i gamma_2 gamma_4                    (python/baryons.py:58)
+
+Every table the kernels need is computed here from those four matrices:
+
+* the 16 Dirac structures in PLEGMA's order (1, g1..g4, g5, g5g1..g5g4,
+  -i/2[g1,g2], -i/2[g1,g3], -i/2[g2,g3], -i/2[g4,g1], -i/2[g4,g2], -i/2[g4,g3]),
+  each as a signed permutation (every one has exactly one non-zero per row);
+* the diquark spin tables for the nucleon (C g5 x C g5-bar,
+  PLEGMA_baryons_NtoN.cu:3-4) and the Delta (C g_k x C g_k-bar,
+  PLEGMA_baryons_deltas.cu:3-4), Gamma-bar = g4 Gamma^dagger g4;
+* the Levi-Civita permutation list in the order PLEGMA sums it
+  (PLEGMA_kernel_utils.cuh:49-56);
+* the momentum list in `createMom` order (lib/PLEGMA_FT.cu:50-72).
+
+`emit_header()` writes these as constexpr tables for the CUDA sources.
+"""
+from __future__ import annotations
+
+import hashlib
+import itertools
+import json
+from typing import List, Tuple
+
+import numpy as np
+
+I = 1j
+NS = 4
+NC = 3
+
+_s = [np.array([[0, 1], [1, 0]], dtype=complex),
+      np.array([[0, -I], [I, 0]], dtype=complex),
+      np.array([[1, 0], [0, -1]], dtype=complex)]
+_z = np.zeros((2, 2), dtype=complex)
+_e = np.eye(2, dtype=complex)
+
+
+def _blk(a, b, c, d):
+    return np.block([[a, b], [c, d]])
+
+
+G1 = I * _blk(_z, _s[0], -_s[0], _z)
+G2 = I * _blk(_z, _s[1], -_s[1], _z)
+G3 = I * _blk(_z, _s[2], -_s[2], _z)
+G4 = _blk(_e, _z, _z, -_e)
+ONE = np.eye(4, dtype=complex)
+G5 = G1 @ G2 @ G3 @ G4
+CMAT = I * G2 @ G4
+GK = [G1, G2, G3]
+
+
+def bar(m: np.ndarray) -> np.ndarray:
+    """Dirac adjoint of a source structure: g4 M^dagger g4."""
+    return G4 @ m.conj().T @ G4
+
+
+def _sigma(a, b):
+    return -0.5 * I * (a @ b - b @ a)
+
+
+#: The 16 structures in the order of PLEGMA_gammas.cuh (and the GAMMAS enum).
+GAMMA16 = [ONE, G1, G2, G3, G4, G5, G5 @ G1, G5 @ G2, G5 @ G3, G5 @ G4,
+           _sigma(G1, G2), _sigma(G1, G3), _sigma(G2, G3),
+           _sigma(G4, G1), _sigma(G4, G2), _sigma(G4, G3)]
+GAMMA16_NAMES = ["1", "g1", "g2", "g3", "g4", "g5", "g5g1", "g5g2", "g5g3", "g5g4",
+                 "s12", "s13", "s23", "s41", "s42", "s43"]
+
+CG5 = CMAT @ G5
+CGK = [CMAT @ g for g in GK]
+P_PLUS = 0.5 * (ONE + G4)
+P_MINUS = 0.5 * (ONE - G4)
+
+
+def signed_permutation(m: np.ndarray) -> Tuple[List[int], List[complex]]:
+    """Row r of `m` has its only non-zero at column perm[r] with value phase[r]."""
+    perm, phase = [], []
+    for r in range(NS):
+        nz = [c for c in range(NS) if abs(m[r, c]) > 1e-12]
+        if len(nz) != 1:
+            raise ValueError("not a signed permutation")
+        perm.append(nz[0])
+        phase.append(complex(np.round(m[r, nz[0]], 12)))
+    return perm, phase
+
+
+def gamma16_tables():
+    """(perm[16][4], re[16][4], im[16][4]) of the 16 Dirac structures."""
+    perms, res, ims = [], [], []
+    for g in GAMMA16:
+        p, v = signed_permutation(g)
+        perms.append(p)
+        res.append([int(round(x.real)) for x in v])
+        ims.append([int(round(x.imag)) for x in v])
+    return perms, res, ims
+
+
+def diquark_table(gamma: np.ndarray):
+    """Spin table of a baryon two-point function with interpolator
+    eps_abc (q1_a^T Gamma q2_b) q3_c at the sink and its adjoint at the source.
+
+    Entries (nu, lambda, lambda', nu', value) with value = Gamma[nu][lambda] *
+    Gamma-bar[lambda'][nu'], enumerated over the non-zeros of Gamma (row major)
+    and then of Gamma-bar (row major).  The value is real for C g5 and C g_k.
+    """
+    gb = bar(gamma)
+    rows = []
+    for nu, lu in itertools.product(range(NS), range(NS)):
+        if abs(gamma[nu, lu]) < 1e-12:
+            continue
+        for lup, nup in itertools.product(range(NS), range(NS)):
+            if abs(gb[lup, nup]) < 1e-12:
+                continue
+            v = gamma[nu, lu] * gb[lup, nup]
+            if abs(v.imag) > 1e-12:
+                raise ValueError("complex diquark weight")
+            rows.append((nu, lu, lup, nup, int(round(v.real))))
+    return rows
+
+
+def nucleon_table():
+    return diquark_table(CG5)
+
+
+def delta_tables():
+    return [diquark_table(c) for c in CGK]
+
+
+def levi_civita():
+    """The six colour permutations (a, b, c) and their signs, even ones first:
+    the cyclic rotations of (0,1,2), then the transpositions (0<->2), (1<->2),
+    (0<->1) of the identity.  This is the summation order PLEGMA uses."""
+    base = (0, 1, 2)
+    even = [tuple(base[(i - k) % 3] for i in range(3)) for k in range(3)]
+    odd = []
+    for i, j in ((0, 2), (1, 2), (0, 1)):
+        p = list(base)
+        p[i], p[j] = p[j], p[i]
+        odd.append(tuple(p))
+    return even + odd, [1, 1, 1, -1, -1, -1]
+
+
+def create_mom(q2_max: int, dims: int = 3) -> List[Tuple[int, ...]]:
+    """Momentum list in the order of PLEGMA_FT::createMom (lib/PLEGMA_FT.cu:50-72):
+    by |n|^2 ascending, each component running from +iQ down to -iQ."""
+    out = []
+    for iq in range(q2_max + 1):
+        rng = range(iq, -iq - 1, -1)
+        if dims == 3:
+            for nx in rng:
+                for ny in rng:
+                    for nz in rng:
+                        if nx * nx + ny * ny + nz * nz == iq:
+                            out.append((nx, ny, nz))
+        else:
+            for nx in rng:
+                for ny in rng:
+                    for nz in rng:
+                        for nt in rng:
+                            if nx * nx + ny * ny + nz * nz + nt * nt == iq:
+                                out.append((nx, ny, nz, nt))
+    return out
+
+
+def table_digest(rows) -> str:
+    """SHA-256 of a table flattened to integers; used to pin tables against
+    the reference's without storing them."""
+    flat = [int(round(float(x))) for x in np.asarray(rows, dtype=float).ravel()]
+    return hashlib.sha256(json.dumps(flat).encode()).hexdigest()
+
+
+def _c_array(name, ctype, data, fmt="{}"):
+    """A brace-initialiser macro P2_INIT_<name> and a constexpr array using it
+    (device code declares local constexpr copies from the macro so that fully
+    unrolled loops fold every lookup)."""
+    arr = np.asarray(data)
+    dims = "".join(f"[{d}]" for d in arr.shape)
+
+    def rec(a):
+        if a.ndim == 1:
+            return "{" + ",".join(fmt.format(int(x)) for x in a) + "}"
+        return "{" + ",".join(rec(x) for x in a) + "}"
+    macro = "P2_INIT_" + name[1:] if name.startswith("k") else "P2_INIT_" + name
+    return (f"#define {macro} {rec(arr)}\n"
+            f"static constexpr {ctype} {name}{dims} = {macro};\n")
+
+
+def header_text() -> str:
+    perms, res, ims = gamma16_tables()
+    nuc = nucleon_table()
+    dl = delta_tables()
+    eps, sgn = levi_civita()
+    out = ["// Generated by plegma_b200/spin.py from the gamma-matrix definitions.\n",
+           "// Do not edit: rerun `python -m plegma_b200.spin` instead.\n",
+           "#pragma once\n", "namespace p2 {\n",
+           _c_array("kGammaPerm", "int", perms),
+           _c_array("kGammaRe", "int", res),
+           _c_array("kGammaIm", "int", ims),
+           _c_array("kNucIdx", "int", [r[:4] for r in nuc]),
+           _c_array("kNucVal", "int", [r[4] for r in nuc]),
+           _c_array("kDeltaIdx", "int", [[r[:4] for r in t] for t in dl]),
+           _c_array("kDeltaVal", "int", [[r[4] for r in t] for t in dl]),
+           _c_array("kEps", "int", eps),
+           _c_array("kEpsSign", "int", sgn),
+           "}  // namespace p2\n"]
+    return "".join(out)
+
+
+def emit_header(path: str) -> bool:
+    """Write the generated table header; returns True if the file changed."""
+    text = header_text()
+    try:
+        with open(path) as f:
+            if f.read() == text:
+                return False
+    except FileNotFoundError:
+        pass
+    with open(path, "w") as f:
+        f.write(text)
+    return True
+
+
+if __name__ == "__main__":
+    import os
+    here = os.path.dirname(os.path.abspath(__file__))
+    emit_header(os.path.join(here, "csrc", "spin_tables.h"))
