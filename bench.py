@@ -1,0 +1,319 @@
+#!/usr/bin/env python
+"""Benchmark: hadron two-point contraction + momentum projection at 48^3 x 96.
+
+Workload (one step): one source, both Wick contractions of the nucleon C g5
+(2 datasets x 16 open spin) plus all 16 x 16 meson Gamma insertions
+(K = 288 components per site), projected onto the 123 momenta |n|^2 <= 9 for
+all 96 time slices = 10,616,832 sites.  Propagators u, d: seeded synthetic
+FP64 (Gaussian entries x exp(-0.5 |t - t0|)), 24.5 GB each, resident in HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--form split|plain]
+
+Under torchrun each rank contracts its own source (seed + rank): the path
+shards by source with no data exchange, so scaling is weak and the value is
+all ranks' sites over the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L = (48, 48, 48, 96)
+Q2MAX = 9
+SEED = 1003
+METRIC = "2pt contraction+projection sites/s at 48^3x96"
+WORKLOAD = "48^3x96 nucleon Cg5 (2x16) + 16x16 meson Gamma pairs, K=288, |n|^2<=9 (123 momenta), 1 source, 96 slices"
+
+
+def source_for(seed):
+    rng = np.random.default_rng(seed)
+    return (int(rng.integers(0, L[0])), int(rng.integers(0, L[1])), int(rng.integers(0, L[2])),
+            int(rng.integers(0, L[3])))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.stop = threading.Event()
+        self.th = None
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.th = threading.Thread(target=self._run, daemon=True)
+        self.th.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.th.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 4 + i and r[4 + i].lower().startswith("active"):
+                    reasons.add(n)
+        pw = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None, "samples": len(self.rows), "reasons": sorted(reasons)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], p["bf16_tflops"], "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+def cpu_baseline_port(steps=1):
+    """The FP64 oracle (faithful restatement of the reference loops, OpenMP on
+    all host cores) on a bounded sample: one time slice of a 16^3 spatial
+    lattice with the same K = 288 components and 123 momenta (cost per site
+    does not depend on the volume)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as orc
+    from plegma_b200 import spin
+    Ls = (16, 16, 16, 4)
+    V3 = 16 ** 3
+    rng = np.random.default_rng(SEED)
+    u = (rng.standard_normal((144, V3 * 4)) + 1j * rng.standard_normal((144, V3 * 4)))
+    d = (rng.standard_normal((144, V3 * 4)) + 1j * rng.standard_normal((144, V3 * 4)))
+    moms = np.array(spin.create_mom(Q2MAX), dtype=np.int32)
+    orc.twopt(Ls, u, d, (1, 2, 3, 0), moms, 1 | 8, [0], want_abs=False)  # warm-up (page-in, thread pool)
+    vals = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        orc.twopt(Ls, u, d, (1, 2, 3, 0), moms, 1 | 8, [1], want_abs=False)
+        vals.append(V3 / (time.perf_counter() - t))
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": float(np.median(vals)), "unit": "sites/s", "cores": cores, "kind": "port",
+            "sample": f"1 time slice of 16^3 ({V3} sites), K=288, 123 momenta, FP64 oracle, median of {steps}"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        cpu_baseline_port(1)
+    t = time.perf_counter()
+    cb = cpu_baseline_port(args.steps)
+    el = time.perf_counter() - t
+    v = cb["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "sites/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "sample": cb["sample"]},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": "sites/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="auto", choices=["auto", "split", "plain"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from plegma_b200 import lib as p2
+    ctx = p2.Context(L, device=local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+
+    seed = SEED + rank
+    src = source_for(seed)
+    V3 = L[0] * L[1] * L[2]
+    sites = V3 * L[3]
+    what = p2.NUCLEON_CG5 | p2.MESON_G16
+    K = p2.components(what)
+    moms = p2.mom_list(Q2MAX)
+    nmom = len(moms)
+    blocks, total = p2.block_info(what, L[3], nmom)
+    u = torch.empty(144 * sites, dtype=torch.complex128, device="cuda")
+    d = torch.empty_like(u)
+    ctx.synth(u.data_ptr(), True, p2.P2_FP64, seed, 0, src[3], 0.5)
+    ctx.synth(d.data_ptr(), True, p2.P2_FP64, seed, 1, src[3], 0.5)
+    out = torch.zeros(total, dtype=torch.complex128, device="cuda")
+    props = [ctx.prop(u.data_ptr(), nt=L[3]), ctx.prop(d.data_ptr(), nt=L[3])]
+
+    forms = {}
+    if args.form in ("auto", "split"):
+        forms["split"] = p2.P2_SPLIT_FP16
+    if args.form in ("auto", "plain"):
+        forms["plain"] = p2.P2_PLAIN_FP64
+
+    def step(mode):
+        ctx.contract_project(props, [ctx.request(src, L[3], what, out.data_ptr(), mode=mode, q2max=Q2MAX)])
+
+    results = {}
+    hbm, bf16, peak_kind = peaks()
+    for name, mode in forms.items():
+        try:
+            step(mode)
+        except p2.P2Error as e:
+            if e.status == p2.P2_ERR_UNSUPPORTED and args.form == "auto":
+                continue
+            raise
+        for _ in range(max(args.warmup - 1, 0)):
+            step(mode)
+        torch.cuda.synchronize()
+        ctx.profile(True)
+        ctx.profile_read(reset=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                step(mode)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        prof = ctx.profile_read(reset=True)
+        ctx.profile(False)
+        if dist:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        results[name] = {"ms": ms, "prof": prof, "clocks": clk.summary()}
+
+    head = "split" if "split" in results else "plain"
+    r = results[head]
+    ms = r["ms"]
+    value = sites * world / (ms * 1e-3)
+    prof = r["prof"]
+    launches = sum(v[0] for v in prof.values())
+    tot_ms = sum(v[1] for v in prof.values()) or 1.0
+    kernels = {k: {"launches": v[0], "ms_per_step": v[1] / args.steps, "share": v[1] / tot_ms}
+               for k, v in prof.items()}
+    # roofline of the site-contraction kernel (HBM bound; the spec's figure is
+    # the 2 x 144 complex propagator entries per site)
+    ck = [k for k in prof if k.startswith("contract")]
+    roof = None
+    if ck:
+        kname = ck[0]
+        n, kms = prof[kname]
+        bytes_per_site = 2 * 144 * 16
+        ach = bytes_per_site * sites * args.steps / (kms * 1e-3) / 1e9
+        roof = {"kernel": kname, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": bytes_per_site * sites * args.steps / max(n, 1)}
+
+    # end to end through the C ABI with host buffers (pinned), copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        try:
+            import psutil
+            avail = psutil.virtual_memory().available
+        except Exception:
+            avail = 0
+        need = 2 * u.numel() * 16 + (8 << 30)
+        if avail > need:
+            hu = torch.empty(u.numel(), dtype=torch.complex128, pin_memory=True)
+            hd = torch.empty_like(hu)
+            hu.copy_(u)
+            hd.copy_(d)
+            del u, d
+            torch.cuda.empty_cache()
+            hout = np.zeros(total, dtype=np.complex128)
+            hprops = [ctx.prop(hu.data_ptr(), location=p2.P2_HOST, nt=L[3]),
+                      ctx.prop(hd.data_ptr(), location=p2.P2_HOST, nt=L[3])]
+
+            def estep():
+                ctx.contract_project(hprops, [ctx.request(src, L[3], what, hout.ctypes.data, p2.P2_HOST,
+                                                          mode=forms[head], q2max=Q2MAX)])
+            estep()
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            n_e = max(1, min(args.steps, 3))
+            for _ in range(n_e):
+                estep()
+            torch.cuda.synchronize()
+            el = (time.perf_counter() - t) / n_e
+            e2e = {"value": sites * world / el, "unit": "sites/s", "h2d_bytes_per_step": 2 * hu.numel() * 16,
+                   "d2h_bytes_per_step": total * 16, "steps": n_e, "timer": "host wall clock around the C-ABI call"}
+        else:
+            e2e = {"value": None, "unit": "sites/s", "note": f"host memory {avail >> 30} GiB < {need >> 30} GiB"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline_port(1)
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "error": str(ex)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "sites/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+f16x2" if head == "split" else "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "form": head, "L": list(L), "K": K, "nmom": nmom,
+                           "sites_per_step": sites, "l2": "inputs (49 GB) larger than L2",
+                           "parallelism": f"source-sharded x{world}"},
+                "forms": {k: {"ms_per_step": v["ms"], "sites_per_s": sites * world / (v["ms"] * 1e-3)}
+                          for k, v in results.items()},
+                "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": r["clocks"]}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -170,6 +170,28 @@ p2_status p2_contract_position(p2_ctx* ctx, const p2_prop* props, int nprops, co
 p2_status p2_ft_apply(p2_ctx* ctx, const double* field, int dof, int nt, const int* moms, int nmom, int sign,
                       double* out, int out_location);
 
+/* ---- memory ------------------------------------------------------------ */
+/* Field storage for callers that do not link the CUDA runtime themselves
+ * (PLEGMA_Field::create_device / create_host, lib/PLEGMA_Field.cu:226-235):
+ * P2_DEVICE allocates device memory on the context's device, P2_HOST pinned
+ * host memory.  p2_copy copies between any two of them and waits for it. */
+p2_status p2_alloc(p2_ctx* ctx, size_t bytes, int location, void** ptr);
+p2_status p2_free(p2_ctx* ctx, void* ptr, int location);
+p2_status p2_copy(p2_ctx* ctx, void* dst, const void* src, size_t bytes);
+
+/* ---- kernel timing ----------------------------------------------------- */
+/* When enabled, every kernel the library launches is bracketed by CUDA
+ * events on the launching stream; p2_profile_read() returns per-kernel
+ * launch counts and summed device time (it synchronises the events). */
+typedef struct {
+  char name[48];
+  long long launches;
+  double ms;
+} p2_kernel_time;
+p2_status p2_profile_enable(p2_ctx* ctx, int on);
+/* Fills up to max entries, returns the number of kernels seen; reset != 0 clears. */
+int p2_profile_read(p2_ctx* ctx, p2_kernel_time* out, int max, int reset);
+
 /* ---- synthetic inputs (benchmarks and tests) --------------------------- */
 /* Fill a propagator with entries Re, Im ~ N(0,1) scaled by exp(-a*|t - t0|),
  * drawn from a counter-based SplitMix64 + Box-Muller stream keyed by

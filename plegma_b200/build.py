@@ -69,5 +69,20 @@ def build(force=False, verbose=False, jobs=None):
     return LIB
 
 
+def build_cxx_driver(force=False):
+    """The C++ drop-in test driver (tests/cxx/calc_2pt.cpp) linked against the library."""
+    src = os.path.join(ROOT, "tests", "cxx", "calc_2pt.cpp")
+    out_dir = os.path.join(ROOT, "tests", "cxx", "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    exe = os.path.join(out_dir, "calc_2pt")
+    deps = [src, os.path.join(ROOT, "include", "plegma", "PLEGMA_2pt.h"), os.path.join(ROOT, "include", "plegma2pt.h"),
+            LIB]
+    if force or _stale(exe, deps):
+        subprocess.run(["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-o", exe, src,
+                        "-L" + LIBDIR, "-lplegma2pt", "-Wl,-rpath," + LIBDIR], check=True)
+    return exe
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build_cxx_driver(force="--force" in sys.argv))

@@ -223,7 +223,10 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request& r, const 
       a.K = pl.K;
       a.k = offsets_of(r.contractions);
       a.out = c->cbuf.p;
-      P2_TRY(c, p2::launch_contract_plain(a, c->nsm, c->stream), "contract kernel");
+      {
+        ProfScope ps(c, "contract_plain_fp64");
+        P2_TRY(c, p2::launch_contract_plain(a, c->nsm, c->stream), "contract kernel");
+      }
 
       p2::ProjArgs pa{};
       pa.c = c->cbuf.p;
@@ -244,7 +247,10 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request& r, const 
       pa.nsplit = (int)((c->V3 + pa.chunk - 1) / pa.chunk);
       P2_TRY(c, c->part.ensure((size_t)n * pa.nsplit * pl.nmom * pl.K * 16), "partials alloc");
       pa.part = (double*)c->part.p;
-      P2_TRY(c, p2::launch_project_fp64(pa, c->stream), "projection kernel");
+      {
+        ProfScope ps(c, "project_fp64");
+        P2_TRY(c, p2::launch_project_fp64(pa, c->stream), "projection kernel");
+      }
 
       p2::ScatterArgs sa{};
       sa.part = (const double*)c->part.p;
@@ -257,7 +263,10 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request& r, const 
       sa.nblocks = (int)pl.blocks.size();
       for (size_t b = 0; b < pl.blocks.size(); b++) sa.blk[b] = pl.blocks[b];
       sa.out = dres;
-      P2_TRY(c, p2::launch_scatter(sa, c->stream), "reduction kernel");
+      {
+        ProfScope ps(c, "reduce_scatter");
+        P2_TRY(c, p2::launch_scatter(sa, c->stream), "reduction kernel");
+      }
       if (u.location == P2_HOST || d.location == P2_HOST)
         P2_TRY(c, cudaStreamSynchronize(c->stream), "staging reuse");
     }
@@ -267,7 +276,91 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request& r, const 
 
 }  // namespace
 
+cudaEvent_t p2_ctx::prof_begin(const char* name, int& slot) {
+  slot = -1;
+  for (size_t i = 0; i < prof.size(); i++)
+    if (prof[i].name == name) slot = (int)i;
+  if (slot < 0) {
+    prof.emplace_back();
+    prof.back().name = name;
+    slot = (int)prof.size() - 1;
+  }
+  cudaEvent_t e = nullptr;
+  Prof& p = prof[slot];
+  if (!p.pool.empty()) {
+    e = p.pool.back();
+    p.pool.pop_back();
+  } else if (cudaEventCreate(&e) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  cudaEventRecord(e, stream);
+  return e;
+}
+
+void p2_ctx::prof_end(int slot, cudaEvent_t start) {
+  cudaEvent_t e = nullptr;
+  Prof& p = prof[slot];
+  if (!p.pool.empty()) {
+    e = p.pool.back();
+    p.pool.pop_back();
+  } else if (cudaEventCreate(&e) != cudaSuccess) {
+    cudaGetLastError();
+    p.pool.push_back(start);
+    return;
+  }
+  cudaEventRecord(e, stream);
+  p.pending.emplace_back(start, e);
+}
+
+void p2_ctx::prof_collect() {
+  for (Prof& p : prof) {
+    for (auto& ev : p.pending) {
+      cudaEventSynchronize(ev.second);
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, ev.first, ev.second) == cudaSuccess) {
+        p.ms += ms;
+        p.launches++;
+      }
+      cudaGetLastError();
+      p.pool.push_back(ev.first);
+      p.pool.push_back(ev.second);
+    }
+    p.pending.clear();
+  }
+}
+
+void p2_ctx::prof_clear() {
+  prof_collect();
+  for (Prof& p : prof) {
+    p.ms = 0;
+    p.launches = 0;
+  }
+}
+
 extern "C" {
+
+p2_status p2_profile_enable(p2_ctx* c, int on) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  c->profiling = on != 0;
+  return P2_OK;
+}
+
+int p2_profile_read(p2_ctx* c, p2_kernel_time* out, int max, int reset) {
+  if (!c) return -1;
+  c->prof_collect();
+  int n = 0;
+  for (const auto& p : c->prof) {
+    if (out && n < max) {
+      std::snprintf(out[n].name, sizeof(out[n].name), "%s", p.name.c_str());
+      out[n].launches = p.launches;
+      out[n].ms = p.ms;
+    }
+    n++;
+  }
+  if (reset) c->prof_clear();
+  return n;
+}
 
 p2_status p2_ctx_create(const p2_geom* g, p2_ctx** out) {
   if (!g || !out) return P2_ERR_INVALID_ARG;
@@ -293,6 +386,7 @@ p2_status p2_ctx_create(const p2_geom* g, p2_ctx** out) {
   }
   int nsm = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g->device) == cudaSuccess && nsm > 0) c->nsm = nsm;
+  cudaDeviceGetAttribute(&c->project_split_smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, g->device);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
     delete c;
@@ -315,6 +409,9 @@ p2_status p2_ctx_destroy(p2_ctx* c) {
   }
   cudaStreamSynchronize(c->stream);
   for (DevBuf* b : {&c->cbuf, &c->part, &c->tab, &c->res, &c->stage_u, &c->stage_d, &c->scratch}) b->release();
+  c->prof_collect();
+  for (auto& p : c->prof)
+    for (cudaEvent_t e : p.pool) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->stream);
   p2::precision_release(c);
   delete c;
@@ -326,7 +423,16 @@ const char* p2_last_error(const p2_ctx* c) { return c ? c->err.c_str() : "null c
 p2_status p2_sync(p2_ctx* c) {
   if (!c) return P2_ERR_INVALID_ARG;
   if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
-  return c->cuda(cudaStreamSynchronize(c->stream), "p2_sync");
+  P2_TRY(c, cudaStreamSynchronize(c->stream), "p2_sync");
+  if (c->errflag.p) {
+    int e = 0;
+    P2_TRY(c, cudaMemcpy(&e, c->errflag.p, sizeof(int), cudaMemcpyDeviceToHost), "error flag read");
+    if (e) {
+      cudaMemset(c->errflag.p, 0, sizeof(int));
+      return c->fail(P2_ERR_DEVICE_TIMEOUT, "a tensor-core pipeline wait gave up; results of the call are invalid");
+    }
+  }
+  return P2_OK;
 }
 
 p2_status p2_set_stream(p2_ctx* c, void* s) {
@@ -465,7 +571,10 @@ p2_status p2_contract_position(p2_ctx* c, const p2_prop* props, int nprops, cons
     } else {
       a.out = dst;
     }
-    P2_TRY(c, p2::launch_contract_plain(a, c->nsm, c->stream), "contract kernel");
+    {
+        ProfScope ps(c, "contract_plain_fp64");
+        P2_TRY(c, p2::launch_contract_plain(a, c->nsm, c->stream), "contract kernel");
+      }
     if (r->out_location == P2_HOST) {
       P2_TRY(c, cudaMemcpyAsync(dst, c->cbuf.p, slice * run.n * 16, cudaMemcpyDeviceToHost, c->stream),
              "position download");
@@ -510,7 +619,10 @@ p2_status p2_ft_apply(p2_ctx* c, const double* field, int dof, int nt, const int
   pa.nsplit = (int)((c->V3 + pa.chunk - 1) / pa.chunk);
   P2_TRY(c, c->part.ensure((size_t)nt * pa.nsplit * nmom * dof * 16), "partials alloc");
   pa.part = (double*)c->part.p;
-  P2_TRY(c, p2::launch_project_fp64(pa, c->stream), "projection kernel");
+  {
+        ProfScope ps(c, "project_fp64");
+        P2_TRY(c, p2::launch_project_fp64(pa, c->stream), "projection kernel");
+      }
   const size_t total = (size_t)nt * dof * nmom;
   double* dst = out;
   if (out_location == P2_HOST) {
@@ -529,12 +641,41 @@ p2_status p2_ft_apply(p2_ctx* c, const double* field, int dof, int nt, const int
   sa.oT = (long long)dof * nmom;
   sa.oK = nmom;
   sa.out = dst;
-  P2_TRY(c, p2::launch_scatter(sa, c->stream), "reduction kernel");
+  {
+        ProfScope ps(c, "reduce_scatter");
+        P2_TRY(c, p2::launch_scatter(sa, c->stream), "reduction kernel");
+      }
   if (out_location == P2_HOST) {
     P2_TRY(c, cudaMemcpyAsync(out, dst, total * 16, cudaMemcpyDeviceToHost, c->stream), "result download");
     P2_TRY(c, cudaStreamSynchronize(c->stream), "result download");
   }
   return P2_OK;
+}
+
+p2_status p2_alloc(p2_ctx* c, size_t bytes, int location, void** ptr) {
+  if (!c || !ptr || bytes == 0) return c ? c->fail(P2_ERR_INVALID_ARG, "p2_alloc: bad arguments") : P2_ERR_INVALID_ARG;
+  *ptr = nullptr;
+  if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
+  if (location == P2_DEVICE) return c->cuda(cudaMalloc(ptr, bytes), "p2_alloc device");
+  if (location == P2_HOST) return c->cuda(cudaMallocHost(ptr, bytes), "p2_alloc host");
+  return c->fail(P2_ERR_INVALID_ARG, "p2_alloc: bad location");
+}
+
+p2_status p2_free(p2_ctx* c, void* ptr, int location) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  if (!ptr) return P2_OK;
+  if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
+  if (location == P2_DEVICE) return c->cuda(cudaFree(ptr), "p2_free device");
+  if (location == P2_HOST) return c->cuda(cudaFreeHost(ptr), "p2_free host");
+  return c->fail(P2_ERR_INVALID_ARG, "p2_free: bad location");
+}
+
+p2_status p2_copy(p2_ctx* c, void* dst, const void* src, size_t bytes) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  if (!dst || !src) return c->fail(P2_ERR_INVALID_ARG, "p2_copy: null pointer");
+  if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
+  P2_TRY(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c->stream), "p2_copy");
+  return c->cuda(cudaStreamSynchronize(c->stream), "p2_copy");
 }
 
 p2_status p2_synth_propagator(p2_ctx* c, void* dst, int on_device, int precision, uint64_t seed, int flavour, int t0,

@@ -1,0 +1,316 @@
+// Site contraction kernels: propagators staged through shared memory, one
+// site per half-warp, results written to a position-space buffer that the
+// projection kernels consume.
+//
+// Replaces the per-site part of contract_baryons_device / contract_NtoN_kernel
+// (lib/kernels/PLEGMA_baryons.cuh:82-147, PLEGMA_baryons_NtoN.cu:6-46) and
+// contract_mesons_{all,new,}_device (PLEGMA_mesonsAll.cuh:7-95,
+// PLEGMA_mesonsNew.cuh:5-56, PLEGMA_mesons.cuh:10-65).
+//
+// Two instantiations:
+//  - plain:  FP64 propagators, FP64 arithmetic, complex-double output;
+//  - split:  FP64 or FP32 propagators multiplied by 2^-E(slice, flavour)
+//            (exact power-of-two scaling, so correlators that fall over ten
+//            decades in t stay inside FP32's range), FP32 arithmetic,
+//            complex-float output, plus max(|Re|,|Im|) per (slice, component)
+//            for the FP16 split of the projection.
+//
+// Layout and schedule
+//  - a CTA of 256 threads is persistent over tiles of 16 consecutive sites of
+//    one time slice (tile = (tau, x0));
+//  - each tile's 2 x 144 complex per site are copied with cp.async, coalesced
+//    along the site axis of the SoA propagator, into shared memory as
+//    [site][flavour*144 + component] (row padded to 289 complex);
+//  - two stages: tile i+1's copies are in flight while tile i is contracted;
+//  - half-warp h contracts site h of the tile (site_contract.cuh).
+#include "kernels.cuh"
+#include "site_contract.cuh"
+
+namespace p2 {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kSitesPerTile = 16;
+constexpr int kRow = 289;  // complex per site row (2 * 144 + 1 pad)
+constexpr int kStage = kSitesPerTile * kRow;
+
+template <typename Tin>
+__device__ __forceinline__ void issue_tile(const ContractArgs& a, Cx<Tin>* st, long long tile, long long ntiles,
+                                           int tiles_per_tau) {
+  if (tile < ntiles) {
+    const int tl = (int)(tile / tiles_per_tau);
+    const int x0 = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile;
+    const int t = (a.t0 + a.tau0 + tl) % a.T;
+    const long long ju = (long long)((t - a.t_first_u + a.T) % a.T) * a.V3;
+    const long long jd = (long long)((t - a.t_first_d + a.T) % a.T) * a.V3;
+    const Cx<Tin>* U = (const Cx<Tin>*)a.u;
+    const Cx<Tin>* D = (const Cx<Tin>*)a.d;
+#pragma unroll 2
+    for (int r = 0; r < (2 * 144 * kSitesPerTile) / kThreads; r++) {
+      const int i = threadIdx.x + r * kThreads;
+      const int s = i & (kSitesPerTile - 1);
+      const int rest = i >> 4;
+      const int f = rest >= 144;
+      const int comp = rest - 144 * f;
+      const int x = x0 + s;
+      const bool ok = x < a.V3;
+      const Cx<Tin>* src = f ? D + (long long)comp * a.vol_d + jd + (ok ? x : 0)
+                             : U + (long long)comp * a.vol_u + ju + (ok ? x : 0);
+      if (sizeof(Tin) == 8)
+        cp_async16(st + s * kRow + rest, src, ok ? 16 : 0);
+      else
+        cp_async8(st + s * kRow + rest, src, ok ? 8 : 0);
+    }
+  }
+  cp_async_commit();
+}
+
+// Index of a diagonal structure in the 10-structure list (1, g5, g1..g4,
+// g5g1..g5g4) of contractMesons / contractMesonsNew, or -1.
+__device__ __forceinline__ int diag10_slot(int g) {
+  return g == 0 ? 0 : g == 5 ? 1 : (g >= 1 && g <= 4) ? g + 1 : (g >= 6 && g <= 9) ? g : -1;
+}
+
+template <typename R>
+struct Writer {
+  Cx<R>* out;
+  long long V3;
+  int* smax;  // split form: per-component running max (float bits), or null
+  __device__ __forceinline__ void put(int k, Cx<R> v) const {
+    out[(long long)k * V3] = v;
+    if (smax) {
+      const float m = fmaxf(fabsf((float)v.x), fabsf((float)v.y));
+      atomicMax(smax + k, __float_as_int(m));
+    }
+  }
+};
+
+template <typename R>
+__device__ __forceinline__ void contract_site(const ContractArgs& a, const Cx<R>* U, const Cx<R>* D,
+                                              const LaneTables& lt, int l, unsigned mask, const Writer<R>& w) {
+  if (a.what & 1u) {
+    const Cx<R> p = nucleon_site<R>(U, D, lt, l, mask);
+    const Cx<R> n = nucleon_site<R>(D, U, lt, l, mask);
+    w.put(a.k.nuc + l, p);
+    w.put(a.k.nuc + 16 + l, n);
+  }
+  if (a.what & (8u | 16u | 32u)) {
+    Cx<R> c[16];
+    meson_site<R>(U, D, lt, l, mask, c);
+    if (a.what & 8u) {
+#pragma unroll
+      for (int g2 = 0; g2 < 16; g2++) w.put(a.k.g16 + l * 16 + g2, c[g2]);
+    }
+    if (a.what & 16u) {
+      if (l == 0) w.put(a.k.all34 + 0, c[0]);
+      if (l == 5) w.put(a.k.all34 + 1, c[5]);
+      if (l >= 1 && l <= 4) {
+#pragma unroll
+        for (int g2 = 1; g2 <= 4; g2++) w.put(a.k.all34 + 2 + (l - 1) * 4 + (g2 - 1), c[g2]);
+      }
+      if (l >= 6 && l <= 9) {
+#pragma unroll
+        for (int g2 = 6; g2 <= 9; g2++) w.put(a.k.all34 + 18 + (l - 6) * 4 + (g2 - 6), c[g2]);
+      }
+    }
+    if (a.what & 32u) {
+      const int j = diag10_slot(l);
+#pragma unroll
+      for (int g2 = 0; g2 < 16; g2++)
+        if (g2 == l && j >= 0) w.put(a.k.new10 + j, c[g2]);
+    }
+  }
+  if (a.what & 64u) {
+    const int j = diag10_slot(l);
+    Cx<R> c[16];
+    meson_site<R>(U, U, lt, l, mask, c);
+#pragma unroll
+    for (int g2 = 0; g2 < 16; g2++)
+      if (g2 == l && j >= 0) w.put(a.k.diag10 + j, c[g2]);
+    meson_site<R>(D, D, lt, l, mask, c);
+#pragma unroll
+    for (int g2 = 0; g2 < 16; g2++)
+      if (g2 == l && j >= 0) w.put(a.k.diag10 + 10 + j, c[g2]);
+  }
+}
+
+// Plain FP64 form.
+__global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<double>* sm = (Cx<double>*)smem_raw;
+  const int tid = threadIdx.x;
+  const int hw = tid >> 4, l = tid & 15;
+  const unsigned mask = halfwarp_mask();
+  const LaneTables lt = load_lane_tables(l);
+
+  const int tiles_per_tau = (a.V3 + kSitesPerTile - 1) / kSitesPerTile;
+  const long long ntiles = (long long)a.ntau * tiles_per_tau;
+  long long tile = blockIdx.x;
+
+  issue_tile<double>(a, sm, tile, ntiles, tiles_per_tau);
+  issue_tile<double>(a, sm + kStage, tile + gridDim.x, ntiles, tiles_per_tau);
+
+  for (int it = 0; tile < ntiles; tile += gridDim.x, it++) {
+    Cx<double>* st = sm + (it & 1) * kStage;
+    cp_async_wait<1>();
+    __syncthreads();
+    const int tl = (int)(tile / tiles_per_tau);
+    const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + hw;
+    if (x < a.V3) {
+      const Cx<double>* U = st + hw * kRow;
+      Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr};
+      contract_site<double>(a, U, U + 144, lt, l, mask, w);
+    }
+    __syncthreads();
+    issue_tile<double>(a, st, tile + 2LL * gridDim.x, ntiles, tiles_per_tau);
+  }
+  cp_async_wait<0>();
+}
+
+// Split form: FP32 arithmetic on power-of-two scaled inputs.
+template <typename Tin>
+__global__ void __launch_bounds__(kThreads, 1) k_contract_f32(const ContractArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<Tin>* sm = (Cx<Tin>*)smem_raw;
+  Cx<float>* sf = (Cx<float>*)(smem_raw + 2 * kStage * sizeof(Cx<Tin>));
+  int* smax = (int*)(sf + kStage);
+  const int tid = threadIdx.x;
+  const int hw = tid >> 4, l = tid & 15;
+  const unsigned mask = halfwarp_mask();
+  const LaneTables lt = load_lane_tables(l);
+
+  const int tiles_per_tau = (a.V3 + kSitesPerTile - 1) / kSitesPerTile;
+  const long long ntiles = (long long)a.ntau * tiles_per_tau;
+  long long tile = blockIdx.x;
+  for (int k = tid; k < a.K; k += kThreads) smax[k] = 0;
+
+  issue_tile<Tin>(a, sm, tile, ntiles, tiles_per_tau);
+  issue_tile<Tin>(a, sm + kStage, tile + gridDim.x, ntiles, tiles_per_tau);
+
+  int cur = -1;  // slice whose maxima smax holds
+  for (int it = 0; tile < ntiles; tile += gridDim.x, it++) {
+    Cx<Tin>* st = sm + (it & 1) * kStage;
+    const int tl = (int)(tile / tiles_per_tau);
+    cp_async_wait<1>();
+    __syncthreads();
+    if (tl != cur) {
+      if (cur >= 0)
+        for (int k = tid; k < a.K; k += kThreads) {
+          atomicMax(a.cmax + (long long)cur * a.K + k, smax[k]);
+          smax[k] = 0;
+        }
+      cur = tl;
+    }
+    // scale by 2^-E per flavour and convert to FP32 once per tile
+    {
+      const int eu = a.exp_u[tl], ed = a.exp_d[tl];
+      for (int i = tid; i < kSitesPerTile * 288; i += kThreads) {
+        const int s = i / 288, c = i - s * 288;
+        const Cx<Tin> v = st[s * kRow + c];
+        const int e = c < 144 ? eu : ed;
+        Cx<float> f;
+        if (sizeof(Tin) == 8) {
+          f.x = (float)scalbn((double)v.x, -e);
+          f.y = (float)scalbn((double)v.y, -e);
+        } else {
+          f.x = scalbnf((float)v.x, -e);
+          f.y = scalbnf((float)v.y, -e);
+        }
+        sf[s * kRow + c] = f;
+      }
+    }
+    __syncthreads();
+    // the staged tile has been converted: refill this stage while contracting
+    issue_tile<Tin>(a, st, tile + 2LL * gridDim.x, ntiles, tiles_per_tau);
+    const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + hw;
+    if (x < a.V3) {
+      const Cx<float>* U = sf + hw * kRow;
+      Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, smax};
+      contract_site<float>(a, U, U + 144, lt, l, mask, w);
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  if (cur >= 0)
+    for (int k = tid; k < a.K; k += kThreads) atomicMax(a.cmax + (long long)cur * a.K + k, smax[k]);
+}
+
+// Per-slice exponent E with max(|Re|,|Im|) < 2^E over a strided sample of
+// sites and components (every 7th component, every 97th site), so that the
+// scaled entries are O(1) in FP32.  Only the binary exponents are compared,
+// so FP64 entries far below FP32's range are handled exactly.
+__global__ void k_sample_exponents(const SampleArgs a) {
+  __shared__ int red[256];
+  const int tl = blockIdx.x;
+  const int t = (a.t0 + a.tau0 + tl) % a.T;
+  const long long j = (long long)((t - a.t_first + a.T) % a.T) * a.V3;
+  int emax = -100000;
+  for (int i = threadIdx.x; i < 21 * 1024; i += blockDim.x) {
+    const int comp = (i % 21) * 7;
+    const long long x = ((long long)(i / 21) * 97) % a.V3;
+    const long long idx = (long long)comp * a.vol + j + x;
+    double re, im;
+    if (a.fp32) {
+      const float2 v = ((const float2*)a.p)[idx];
+      re = v.x;
+      im = v.y;
+    } else {
+      const double2 v = ((const double2*)a.p)[idx];
+      re = v.x;
+      im = v.y;
+    }
+    int e;
+    if (re != 0.0) {
+      frexp(re, &e);
+      emax = max(emax, e);
+    }
+    if (im != 0.0) {
+      frexp(im, &e);
+      emax = max(emax, e);
+    }
+  }
+  red[threadIdx.x] = emax;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = max(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) a.exp_out[tl] = red[0] == -100000 ? 0 : red[0];
+}
+
+}  // namespace
+
+int contract_plain_smem_bytes() { return 2 * kStage * (int)sizeof(Cx<double>); }
+
+cudaError_t launch_contract_plain(const ContractArgs& a, int grid, cudaStream_t s) {
+  const int smem = contract_plain_smem_bytes();
+  cudaError_t e = cudaFuncSetAttribute(k_contract_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  k_contract_plain<<<grid, kThreads, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_contract_f32(const ContractArgs& a, int fp32_in, int grid, cudaStream_t s) {
+  const int tin = fp32_in ? (int)sizeof(Cx<float>) : (int)sizeof(Cx<double>);
+  const int smem = 2 * kStage * tin + kStage * (int)sizeof(Cx<float>) + a.K * (int)sizeof(int);
+  cudaError_t e;
+  if (fp32_in) {
+    e = cudaFuncSetAttribute(k_contract_f32<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    k_contract_f32<float><<<grid, kThreads, smem, s>>>(a);
+  } else {
+    e = cudaFuncSetAttribute(k_contract_f32<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    k_contract_f32<double><<<grid, kThreads, smem, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sample_exponents(const SampleArgs& a, cudaStream_t s) {
+  k_sample_exponents<<<a.ntau, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace p2

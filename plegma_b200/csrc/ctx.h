@@ -52,7 +52,25 @@ struct p2_ctx {
   bool host_only = false;  // created with device < 0
   std::string err = "no error";
   p2host::DevBuf cbuf, part, tab, res, stage_u, stage_d, scratch;
+  // split form: phase tiles, per-slice exponents, component maxima, tables, partials, error flag
+  p2host::DevBuf phaseA, expb, cmaxb, momrow, kexp, fpart, rowtab, errflag;
+  int project_split_smem_max = 0;  // opt-in shared memory per block of the device
   size_t ws_budget = 0;
+
+  // kernel timing (p2_profile_enable)
+  struct Prof {
+    std::string name;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    std::vector<cudaEvent_t> pool;
+    double ms = 0;
+    long long launches = 0;
+  };
+  bool profiling = false;
+  std::vector<Prof> prof;
+  cudaEvent_t prof_begin(const char* name, int& slot);
+  void prof_end(int slot, cudaEvent_t start);
+  void prof_collect();
+  void prof_clear();
 
   p2_status fail(p2_status s, const std::string& m) {
     err = m;
@@ -63,6 +81,19 @@ struct p2_ctx {
     cudaGetLastError();
     err = std::string(where) + ": " + cudaGetErrorString(e);
     return e == cudaErrorMemoryAllocation ? P2_ERR_OOM : P2_ERR_CUDA;
+  }
+};
+
+// Brackets one kernel launch with events when profiling is on.
+struct ProfScope {
+  p2_ctx* c;
+  int slot = -1;
+  cudaEvent_t start = nullptr;
+  ProfScope(p2_ctx* ctx, const char* name) : c(ctx) {
+    if (c->profiling) start = c->prof_begin(name, slot);
+  }
+  ~ProfScope() {
+    if (start) c->prof_end(slot, start);
   }
 };
 

@@ -24,7 +24,21 @@ struct ContractArgs {
   unsigned what;
   int K;
   CompOffsets k;
-  void* out;  // [ntau][K][V3] complex (double for the plain form)
+  void* out;  // [ntau][K][V3] complex (double for the plain form, float for the split form)
+  // split form only: power-of-two scale exponents per chunk slice (input x 2^-E),
+  // and the running max |Re|,|Im| per (slice, component) as float bits
+  const int* exp_u;
+  const int* exp_d;
+  int* cmax;  // [ntau][K]
+};
+
+// Per-slice magnitude exponents of a propagator view, from a strided sample.
+struct SampleArgs {
+  const void* p;
+  int fp32;
+  long long vol;
+  int t_first, V3, T, t0, tau0, ntau;
+  int* exp_out;  // [ntau]
 };
 
 struct ProjArgs {
@@ -54,7 +68,54 @@ struct ScatterArgs {
   double* out;
 };
 
+// ---- split-FP16 projection ------------------------------------------------
+// Phase rows: for every representative momentum h of a +-h pair, a cos row and
+// (h != 0) a sin row; cos(h.(x-x0)) and sin(h.(x-x0)) over the sites, stored
+// as hi+lo FP16 tiles of 128 rows x 64 sites in the tensor core's 128-byte
+// swizzled K-major layout: A[mtile][kstep][hi, lo][128 x 64].
+struct PhaseBuildArgs {
+  const double* tab;  // [3][nh][Lmax] complex, exp(-i 2 pi h_d (x_d - x0_d) / L_d)
+  const int* row_h;   // [nrows] representative of each row
+  const int* row_sin; // [nrows] 0 = cos row, 1 = sin row
+  int nrows, nmtile, nkstep, V3, Lx, Ly, Lmax, nh;
+  void* A;
+};
+
+struct SplitGemmArgs {
+  const void* c;     // complex float [ntau][K][V3]
+  const int* cmax;   // [ntau][K] max(|Re|,|Im|) as float bits
+  const void* A;     // phase tiles
+  int ntau, K, V3, nkstep, nmtile;
+  int NT, ntile;     // components per N-tile (multiple of 16, <= 144), N-tiles
+  int ks_per_split, nsplit;
+  float* part;       // [ntau][nsplit][nmtile][128][ntile * 2 * NT]
+  int* err;          // set to 1 if a bounded wait gave up
+};
+
+struct SplitReduceArgs {
+  const float* part;
+  int ntau, nsplit, nmtile, ncols, NT;
+  int nmom, K;
+  const int* mom_row;  // [nmom][3]: cos row, sin row (-1 for h = 0), sign (+1: p = h, -1: p = -h)
+  const int* cmax;     // [ntau][K]
+  const int* exp_u;    // [ntau]
+  const int* exp_d;    // [ntau]
+  const int* kexp;     // [K][2]: powers of the u and d scales in component k
+  int tau0, totalT;
+  int nblocks;
+  ScatterBlock blk[kMaxBlocks];
+  double* out;
+};
+
+cudaError_t launch_build_phases(const PhaseBuildArgs& a, cudaStream_t s);
+cudaError_t launch_project_split(const SplitGemmArgs& a, cudaStream_t s);
+cudaError_t launch_split_reduce(const SplitReduceArgs& a, cudaStream_t s);
+int project_split_smem_bytes(int NT);
+
 cudaError_t launch_contract_plain(const ContractArgs& a, int grid, cudaStream_t s);
+// FP32 site contraction; fp32_in selects complex-float propagators.
+cudaError_t launch_contract_f32(const ContractArgs& a, int fp32_in, int grid, cudaStream_t s);
+cudaError_t launch_sample_exponents(const SampleArgs& a, cudaStream_t s);
 cudaError_t launch_project_fp64(const ProjArgs& a, cudaStream_t s);
 cudaError_t launch_scatter(const ScatterArgs& a, cudaStream_t s);
 cudaError_t launch_synth(void* dst, int fp32, uint64_t seed, int flavour, int t0, double decay, int t_first, int nt,

@@ -1,11 +1,286 @@
-// Split-FP16 form (filled in by the tensor-core projection).
+// Split-FP16 form: orchestration of the FP32 site contraction and the
+// tensor-core projection (project_split.cu) for one or more requests.
+//
+// Per chunk of time slices:
+//   1. per-slice exponents E_u, E_d from a strided sample of each propagator;
+//   2. FP32 contraction of the inputs scaled by 2^-E, plus max |c_k| per slice;
+//   3. hi+lo FP16 projection GEMM on tcgen05 with FP32 accumulation in TMEM;
+//   4. FP64 reduction over site splits, pair recombination
+//        C(+-h) = (Cc_re +- Cs_im) + i (Cc_im -+ Cs_re),
+//      and exact un-scaling by 2^(n_u E_u + n_d E_d - s_k).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "ctx.h"
+
+using namespace p2host;
+
+namespace {
+
+// powers (n_u, n_d) of the flavour scales carried by each component
+std::vector<int> component_exponents(unsigned what) {
+  std::vector<int> e;
+  auto push = [&](int n, int nu, int nd) {
+    for (int i = 0; i < n; i++) {
+      e.push_back(nu);
+      e.push_back(nd);
+    }
+  };
+  if (what & P2_NUCLEON_CG5) {
+    push(16, 2, 1);  // proton: u u d
+    push(16, 1, 2);  // neutron: d d u
+  }
+  if (what & P2_DELTA_ISO12)
+    for (int g = 0; g < 3; g++) {
+      push(16, 2, 1);
+      push(16, 1, 2);
+    }
+  if (what & P2_DELTA_ISO32)
+    for (int g = 0; g < 3; g++) {
+      push(16, 3, 0);
+      push(16, 0, 3);
+    }
+  if (what & P2_MESON_G16) push(256, 1, 1);
+  if (what & P2_MESON_ALL34) push(34, 1, 1);
+  if (what & P2_MESON_NEW10) push(10, 1, 1);
+  if (what & P2_MESON_DIAG10) {
+    push(10, 2, 0);
+    push(10, 0, 2);
+  }
+  return e;
+}
+
+struct PhaseRows {
+  std::vector<int> reps;     // unique representatives, 3 ints each
+  std::vector<int> row_h;    // per row: representative index
+  std::vector<int> row_sin;  // per row: 0 cos, 1 sin
+  std::vector<int> mom_row;  // per momentum: cos row, sin row, sign
+};
+
+PhaseRows phase_rows(const std::vector<int>& moms) {
+  PhaseRows pr;
+  const int n = (int)moms.size() / 3;
+  std::vector<int> cos_row, sin_row;
+  for (int p = 0; p < n; p++) {
+    int v[3] = {moms[3 * p], moms[3 * p + 1], moms[3 * p + 2]};
+    int sg = 1;
+    for (int d = 0; d < 3; d++)
+      if (v[d] != 0) {
+        sg = v[d] > 0 ? 1 : -1;
+        break;
+      }
+    int h[3] = {sg * v[0], sg * v[1], sg * v[2]};
+    int idx = -1;
+    for (size_t q = 0; q < pr.reps.size() / 3; q++)
+      if (pr.reps[3 * q] == h[0] && pr.reps[3 * q + 1] == h[1] && pr.reps[3 * q + 2] == h[2]) idx = (int)q;
+    if (idx < 0) {
+      idx = (int)pr.reps.size() / 3;
+      pr.reps.insert(pr.reps.end(), h, h + 3);
+      cos_row.push_back((int)pr.row_h.size());
+      pr.row_h.push_back(idx);
+      pr.row_sin.push_back(0);
+      if (h[0] || h[1] || h[2]) {
+        sin_row.push_back((int)pr.row_h.size());
+        pr.row_h.push_back(idx);
+        pr.row_sin.push_back(1);
+      } else {
+        sin_row.push_back(-1);
+      }
+    }
+    pr.mom_row.push_back(cos_row[idx]);
+    pr.mom_row.push_back(sin_row[idx]);
+    pr.mom_row.push_back(sg);
+  }
+  return pr;
+}
+
+template <typename T>
+p2_status upload(p2_ctx* c, DevBuf& b, const std::vector<T>& v, const char* what) {
+  P2_TRY(c, b.ensure(std::max<size_t>(v.size() * sizeof(T), 16)), what);
+  P2_TRY(c, cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream), what);
+  return P2_OK;
+}
+
+p2_status run_one(p2_ctx* c, const p2_prop* props, const p2_request& r) {
+  Plan pl;
+  p2_status st = make_plan(c, r, pl);
+  if (st != P2_OK) return st;
+  const p2_prop& u = props[r.prop_u];
+  const p2_prop& d = props[r.prop_d];
+  if (u.precision != d.precision) return c->fail(P2_ERR_UNSUPPORTED, "u and d must share a precision");
+  if (r.contractions & (P2_DELTA_ISO12 | P2_DELTA_ISO32))
+    return c->fail(P2_ERR_UNSUPPORTED, "Delta contractions are not available in the split form yet");
+  const int fp32_in = u.precision == P2_FP32;
+  const int K = pl.K;
+
+  // phase rows of the +-p pairs and their hi/lo FP16 tiles
+  PhaseRows pr = phase_rows(pl.moms);
+  const int nh = (int)pr.reps.size() / 3;
+  const int nrows = (int)pr.row_h.size();
+  const int nmtile = (nrows + 127) / 128;
+  const int nkstep = (int)((c->V3 + 63) / 64);
+  std::vector<double> tabh = phase_tables(c, pr.reps.data(), nh, r.source, -1, pl.Lmax);
+  if ((st = upload(c, c->tab, tabh, "phase table")) != P2_OK) return st;
+  std::vector<int> rows(pr.row_h);
+  rows.insert(rows.end(), pr.row_sin.begin(), pr.row_sin.end());
+  if ((st = upload(c, c->rowtab, rows, "phase rows")) != P2_OK) return st;
+  P2_TRY(c, c->phaseA.ensure((size_t)nmtile * nkstep * 2 * 128 * 64 * 2), "phase tiles alloc");
+  {
+    p2::PhaseBuildArgs b{};
+    b.tab = (const double*)c->tab.p;
+    b.row_h = (const int*)c->rowtab.p;
+    b.row_sin = (const int*)c->rowtab.p + nrows;
+    b.nrows = nrows;
+    b.nmtile = nmtile;
+    b.nkstep = nkstep;
+    b.V3 = (int)c->V3;
+    b.Lx = c->Ll[0];
+    b.Ly = c->Ll[1];
+    b.Lmax = pl.Lmax;
+    b.nh = nh;
+    b.A = c->phaseA.p;
+    ProfScope ps(c, "build_phase_tiles");
+    P2_TRY(c, p2::launch_build_phases(b, c->stream), "phase tiles");
+  }
+  if ((st = upload(c, c->momrow, pr.mom_row, "momentum rows")) != P2_OK) return st;
+  if ((st = upload(c, c->kexp, component_exponents(r.contractions), "component exponents")) != P2_OK) return st;
+
+  double* dres = r.out;
+  if (r.out_location == P2_HOST) {
+    P2_TRY(c, c->res.ensure(pl.total * 16), "result alloc");
+    P2_TRY(c, cudaMemsetAsync(c->res.p, 0, pl.total * 16, c->stream), "result clear");
+    dres = (double*)c->res.p;
+  }
+
+  // N tiling: at most 144 components (288 TMEM columns) per CTA
+  const int ntile = (K + 143) / 144;
+  const int NT = ((K + ntile - 1) / ntile + 15) / 16 * 16;
+  // chunk of slices: FP32 position buffer within the workspace budget
+  const size_t per_slice = (size_t)K * c->V3 * 8;
+  const int tc = (int)std::max<size_t>(1, std::min<size_t>(c->ws_budget / std::max<size_t>(per_slice, 1), c->T));
+  P2_TRY(c, c->cbuf.ensure((size_t)tc * per_slice), "position buffer alloc");
+  P2_TRY(c, c->expb.ensure((size_t)2 * tc * sizeof(int)), "exponent alloc");
+  P2_TRY(c, c->cmaxb.ensure((size_t)tc * K * sizeof(int)), "maxima alloc");
+
+  for (const TauRun& run : local_runs(c, u, d, r.source, r.totalT)) {
+    for (int off = 0; off < run.n; off += tc) {
+      const int n = std::min(tc, run.n - off);
+      const int tau0 = run.tau0 + off;
+      const int t_begin = (r.source[3] + tau0) % c->T;
+      p2::ContractArgs a{};
+      if ((st = chunk_view(c, u, c->stage_u, t_begin, n, a, true)) != P2_OK) return st;
+      if ((st = chunk_view(c, d, c->stage_d, t_begin, n, a, false)) != P2_OK) return st;
+      int* eu = (int*)c->expb.p;
+      int* ed = eu + tc;
+      {
+        ProfScope ps(c, "sample_exponents");
+        p2::SampleArgs sa{a.u, fp32_in, a.vol_u, a.t_first_u, (int)c->V3, c->T, r.source[3], tau0, n, eu};
+        P2_TRY(c, p2::launch_sample_exponents(sa, c->stream), "exponent sample");
+        p2::SampleArgs sd{a.d, fp32_in, a.vol_d, a.t_first_d, (int)c->V3, c->T, r.source[3], tau0, n, ed};
+        P2_TRY(c, p2::launch_sample_exponents(sd, c->stream), "exponent sample");
+      }
+      P2_TRY(c, cudaMemsetAsync(c->cmaxb.p, 0, (size_t)n * K * sizeof(int), c->stream), "maxima clear");
+      a.V3 = (int)c->V3;
+      a.T = c->T;
+      a.t0 = r.source[3];
+      a.tau0 = tau0;
+      a.ntau = n;
+      a.what = r.contractions;
+      a.K = K;
+      a.k = offsets_of(r.contractions);
+      a.out = c->cbuf.p;
+      a.exp_u = eu;
+      a.exp_d = ed;
+      a.cmax = (int*)c->cmaxb.p;
+      {
+        ProfScope ps(c, "contract_f32");
+        P2_TRY(c, p2::launch_contract_f32(a, fp32_in, c->nsm, c->stream), "contract kernel");
+      }
+      // projection GEMM: enough CTAs for about two waves
+      const int per = ntile * nmtile * n;
+      int nsplit = std::max(1, (2 * c->nsm + per - 1) / per);
+      nsplit = std::min(nsplit, nkstep);
+      const int ks_per = (nkstep + nsplit - 1) / nsplit;
+      nsplit = (nkstep + ks_per - 1) / ks_per;
+      const int ncols = ntile * 2 * NT;
+      P2_TRY(c, c->fpart.ensure((size_t)n * nsplit * nmtile * 128 * ncols * sizeof(float)), "partials alloc");
+      p2::SplitGemmArgs g{};
+      g.c = c->cbuf.p;
+      g.cmax = (const int*)c->cmaxb.p;
+      g.A = c->phaseA.p;
+      g.ntau = n;
+      g.K = K;
+      g.V3 = (int)c->V3;
+      g.nkstep = nkstep;
+      g.nmtile = nmtile;
+      g.NT = NT;
+      g.ntile = ntile;
+      g.ks_per_split = ks_per;
+      g.nsplit = nsplit;
+      g.part = (float*)c->fpart.p;
+      g.err = (int*)c->errflag.p;
+      {
+        ProfScope ps(c, "project_split_tc");
+        P2_TRY(c, p2::launch_project_split(g, c->stream), "tensor-core projection");
+      }
+      p2::SplitReduceArgs rd{};
+      rd.part = (const float*)c->fpart.p;
+      rd.ntau = n;
+      rd.nsplit = nsplit;
+      rd.nmtile = nmtile;
+      rd.ncols = ncols;
+      rd.NT = NT;
+      rd.nmom = pl.nmom;
+      rd.K = K;
+      rd.mom_row = (const int*)c->momrow.p;
+      rd.cmax = (const int*)c->cmaxb.p;
+      rd.exp_u = eu;
+      rd.exp_d = ed;
+      rd.kexp = (const int*)c->kexp.p;
+      rd.tau0 = tau0;
+      rd.totalT = r.totalT;
+      rd.nblocks = (int)pl.blocks.size();
+      for (size_t b = 0; b < pl.blocks.size(); b++) rd.blk[b] = pl.blocks[b];
+      rd.out = dres;
+      {
+        ProfScope ps(c, "split_reduce");
+        P2_TRY(c, p2::launch_split_reduce(rd, c->stream), "split reduction");
+      }
+      if (u.location == P2_HOST || d.location == P2_HOST)
+        P2_TRY(c, cudaStreamSynchronize(c->stream), "staging reuse");
+    }
+  }
+  if (r.out_location == P2_HOST) {
+    P2_TRY(c, cudaMemcpyAsync(r.out, dres, pl.total * 16, cudaMemcpyDeviceToHost, c->stream), "result download");
+    P2_TRY(c, cudaStreamSynchronize(c->stream), "result download");
+  }
+  return P2_OK;
+}
+
+}  // namespace
 
 namespace p2 {
 
-p2_status precision_run_batch(p2_ctx* c, const p2_prop*, int, const p2_request*, int) {
-  return c->fail(P2_ERR_UNSUPPORTED, "split-FP16 form not built");
+p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, int nprops, const p2_request* reqs, int nreq) {
+  (void)nprops;
+  if (!c->errflag.p) {
+    P2_TRY(c, c->errflag.ensure(16), "error flag alloc");
+    P2_TRY(c, cudaMemsetAsync(c->errflag.p, 0, 16, c->stream), "error flag clear");
+  }
+  if (c->project_split_smem_max < p2::project_split_smem_bytes(144))
+    return c->fail(P2_ERR_UNSUPPORTED, "device shared memory per block too small for the tensor-core projection");
+  for (int i = 0; i < nreq; i++) {
+    p2_status s = run_one(c, props, reqs[i]);
+    if (s != P2_OK) return s;
+  }
+  return P2_OK;
 }
-void precision_release(p2_ctx*) {}
+
+void precision_release(p2_ctx* c) {
+  for (DevBuf* b : {&c->phaseA, &c->expb, &c->cmaxb, &c->momrow, &c->kexp, &c->fpart, &c->rowtab, &c->errflag})
+    b->release();
+}
 
 }  // namespace p2

@@ -1,0 +1,320 @@
+// Split-FP16 momentum projection on the tcgen05 tensor cores.
+//
+// Per time slice the projection C(t,p,k) = sum_x c_k(x,t) exp(-i p.(x-x0))
+// is a dense [nmom x V3] . [V3 x K] product (the reference computes it per
+// site and momentum with cos/sin and a shared-memory tree,
+// lib/kernels/PLEGMA_kernel_utils.cuh:820-860).  Here it runs as a real GEMM
+//
+//   D[row][n] = sum_x A[row][x] B[n][x]
+//   rows: cos(h.(x-x0)) and sin(h.(x-x0)) for one representative h of every
+//         +-p pair (123 momenta -> 123 rows, one M=128 tile), so each pair
+//         costs two real rows instead of two complex rows;
+//   n:    Re and Im of every component (2K columns).
+//
+// Both operands are split into FP16 hi + lo parts (hi = fp16(v), lo =
+// fp16(v - hi)); three products Ah*Bh + Ah*Bl + Al*Bh accumulate in FP32 in
+// TMEM.  B is scaled per (slice, component) by 2^(14 - e), e the exponent of
+// max |c_k|, so the largest value sits just below 2^14.  The cross-CTA sum
+// over site splits and the un-scaling are FP64 (k_split_reduce), in a fixed
+// order.
+//
+// CTA: 256 threads, one N-tile of NT components (2NT TMEM columns), a range
+// of 64-site k-steps.  Per k-step: thread 0 bulk-copies the two 16 KB phase
+// tiles (prebuilt in the swizzled layout) into the stage; all threads load
+// c (coalesced along x), split it and store it swizzled; one thread issues
+// 3 x 4 (x 2 N-halves) tcgen05.mma and commits to the stage's mbarrier,
+// which frees the stage two k-steps later.
+#include <cuda_fp16.h>
+
+#include "kernels.cuh"
+#include "p2_common.cuh"
+#include "tc.cuh"
+
+namespace p2 {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kKS = 64;                   // sites per k-step
+constexpr int kATile = 128 * kKS * 2;     // bytes of one 128 x 64 FP16 tile
+
+__host__ __device__ constexpr int b_tile_bytes(int NT) { return 2 * NT * kKS * 2; }
+__host__ __device__ constexpr int stage_bytes(int NT) { return 2 * kATile + 2 * b_tile_bytes(NT); }
+__host__ __device__ constexpr int tmem_cols(int NT) {
+  return 2 * NT <= 32 ? 32 : 2 * NT <= 64 ? 64 : 2 * NT <= 128 ? 128 : 2 * NT <= 256 ? 256 : 512;
+}
+
+__global__ void k_build_phases(const PhaseBuildArgs a) {
+  const long long n = (long long)a.nmtile * a.nkstep * 128 * kKS;
+  const Cx<double>* tab = (const Cx<double>*)a.tab;
+  __half* A = (__half*)a.A;
+  const int LxLy = a.Lx * a.Ly;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int xk = (int)(i % kKS);
+    const int row = (int)((i / kKS) % 128);
+    const long long ks = (i / (kKS * 128)) % a.nkstep;
+    const int mt = (int)(i / ((long long)kKS * 128 * a.nkstep));
+    const int r = mt * 128 + row;
+    const long long x = ks * kKS + xk;
+    double v = 0.0;
+    if (r < a.nrows && x < a.V3) {
+      const int h = a.row_h[r];
+      const int xx = (int)(x % a.Lx), yy = (int)((x / a.Lx) % a.Ly), zz = (int)(x / LxLy);
+      const Cx<double> e = cmul(cmul(tab[(0 * a.nh + h) * a.Lmax + xx], tab[(1 * a.nh + h) * a.Lmax + yy]),
+                                tab[(2 * a.nh + h) * a.Lmax + zz]);
+      v = a.row_sin[r] ? -e.y : e.x;  // e = cos(phi) - i sin(phi)
+    }
+    const __half hi = __double2half(v);
+    const __half lo = __double2half(v - (double)__half2float(hi));
+    unsigned char* tile = (unsigned char*)A + ((long long)mt * a.nkstep + ks) * 2 * kATile;
+    const uint32_t off = tc::sw128_offset(row, xk);
+    *(__half*)(tile + off) = hi;
+    *(__half*)(tile + kATile + off) = lo;
+  }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmArgs a) {
+  constexpr int NR = 2 * NT;                 // B rows (Re, Im per component)
+  constexpr int BT = b_tile_bytes(NT);
+  constexpr int ST = stage_bytes(NT);
+  constexpr int NH = NR > 256 ? 2 : 1;       // MMAs per product (N <= 256 each)
+  constexpr int NM = NR / NH;
+  constexpr uint32_t IDESC = tc::idesc_f16_f32(128, NM);
+  constexpr int TCOLS = tmem_cols(NT);
+  constexpr int JN = NT / 8;                 // components per producer thread
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // the dynamic window is only guaranteed 16-byte aligned: round up to 1024
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* fullA = (uint64_t*)(smem + 2 * ST);
+  uint64_t* done = fullA + 2;
+  uint32_t* tslot = (uint32_t*)(done + 2);
+  int* flag = (int*)(tslot + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nti = blockIdx.x % a.ntile, mt = blockIdx.x / a.ntile;
+  const int split = blockIdx.y, tau = blockIdx.z;
+  const int k0 = nti * NT;
+  const int ks0 = split * a.ks_per_split;
+  const int nk = min(a.nkstep, ks0 + a.ks_per_split) - ks0;
+
+  if (warp == 0) {
+    tc::tmem_alloc(tslot, TCOLS);
+    tc::tmem_relinquish();
+  }
+  if (tid == 0) {
+    tc::mbar_init(&fullA[0], 1);
+    tc::mbar_init(&fullA[1], 1);
+    tc::mbar_init(&done[0], 1);
+    tc::mbar_init(&done[1], 1);
+    tc::fence_mbar_init();
+    *flag = 0;
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tslot;
+
+  // producer role: site pair sp (sites 2sp, 2sp+1 of the k-step), components kg + 8j
+  const int sp = tid & 31, kg = tid >> 5;
+  float sc[JN];
+#pragma unroll
+  for (int j = 0; j < JN; j++) {
+    const int k = k0 + kg + 8 * j;
+    sc[j] = 0.f;
+    if (k < a.K) {
+      const float mx = __int_as_float(a.cmax[(long long)tau * a.K + k]);
+      int e = 0;
+      if (mx > 0.f) frexpf(mx, &e);
+      sc[j] = ldexpf(1.f, 14 - e);
+    }
+  }
+  const Cx<float>* cb = (const Cx<float>*)a.c + (long long)tau * a.K * a.V3;
+  const unsigned char* Ab = (const unsigned char*)a.A + (long long)mt * a.nkstep * 2 * kATile;
+
+  int issued = -1;  // last k-step whose phase copy thread 0 issued
+  bool failed = false;
+  for (int i = 0; i < nk; i++) {
+    const int s = i & 1;
+    unsigned char* st = smem + s * ST;
+    bool bad = false;
+    if (i >= 2) bad = !tc::mbar_wait(&done[s], ((i >> 1) - 1) & 1);
+    if (__syncthreads_or(bad || *flag)) {
+      failed = true;
+      break;
+    }
+    const int ks = ks0 + i;
+    if (tid == 0) {
+      tc::mbar_expect_tx(&fullA[s], 2 * kATile);
+      tc::bulk_g2s(st, Ab + (long long)ks * 2 * kATile, 2 * kATile, &fullA[s]);
+      issued = i;
+    }
+    // B: split c into hi/lo FP16, Re and Im rows per component
+    unsigned char* Bh = st + 2 * kATile;
+    unsigned char* Bl = Bh + BT;
+    const long long x = (long long)ks * kKS + 2 * sp;
+#pragma unroll
+    for (int j = 0; j < JN; j++) {
+      const int kk = kg + 8 * j;
+      const int k = k0 + kk;
+      Cx<float> v0 = czero<float>(), v1 = czero<float>();
+      if (k < a.K) {
+        const Cx<float>* src = cb + (long long)k * a.V3 + x;
+        if (x < a.V3) v0 = src[0];
+        if (x + 1 < a.V3) v1 = src[1];
+      }
+      const float r0 = v0.x * sc[j], i0 = v0.y * sc[j], r1 = v1.x * sc[j], i1 = v1.y * sc[j];
+      const __half2 hr = __floats2half2_rn(r0, r1);
+      const __half2 hi_ = __floats2half2_rn(i0, i1);
+      const float2 fr = __half22float2(hr), fi = __half22float2(hi_);
+      const __half2 lr = __floats2half2_rn(r0 - fr.x, r1 - fr.y);
+      const __half2 li = __floats2half2_rn(i0 - fi.x, i1 - fi.y);
+      const uint32_t ore = tc::sw128_offset(2 * kk, 2 * sp);
+      const uint32_t oim = tc::sw128_offset(2 * kk + 1, 2 * sp);
+      *(__half2*)(Bh + ore) = hr;
+      *(__half2*)(Bh + oim) = hi_;
+      *(__half2*)(Bl + ore) = lr;
+      *(__half2*)(Bl + oim) = li;
+    }
+    tc::fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      if (!tc::mbar_wait(&fullA[s], (i >> 1) & 1)) {
+        *flag = 1;
+      } else {
+        tc::tc_fence_after();
+        const uint32_t a_hi = tc::smem_u32(st), a_lo = a_hi + kATile;
+        const uint32_t b_hi = tc::smem_u32(Bh), b_lo = tc::smem_u32(Bl);
+#pragma unroll
+        for (int kk = 0; kk < kKS / 16; kk++) {
+#pragma unroll
+          for (int prod = 0; prod < 3; prod++) {
+            const uint32_t aa = (prod == 2 ? a_lo : a_hi) + kk * 32;
+            const uint32_t bb = (prod == 1 ? b_lo : b_hi) + kk * 32;
+#pragma unroll
+            for (int h = 0; h < NH; h++) {
+              const uint32_t acc = (i > 0 || kk > 0 || prod > 0) ? 1u : 0u;
+              tc::mma_f16(tmem + h * NM, tc::desc_sw128(aa), tc::desc_sw128(bb + h * (NM / 8) * 1024), IDESC, acc);
+            }
+          }
+        }
+        tc::mma_commit(&done[s]);
+      }
+    }
+  }
+  if (!failed && nk > 0) {
+    const int last = nk - 1;
+    bool bad = !tc::mbar_wait(&done[last & 1], (last >> 1) & 1);
+    failed = __syncthreads_or(bad || *flag);
+  } else {
+    failed = __syncthreads_or(failed || *flag);
+  }
+  if (failed) {
+    // let any phase copy still in flight land before the CTA exits
+    if (tid == 0 && issued >= 0) tc::mbar_wait(&fullA[issued & 1], (issued >> 1) & 1, 1LL << 22);
+    if (tid == 0) atomicExch(a.err, 1);
+  } else {
+    tc::tc_fence_after();
+    // epilogue: warps w and w+4 share TMEM lanes 32*(w%4).., half the columns each
+    const int row = 32 * (warp & 3) + lane;
+    const int c0 = (warp >> 2) * (NR / 2);
+    float* dst = a.part + ((((long long)tau * a.nsplit + split) * a.nmtile + mt) * 128 + row) * (long long)(a.ntile * NR) +
+                 nti * NR;
+#pragma unroll 1
+    for (int c = c0; c < c0 + NR / 2; c += 16) {
+      float v[16];
+      tc::tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c, v);
+      float4* d4 = (float4*)(dst + c);
+#pragma unroll
+      for (int q = 0; q < 4; q++) d4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, TCOLS);
+}
+
+__global__ void k_split_reduce(const SplitReduceArgs a) {
+  const long long n = (long long)a.ntau * a.nmom * a.K;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i % a.K);
+    const int p = (int)((i / a.K) % a.nmom);
+    const int tau = (int)(i / ((long long)a.K * a.nmom));
+    const int rc = a.mom_row[3 * p], rs = a.mom_row[3 * p + 1], sg = a.mom_row[3 * p + 2];
+    const int col = (k / a.NT) * 2 * a.NT + 2 * (k % a.NT);
+    double cr = 0, ci = 0, sr = 0, si = 0;
+    for (int sp = 0; sp < a.nsplit; sp++) {
+      const float* base = a.part + ((long long)tau * a.nsplit + sp) * a.nmtile * 128 * (long long)a.ncols;
+      const float* pc = base + (long long)rc * a.ncols + col;
+      cr += (double)pc[0];
+      ci += (double)pc[1];
+      if (rs >= 0) {
+        const float* ps = base + (long long)rs * a.ncols + col;
+        sr += (double)ps[0];
+        si += (double)ps[1];
+      }
+    }
+    const float mx = __int_as_float(a.cmax[(long long)tau * a.K + k]);
+    int e = 0;
+    if (mx > 0.f) frexpf(mx, &e);
+    const int pw = a.kexp[2 * k] * a.exp_u[tau] + a.kexp[2 * k + 1] * a.exp_d[tau] - (14 - e);
+    const double f = ldexp(1.0, pw);
+    Cx<double> v = cx<double>((cr + sg * si) * f, (ci - sg * sr) * f);
+    for (int b = 0; b < a.nblocks; b++) {
+      const ScatterBlock& B = a.blk[b];
+      const int rel = k - B.k0;
+      if (rel >= 0 && rel < B.groups * B.datasets * B.comps) {
+        const int comp = rel % B.comps;
+        const int gd = rel / B.comps;
+        const long long o = B.base + (((long long)gd * a.totalT + a.tau0 + tau) * a.nmom + p) * B.comps + comp;
+        ((Cx<double>*)a.out)[o] = v;
+      }
+    }
+  }
+}
+
+template <int NT>
+cudaError_t launch_nt(const SplitGemmArgs& a, cudaStream_t s) {
+  const int smem = stage_bytes(NT) * 2 + 64 + 1024;
+  cudaError_t e = cudaFuncSetAttribute(k_project_split<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid(a.ntile * a.nmtile, a.nsplit, a.ntau);
+  k_project_split<NT><<<grid, kThreads, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+int project_split_smem_bytes(int NT) { return stage_bytes(NT) * 2 + 64 + 1024; }
+
+cudaError_t launch_build_phases(const PhaseBuildArgs& a, cudaStream_t s) {
+  const long long n = (long long)a.nmtile * a.nkstep * 128 * kKS;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 32);
+  k_build_phases<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_project_split(const SplitGemmArgs& a, cudaStream_t s) {
+  switch (a.NT) {
+    case 16: return launch_nt<16>(a, s);
+    case 32: return launch_nt<32>(a, s);
+    case 48: return launch_nt<48>(a, s);
+    case 64: return launch_nt<64>(a, s);
+    case 80: return launch_nt<80>(a, s);
+    case 96: return launch_nt<96>(a, s);
+    case 112: return launch_nt<112>(a, s);
+    case 128: return launch_nt<128>(a, s);
+    case 144: return launch_nt<144>(a, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_split_reduce(const SplitReduceArgs& a, cudaStream_t s) {
+  const long long n = (long long)a.ntau * a.nmom * a.K;
+  int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+  if (blocks < 1) blocks = 1;
+  k_split_reduce<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace p2

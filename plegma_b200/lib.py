@@ -63,10 +63,14 @@ class P2Block(C.Structure):
                 ("offset", C.c_size_t)]
 
 
+class P2KernelTime(C.Structure):
+    _fields_ = [("name", C.c_char * 48), ("launches", C.c_longlong), ("ms", C.c_double)]
+
+
 #: Every entry point declared in include/plegma2pt.h.
 EXPORTS = ["p2_ctx_create", "p2_ctx_destroy", "p2_last_error", "p2_sync", "p2_set_stream", "p2_components",
            "p2_mom_list", "p2_block_info", "p2_contract_project", "p2_contract_position", "p2_ft_apply",
-           "p2_synth_propagator"]
+           "p2_synth_propagator", "p2_profile_enable", "p2_profile_read", "p2_alloc", "p2_free", "p2_copy"]
 
 _lib = None
 
@@ -93,6 +97,11 @@ def load(path: str = LIB_PATH) -> C.CDLL:
                                 C.c_void_p, C.c_int]
     lib.p2_synth_propagator.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int,
                                         C.c_double, C.c_int, C.c_int]
+    lib.p2_alloc.argtypes = [C.c_void_p, C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]
+    lib.p2_free.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.p2_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.p2_profile_enable.argtypes = [C.c_void_p, C.c_int]
+    lib.p2_profile_read.argtypes = [C.c_void_p, C.POINTER(P2KernelTime), C.c_int, C.c_int]
     _lib = lib
     return lib
 
@@ -209,6 +218,15 @@ class Context:
     def contract_position(self, props: Sequence[P2Prop], req: P2Request):
         pa = (P2Prop * len(props))(*props)
         self.check(self.lib.p2_contract_position(self.h, pa, len(props), C.byref(req)))
+
+    def profile(self, on: bool = True):
+        self.check(self.lib.p2_profile_enable(self.h, int(on)))
+
+    def profile_read(self, reset: bool = True):
+        """{kernel name: (launches, total ms)} since the last reset."""
+        buf = (P2KernelTime * 64)()
+        n = self.lib.p2_profile_read(self.h, buf, 64, int(reset))
+        return {buf[i].name.decode(): (buf[i].launches, buf[i].ms) for i in range(min(n, 64))}
 
     def ft_apply(self, field_ptr: int, dof: int, nt: int, moms: np.ndarray, sign: int, out_ptr: int,
                  out_location=P2_DEVICE):

@@ -1,0 +1,69 @@
+// A caller of the drop-in C++ surface, written the way the reference's
+// production driver (plegma/Calc_2pt.cpp:73-131) uses PLEGMA_Correlator:
+// two propagators, a momentum-space correlator per source, contractMesons*,
+// contractBaryons, writeFile.  The GPU tests compare what it writes with the
+// C ABI results and the oracle.
+//
+//   calc_2pt Lx Ly Lz Lt sx sy sz st totalT q2max mode out_prefix
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+
+#include "plegma/PLEGMA_2pt.h"
+
+using namespace plegma;
+
+int main(int argc, char** argv) {
+  if (argc != 13) {
+    std::fprintf(stderr, "usage: calc_2pt Lx Ly Lz Lt sx sy sz st totalT q2max mode out_prefix\n");
+    return 2;
+  }
+  const std::array<int, 4> L{{std::atoi(argv[1]), std::atoi(argv[2]), std::atoi(argv[3]), std::atoi(argv[4])}};
+  const site src(std::atoi(argv[5]), std::atoi(argv[6]), std::atoi(argv[7]), std::atoi(argv[8]));
+  const int totalT = std::atoi(argv[9]), q2max = std::atoi(argv[10]);
+  const CONTRACTION_MODE mode = std::atoi(argv[11]) ? SPLIT_FP16 : PLAIN_FP64;
+  const std::string out = argv[12];
+  try {
+    PLEGMA_init(L);
+    PLEGMA_Propagator<double> up(BOTH), dn(DEVICE);
+    up.fillSynthetic(2024, 0, src[3], 0.5);
+    dn.fillSynthetic(2024, 1, src[3], 0.5);
+
+    PLEGMA_Correlator<double> mes(MOMENTUM_SPACE, src, q2max, totalT);
+    mes.setMode(mode);
+    mes.contractMesonsAll(up, dn);
+    mes.writeFile(out + "_mesons_all", DEFAULT_FORMAT);
+    mes.writeFile(out + "_mesons_all", ASCII_FORMAT);
+
+    PLEGMA_Correlator<double> m10(MOMENTUM_SPACE, src, q2max, totalT);
+    m10.setMode(mode);
+    m10.contractMesons(up, dn);
+    m10.writeFile(out + "_mesons10", DEFAULT_FORMAT);
+
+    PLEGMA_Correlator<double> bar(MOMENTUM_SPACE, src, q2max, totalT);
+    bar.setMode(mode);
+    bar.contractBaryons(up, dn);
+    bar.writeFile(out + "_baryons", DEFAULT_FORMAT);
+
+    PLEGMA_Correlator<double> pos(POSITION_SPACE, src, 0, totalT);
+    pos.contractBaryons(up, dn);
+    pos.writeFile(out + "_baryons_pos", DEFAULT_FORMAT);
+
+    // generic transform of the up propagator as a 144-component field
+    PLEGMA_FT<double> ft(q2max);
+    ft.apply(up, FT_GEMV, -1);
+    FILE* f = std::fopen((out + "_ft_up.bin").c_str(), "wb");
+    std::fwrite(ft.H_elem(), sizeof(double), (size_t)2 * ft.Nmoms() * ft.DimT() * 144, f);
+    std::fclose(f);
+
+    up.copyToHost();
+    f = std::fopen((out + "_up.bin").c_str(), "wb");
+    std::fwrite(up.H_elem(), sizeof(double), (size_t)2 * 144 * up.Total_length(), f);
+    std::fclose(f);
+    PLEGMA_finalize();
+  } catch (const PLEGMA_exception& e) {
+    std::fprintf(stderr, "calc_2pt: %s\n", e.what());
+    return 1;
+  }
+  return 0;
+}

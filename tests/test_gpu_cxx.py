@@ -1,0 +1,138 @@
+"""The C++ drop-in surface (include/plegma/PLEGMA_2pt.h), used by a driver
+written like the reference's plegma/Calc_2pt.cpp, checked against the
+oracle: reference buffer layouts (including the time rotation of a window
+that wraps through t = 0), the binary/JSON writer, the ASCII writer, the
+position-space correlator and PLEGMA_FT::apply."""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from plegma_b200 import lib as p2
+
+from p2test import device_props, oracle_blocks
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "tests", "cxx", "_build", "calc_2pt")
+L = (6, 4, 4, 8)
+SRC = (1, 2, 3, 5)
+TOTALT = 6
+Q2 = 2
+
+
+@pytest.fixture(scope="module")
+def outputs(tmp_path_factory):
+    if not os.path.exists(EXE):
+        pytest.fail("tests/cxx/_build/calc_2pt is missing: run __graft_entry__.build()")
+    d = tmp_path_factory.mktemp("cxx")
+    prefix = str(d / "run")
+    args = [EXE] + [str(x) for x in L + SRC] + [str(TOTALT), str(Q2), "0", prefix]
+    subprocess.run(args, check=True, timeout=300)
+    ctx = p2.Context(L)
+    bufs = device_props(ctx, [(2024, 0), (2024, 1)], t0=SRC[3])
+    moms = p2.mom_list(Q2)
+    yield prefix, ctx, bufs, moms
+    ctx.close()
+
+
+def load(prefix):
+    with open(prefix + ".json") as f:
+        meta = json.load(f)
+    raw = np.fromfile(prefix + ".bin", dtype=np.float64)
+    return meta, raw[0::2] + 1j * raw[1::2]
+
+
+def test_synthetic_fill_matches(outputs):
+    prefix, ctx, bufs, _ = outputs
+    up = np.fromfile(prefix + "_up.bin", dtype=np.float64)
+    up = up[0::2] + 1j * up[1::2]
+    assert np.array_equal(up, bufs[0].cpu().numpy())
+
+
+def test_mesons_all_layout_and_values(outputs):
+    prefix, ctx, bufs, moms = outputs
+    meta, v = load(prefix + "_mesons_all")
+    assert meta["shape"] == [TOTALT, len(moms), 34, 2]
+    assert meta["datasets"] == ["mesons/twop_meson"]
+    assert np.array_equal(np.array(meta["mvec"]), moms)
+    ref = oracle_blocks(L, bufs, SRC, moms, p2.MESON_ALL34, list(range(TOTALT)))[p2.MESON_ALL34][0][0, 0]
+    got = v.reshape(TOTALT, len(moms), 34)
+    assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-12
+
+
+def test_ascii_writer(outputs):
+    prefix, ctx, bufs, moms = outputs
+    name = prefix + "_mesons_all_sx%02dsy%02dsz%02dst%02d.dat" % SRC
+    lines = open(name).read().strip().split("\n")
+    assert len(lines) == TOTALT * len(moms)
+    f = lines[len(moms) + 1].split()
+    assert [int(x) for x in f[:4]] == [1] + list(moms[1])
+    _, v = load(prefix + "_mesons_all")
+    got = v.reshape(TOTALT, len(moms), 34)[1, 1, 0]
+    assert abs(float(f[4]) - got.real) <= 1e-6 * abs(got) + 1e-300
+
+
+def test_baryons(outputs):
+    prefix, ctx, bufs, moms = outputs
+    meta, v = load(prefix + "_baryons")
+    assert meta["datasets"] == ["baryons/nucl_nucl/twop_baryon_1", "baryons/nucl_nucl/twop_baryon_2"]
+    ref = oracle_blocks(L, bufs, SRC, moms, p2.NUCLEON_CG5, list(range(TOTALT)))[p2.NUCLEON_CG5][0][0]
+    got = v.reshape(2, TOTALT, len(moms), 16)
+    assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-12
+
+
+def test_mesons10_reference_buffer_layout(outputs):
+    """contractMesons keeps the reference's [t][mom][dataset][10] buffer
+    (PLEGMA_mesons.cuh:113-120); its writer reads that buffer as
+    [dataset][t][mom][10] like the reference's HDF5 writer does."""
+    prefix, ctx, bufs, moms = outputs
+    meta, v = load(prefix + "_mesons10")
+    nm = len(moms)
+    # rebuild H_elem from the writer's view, then read it as [slot][mom][ds][10]
+    lt = TOTALT
+    start = (L[3] - SRC[3]) % L[3]
+    start = 0 if start >= TOTALT else start
+    per = nm * 10
+    h = np.zeros(2 * lt * per, dtype=complex)
+    w = v.reshape(2, lt, per)
+    for d in range(2):
+        for it in range(lt):
+            i = (it - start) % TOTALT
+            h[(d * lt + i) * per:(d * lt + i + 1) * per] = w[d, it]
+    hv = h.reshape(lt, nm, 2, 10)
+    ref = oracle_blocks(L, bufs, SRC, moms, p2.MESON_DIAG10, list(range(TOTALT)))[p2.MESON_DIAG10][0][0]
+    for i in range(lt):
+        tau = (i + start) % TOTALT
+        assert np.allclose(hv[i, :, 0, :], ref[0, tau], rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+        assert np.allclose(hv[i, :, 1, :], ref[1, tau], rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+def test_position_space_baryons(outputs):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as orc
+    prefix, ctx, bufs, _ = outputs
+    meta, v = load(prefix + "_baryons_pos")
+    V3 = L[0] * L[1] * L[2]
+    assert meta["shape"] == [TOTALT, V3, 16, 2]
+    u = bufs[0].cpu().numpy().reshape(144, -1)
+    d = bufs[1].cpu().numpy().reshape(144, -1)
+    _, _, pos = orc.twopt(L, u, d, SRC, [[0, 0, 0]], p2.NUCLEON_CG5, list(range(TOTALT)), want_pos=True)
+    got = v.reshape(2, TOTALT, V3, 16)
+    ref = pos.reshape(TOTALT, 2, 16, V3).transpose(1, 0, 3, 2)
+    assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-13
+
+
+def test_ft_apply(outputs):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as orc
+    prefix, ctx, bufs, moms = outputs
+    raw = np.fromfile(prefix + "_ft_up.bin", dtype=np.float64)
+    got = (raw[0::2] + 1j * raw[1::2]).reshape(L[3], 144, len(moms))
+    u = bufs[0].cpu().numpy()
+    ref = orc.ft(L, u.reshape(144, -1), 144, L[3], moms, -1)
+    assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-13

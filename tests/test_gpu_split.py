@@ -1,0 +1,91 @@
+"""Parity of the split-FP16 form (FP32 contraction, hi+lo FP16 tensor-core
+projection with FP32 accumulation, FP64 cross-block sums) with the FP64
+oracle.  Tolerance: err(t) <= 1e-6 relative to sum_x |c_k(x,t)|, per time
+slice, over all momenta and components."""
+import numpy as np
+import pytest
+
+from plegma_b200 import lib as p2
+
+from p2test import device_props, oracle_blocks, per_t_error, run
+
+pytestmark = pytest.mark.gpu
+
+NUC = p2.NUCLEON_CG5
+TOL = 1e-6
+SPLIT = p2.P2_SPLIT_FP16
+
+
+def test_split_small_nucleon():
+    ctx = p2.Context((4, 4, 4, 8))
+    (u,) = device_props(ctx, [(1001, 0)], t0=0)
+    bufs = [u, u]
+    out, moms = run(ctx, bufs, (0, 0, 0, 0), 8, NUC, q2max=2, mode=SPLIT)
+    taus = list(range(8))
+    ref = oracle_blocks(ctx.L, bufs, (0, 0, 0, 0), moms, NUC, taus)
+    err = per_t_error(out, NUC, 8, moms, ref, taus)
+    assert err.max() < TOL, err
+    ctx.close()
+
+
+def test_split_odd_lattice_all_mesons_asymmetric_momenta():
+    """V3 = 30 (not a multiple of the 64-site k-step), a wrapping window, and
+    a momentum list that is not closed under p -> -p (cos and sin rows of
+    unpaired momenta)."""
+    ctx = p2.Context((3, 5, 2, 6))
+    bufs = device_props(ctx, [(7, 0), (7, 1)], t0=4)
+    what = NUC | p2.MESON_G16 | p2.MESON_ALL34 | p2.MESON_NEW10 | p2.MESON_DIAG10
+    src = (1, 3, 1, 4)
+    moms = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, -2, 1], [1, 1, 1], [-1, 2, 0]], dtype=np.int32)
+    out, moms = run(ctx, bufs, src, 5, what, moms=moms, mode=SPLIT)
+    taus = list(range(5))
+    ref = oracle_blocks(ctx.L, bufs, src, moms, what, taus)
+    err = per_t_error(out, what, 5, moms, ref, taus)
+    assert err.max() < TOL, err
+    ctx.close()
+
+
+def test_split_24_nucleon_mesons_q9():
+    """24^3 x 48, u and d, nucleon + 16x16 mesons, 123 momenta; the decay
+    exp(-0.5|t - t0|) spans ~10 decades in the baryons over the window."""
+    ctx = p2.Context((24, 24, 24, 48))
+    rng = np.random.default_rng(1002)
+    t0 = int(rng.integers(0, 48))
+    src = (int(rng.integers(0, 24)), int(rng.integers(0, 24)), int(rng.integers(0, 24)), t0)
+    bufs = device_props(ctx, [(1002, 0), (1002, 1)], t0=t0)
+    what = NUC | p2.MESON_G16
+    out, moms = run(ctx, bufs, src, 48, what, q2max=9, mode=SPLIT)
+    taus = [0, 1, 24, 47]
+    ref = oracle_blocks(ctx.L, bufs, src, moms, what, taus)
+    err = per_t_error(out, what, 48, moms, ref, taus)
+    assert err.max() < TOL, err
+    ctx.close()
+
+
+def test_split_fp32_propagators():
+    """FP32-stored propagators (the large batched configuration's storage)."""
+    ctx = p2.Context((6, 4, 4, 8))
+    bufs = device_props(ctx, [(1005, 0), (1005, 1)], t0=2, decay=0.4, precision=p2.P2_FP32)
+    what = NUC | p2.MESON_G16
+    out, moms = run(ctx, bufs, (1, 1, 1, 2), 8, what, q2max=4, mode=SPLIT, precision=p2.P2_FP32)
+    taus = list(range(8))
+    ref = oracle_blocks(ctx.L, bufs, (1, 1, 1, 2), moms, what, taus, fp32=True)
+    err = per_t_error(out, what, 8, moms, ref, taus)
+    assert err.max() < TOL, err
+    ctx.close()
+
+
+def test_split_matches_plain_to_tolerance():
+    ctx = p2.Context((8, 8, 8, 8))
+    bufs = device_props(ctx, [(3, 0), (3, 1)], t0=5)
+    what = NUC | p2.MESON_G16
+    a, moms = run(ctx, bufs, (2, 3, 4, 5), 8, what, q2max=3)
+    b, _ = run(ctx, bufs, (2, 3, 4, 5), 8, what, q2max=3, mode=SPLIT)
+    c, _ = run(ctx, bufs, (2, 3, 4, 5), 8, what, q2max=3, mode=SPLIT)
+    assert np.array_equal(b, c)  # deterministic
+    ga = p2.result_blocks(what, 8, len(moms), a)
+    gb = p2.result_blocks(what, 8, len(moms), b)
+    for bit in ga:
+        scale = np.abs(ga[bit]).max(axis=(3, 4), keepdims=True)
+        assert (np.abs(ga[bit] - gb[bit]) / scale).max() < 1e-5
+    ctx.close()
