@@ -151,7 +151,12 @@ def main():
     ap.add_argument("--form", default="auto", choices=["auto", "split", "plain"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--lattice", default=None,
+                    help="Lx,Ly,Lz,Lt override for small profiling cases (not the benchmark workload)")
     args = ap.parse_args()
+    global L
+    if args.lattice:
+        L = tuple(int(x) for x in args.lattice.split(","))
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -169,7 +174,9 @@ def main():
 
     from plegma_b200 import lib as p2
     ctx = p2.Context(L, device=local)
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream shared by torch's events and the library
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
 
     seed = SEED + rank

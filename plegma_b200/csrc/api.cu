@@ -191,8 +191,6 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request& r, const 
   const p2_prop& d = props[r.prop_d];
   if (u.precision != P2_FP64 || d.precision != P2_FP64)
     return c->fail(P2_ERR_UNSUPPORTED, "the plain FP64 form needs FP64 propagators");
-  if (r.contractions & (P2_DELTA_ISO12 | P2_DELTA_ISO32))
-    return c->fail(P2_ERR_UNSUPPORTED, "Delta contractions are not available in the plain FP64 form yet");
 
   std::vector<double> tabh = phase_tables(c, pl.moms.data(), pl.nmom, r.source, -1, pl.Lmax);
   P2_TRY(c, c->tab.ensure(tabh.size() * sizeof(double)), "phase table alloc");
@@ -539,8 +537,6 @@ p2_status p2_contract_position(p2_ctx* c, const p2_prop* props, int nprops, cons
   if (!r->out) return c->fail(P2_ERR_INVALID_ARG, "null output");
   if (r->contractions == 0 || (r->contractions & ~kAllBits))
     return c->fail(P2_ERR_INVALID_ARG, "contractions: empty or unknown bits");
-  if (r->contractions & (P2_DELTA_ISO12 | P2_DELTA_ISO32))
-    return c->fail(P2_ERR_UNSUPPORTED, "Delta contractions are not available in the plain FP64 form yet");
   if (r->totalT < 1 || r->totalT > c->T) return c->fail(P2_ERR_INVALID_ARG, "totalT out of range");
   const p2_prop& u = props[r->prop_u];
   const p2_prop& d = props[r->prop_d];

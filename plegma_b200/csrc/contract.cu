@@ -86,9 +86,35 @@ struct Writer {
   }
 };
 
+// Delta outputs of table g: group g of each isospin block, datasets (u-rich, d-rich).
 template <typename R>
+__device__ __forceinline__ void delta_out(const ContractArgs& a, const Writer<R>& w, int l, int g, const Cx<R> o[4]) {
+  if (a.what & 2u) {
+    w.put(a.k.diso12 + (g * 2 + 0) * 16 + l, o[0]);
+    w.put(a.k.diso12 + (g * 2 + 1) * 16 + l, o[1]);
+  }
+  if (a.what & 4u) {
+    w.put(a.k.diso32 + (g * 2 + 0) * 16 + l, o[2]);
+    w.put(a.k.diso32 + (g * 2 + 1) * 16 + l, o[3]);
+  }
+}
+
+// DELTA selects the instantiation: the Delta blocks only (true) or every other
+// block (false); a request with both runs the two instantiations over the same
+// tiles (the Delta part is ~5x the rest in arithmetic, so the second pass over
+// the propagators is hidden under its compute).
+template <typename R, bool DELTA>
 __device__ __forceinline__ void contract_site(const ContractArgs& a, const Cx<R>* U, const Cx<R>* D,
                                               const LaneTables& lt, int l, unsigned mask, const Writer<R>& w) {
+  if (DELTA) {
+#pragma unroll 1
+    for (int g = 0; g < 3; g++) {
+      Cx<R> o[4];
+      delta_site<R>(U, D, g, l, mask, o);
+      delta_out(a, w, l, g, o);
+    }
+    return;
+  }
   if (a.what & 1u) {
     const Cx<R> p = nucleon_site<R>(U, D, lt, l, mask);
     const Cx<R> n = nucleon_site<R>(D, U, lt, l, mask);
@@ -136,6 +162,7 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Cx<R>
 }
 
 // Plain FP64 form.
+template <bool DELTA>
 __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<double>* sm = (Cx<double>*)smem_raw;
@@ -160,7 +187,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
     if (x < a.V3) {
       const Cx<double>* U = st + hw * kRow;
       Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr};
-      contract_site<double>(a, U, U + 144, lt, l, mask, w);
+      contract_site<double, DELTA>(a, U, U + 144, lt, l, mask, w);
     }
     __syncthreads();
     issue_tile<double>(a, st, tile + 2LL * gridDim.x, ntiles, tiles_per_tau);
@@ -169,7 +196,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
 }
 
 // Split form: FP32 arithmetic on power-of-two scaled inputs.
-template <typename Tin>
+template <typename Tin, bool DELTA>
 __global__ void __launch_bounds__(kThreads, 1) k_contract_f32(const ContractArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<Tin>* sm = (Cx<Tin>*)smem_raw;
@@ -227,7 +254,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_f32(const ContractArgs
     if (x < a.V3) {
       const Cx<float>* U = sf + hw * kRow;
       Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, smax};
-      contract_site<float>(a, U, U + 144, lt, l, mask, w);
+      contract_site<float, DELTA>(a, U, U + 144, lt, l, mask, w);
     }
     __syncthreads();
   }
@@ -284,28 +311,40 @@ __global__ void k_sample_exponents(const SampleArgs a) {
 
 int contract_plain_smem_bytes() { return 2 * kStage * (int)sizeof(Cx<double>); }
 
-cudaError_t launch_contract_plain(const ContractArgs& a, int grid, cudaStream_t s) {
+template <bool DELTA>
+cudaError_t launch_plain_t(const ContractArgs& a, int grid, cudaStream_t s) {
   const int smem = contract_plain_smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(k_contract_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = cudaFuncSetAttribute(k_contract_plain<DELTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  k_contract_plain<<<grid, kThreads, smem, s>>>(a);
+  k_contract_plain<DELTA><<<grid, kThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t launch_contract_f32(const ContractArgs& a, int fp32_in, int grid, cudaStream_t s) {
-  const int tin = fp32_in ? (int)sizeof(Cx<float>) : (int)sizeof(Cx<double>);
-  const int smem = 2 * kStage * tin + kStage * (int)sizeof(Cx<float>) + a.K * (int)sizeof(int);
-  cudaError_t e;
-  if (fp32_in) {
-    e = cudaFuncSetAttribute(k_contract_f32<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    k_contract_f32<float><<<grid, kThreads, smem, s>>>(a);
-  } else {
-    e = cudaFuncSetAttribute(k_contract_f32<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    k_contract_f32<double><<<grid, kThreads, smem, s>>>(a);
-  }
+template <typename Tin, bool DELTA>
+cudaError_t launch_f32_t(const ContractArgs& a, int grid, cudaStream_t s) {
+  const int smem = 2 * kStage * (int)sizeof(Cx<Tin>) + kStage * (int)sizeof(Cx<float>) + a.K * (int)sizeof(int);
+  cudaError_t e = cudaFuncSetAttribute(k_contract_f32<Tin, DELTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  k_contract_f32<Tin, DELTA><<<grid, kThreads, smem, s>>>(a);
   return cudaGetLastError();
+}
+
+constexpr unsigned kDeltaBits = 2u | 4u;
+
+cudaError_t launch_contract_plain(const ContractArgs& a, int grid, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
+  if (a.what & ~kDeltaBits) e = launch_plain_t<false>(a, grid, s);
+  if (e == cudaSuccess && (a.what & kDeltaBits)) e = launch_plain_t<true>(a, grid, s);
+  return e;
+}
+
+cudaError_t launch_contract_f32(const ContractArgs& a, int fp32_in, int grid, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
+  if (a.what & ~kDeltaBits)
+    e = fp32_in ? launch_f32_t<float, false>(a, grid, s) : launch_f32_t<double, false>(a, grid, s);
+  if (e == cudaSuccess && (a.what & kDeltaBits))
+    e = fp32_in ? launch_f32_t<float, true>(a, grid, s) : launch_f32_t<double, true>(a, grid, s);
+  return e;
 }
 
 cudaError_t launch_sample_exponents(const SampleArgs& a, cudaStream_t s) {

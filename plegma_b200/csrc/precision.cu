@@ -110,8 +110,6 @@ p2_status run_one(p2_ctx* c, const p2_prop* props, const p2_request& r) {
   const p2_prop& u = props[r.prop_u];
   const p2_prop& d = props[r.prop_d];
   if (u.precision != d.precision) return c->fail(P2_ERR_UNSUPPORTED, "u and d must share a precision");
-  if (r.contractions & (P2_DELTA_ISO12 | P2_DELTA_ISO32))
-    return c->fail(P2_ERR_UNSUPPORTED, "Delta contractions are not available in the split form yet");
   const int fp32_in = u.precision == P2_FP32;
   const int K = pl.K;
 

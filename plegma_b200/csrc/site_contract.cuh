@@ -214,4 +214,154 @@ __device__ __forceinline__ void meson_site(const Cx<R>* __restrict__ A, const Cx
   }
 }
 
+// ---- Delta C g_k (PLEGMA_baryons_deltas.cu:7-110) ------------------------------
+//
+// All 14 Wick terms (8 of isospin 1/2, 6 of isospin 3/2) are products
+//   X[nu][s1'] Y[lam][s2'] Z[mu][s3']  (colours a, b, c at the sink; the source
+//   colour of a line follows its source spin slot),
+// with Gamma = C g_k on (nu, lam) and Gamma-bar on (lam', nu').  Summing the
+// sink diquark first gives, for the lane's source spins (x', y'),
+//   G^{XY}[c][e] = sum_{(nu,lam)} sA sum eps_abc eps_{c1 c2 e} X[nu][x'][a][c1] Y[lam][y'][b][c2]
+// (the same cofactor form as the nucleon's direct term), and every term is
+// +-G contracted with the third line:
+//   mu' on X's source slot (slot 1):  P[m] = f1 sum G[c][e] Z[m][z1][c][e], summed over y'
+//   mu' on Y's source slot (slot 2):  P[m] = f2 sum G[c][e] Z[m][z2][c][e], summed over x'
+//   mu' on Z (type a):                 D = sum over the 16 lanes of fa G, T = sum D Z[mu][mu']
+// with f1 = -(c1A sA1 - c1B sB1), f2 = c2A sA2 - c2B sB2, fa = cN sN - cL sL from the
+// per-lane descriptors (spin.diquark_lane_tables) and the Wick coefficients c.
+struct DeltaLane {
+  int z1, sA1, sB1, z2, sA2, sB2, sN, sL;
+};
+
+__constant__ int c_delta_lane[3][16][8] = P2_INIT_DeltaLane;
+
+__device__ __forceinline__ DeltaLane load_delta_lane(int g, int l) {
+  DeltaLane d;
+  d.z1 = c_delta_lane[g][l][0];
+  d.sA1 = c_delta_lane[g][l][1];
+  d.sB1 = c_delta_lane[g][l][2];
+  d.z2 = c_delta_lane[g][l][3];
+  d.sA2 = c_delta_lane[g][l][4];
+  d.sB2 = c_delta_lane[g][l][5];
+  d.sN = c_delta_lane[g][l][6];
+  d.sL = c_delta_lane[g][l][7];
+  return d;
+}
+
+__constant__ int c_delta_sink[3][4][3] = P2_INIT_DeltaSink;
+
+// G^{XY} for lane (x' = l >> 2, y' = l & 3) and table g (k = g + 1).
+template <typename R>
+__device__ __forceinline__ void delta_G(const Cx<R>* __restrict__ X, const Cx<R>* __restrict__ Y, int g, int xp,
+                                        int yp, Cx<R> q[9]) {
+#pragma unroll
+  for (int i = 0; i < 9; i++) q[i] = czero<R>();
+#pragma unroll 1
+  for (int iA = 0; iA < 4; iA++) {
+    const Cx<R>* Xb = X + sblk(c_delta_sink[g][iA][0], xp);
+    const Cx<R>* Yb = Y + sblk(c_delta_sink[g][iA][1], yp);
+    const R s = R(c_delta_sink[g][iA][2]);
+    Cx<R> a[9], b[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+      a[i] = cscale(Xb[i], s);
+      b[i] = Yb[i];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+#pragma unroll
+      for (int e = 0; e < 3; e++) {
+        const int e1 = (e + 1) % 3, e2 = (e + 2) % 3;
+        Cx<R>& r = q[c * 3 + e];
+        cmac(r, a[c1 * 3 + e1], b[c2 * 3 + e2]);
+        cmsub(r, a[c1 * 3 + e2], b[c2 * 3 + e1]);
+        cmsub(r, a[c2 * 3 + e1], b[c1 * 3 + e2]);
+        cmac(r, a[c2 * 3 + e2], b[c1 * 3 + e1]);
+      }
+    }
+  }
+}
+
+// One group of Wick terms sharing G and the third line Z; returns the lane's
+// share of T[mu = l >> 2][mu' = l & 3].
+template <typename R>
+__device__ __forceinline__ Cx<R> delta_eval(const Cx<R> g[9], const Cx<R>* __restrict__ Z, const DeltaLane& dl, int l,
+                                            unsigned mask, int c1A, int c1B, int c2A, int c2B, int cN, int cL) {
+  const R f1 = R(-(c1A * dl.sA1 - c1B * dl.sB1));
+  const R f2 = R(c2A * dl.sA2 - c2B * dl.sB2);
+  const R fa = R(cN * dl.sN - cL * dl.sL);
+  const int mu = l >> 2, mup = l & 3;
+  Cx<R> r = czero<R>();
+  // slot 2 (reduce over x'): this lane's y' is mu'
+#pragma unroll 1
+  for (int m = 0; m < 4; m++) {
+    const Cx<R>* Z2 = Z + sblk(m, dl.z2);
+    Cx<R> p2 = czero<R>();
+#pragma unroll
+    for (int i = 0; i < 9; i++) cmac(p2, g[i], Z2[i]);
+    p2 = cscale(p2, f2);
+    p2 = p2 + shfl_xor16(p2, 4, mask);
+    p2 = p2 + shfl_xor16(p2, 8, mask);
+    if (m == mu) r = r + p2;
+  }
+  // slot 1 (reduce over y'): T[.][mu'] sits on lane (x' = mu', y' = 0)
+  const int src = mup << 2;
+#pragma unroll 1
+  for (int m = 0; m < 4; m++) {
+    const Cx<R>* Z1 = Z + sblk(m, dl.z1);
+    Cx<R> p1 = czero<R>();
+#pragma unroll
+    for (int i = 0; i < 9; i++) cmac(p1, g[i], Z1[i]);
+    p1 = cscale(p1, f1);
+    p1 = p1 + shfl_xor16(p1, 1, mask);
+    p1 = p1 + shfl_xor16(p1, 2, mask);
+    const Cx<R> v = shfl_idx16(p1, src, mask);
+    if (m == mu) r = r + v;
+  }
+  // type a
+  const Cx<R>* Zm = Z + sblk(mu, mup);
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    Cx<R> d = cscale(g[i], fa);
+    d = d + shfl_xor16(d, 1, mask);
+    d = d + shfl_xor16(d, 2, mask);
+    d = d + shfl_xor16(d, 4, mask);
+    d = d + shfl_xor16(d, 8, mask);
+    cmac(r, d, Zm[i]);
+  }
+  return r;
+}
+
+// Delta C g_k, k = g + 1: out = {iso-1/2 Delta+ (u,u,d), iso-1/2 Delta0 (d,d,u),
+// iso-3/2 Delta++ (u,u,u), iso-3/2 Delta- (d,d,d)} for lane (mu, mu').
+template <typename R>
+__device__ __forceinline__ void delta_site(const Cx<R>* __restrict__ U, const Cx<R>* __restrict__ D, int g, int l,
+                                           unsigned mask, Cx<R> out[4]) {
+  const DeltaLane dl = load_delta_lane(g, l);
+  const int xp = l >> 2, yp = l & 3;
+  const R third = R(1) / R(3);
+#pragma unroll
+  for (int i = 0; i < 4; i++) out[i] = czero<R>();
+  // flavour pairs (X, Y) of the two diquark lines: uu, dd, ud, du
+#pragma unroll 1
+  for (int pair = 0; pair < 4; pair++) {
+    const Cx<R>* X = (pair == 0 || pair == 2) ? U : D;
+    const Cx<R>* Y = (pair == 0 || pair == 3) ? U : D;
+    Cx<R> q[9];
+    delta_G<R>(X, Y, g, xp, yp, q);
+    if (pair < 2) {
+      // G^{AA}: isospin 1/2 with the other flavour on the third line, isospin 3/2 with the same
+      const Cx<R> a = delta_eval<R>(q, pair == 0 ? D : U, dl, l, mask, 0, 2, 0, -2, 1, -1);
+      const Cx<R> b = delta_eval<R>(q, pair == 0 ? U : D, dl, l, mask, -1, 1, 1, -1, 1, -1);
+      out[pair] = out[pair] + cscale(a, third);
+      out[2 + pair] = out[2 + pair] + b;
+    } else {
+      // G^{AB}: isospin 1/2 with A on the third line
+      const Cx<R> a = delta_eval<R>(q, pair == 2 ? U : D, dl, l, mask, -4, 0, 2, -2, 4, 0);
+      out[pair - 2] = out[pair - 2] + cscale(a, third);
+    }
+  }
+}
+
 }  // namespace p2

@@ -135,6 +135,39 @@ def delta_tables():
     return [diquark_table(c) for c in CGK]
 
 
+def diquark_lane_tables(table):
+    """Factorised form of a diquark table for the lane-parallel kernels.
+
+    The weight of entry (iA, iB) (sink pair iA, source pair iB) factorises as
+    sA[iA] * sB[iB]; the source pairing lambda' <-> nu' is an involution.
+    Returns (sink[4][3] = (nu, lambda, sA), lanes[16][8]) where lane
+    l = (x' = l >> 2, y' = l & 3) holds
+      z1, sA1, sB1  slot-1 terms: Z spin, sB of the pair with lambda' = y',
+                    sB of the pair with nu' = y'
+      z2, sA2, sB2  slot-2 terms: same with x'
+      sN, sL        type-a terms: sB if (x', y') = (nu', lambda') resp.
+                    (lambda', nu') of a pair, else 0.
+    """
+    vals = [r[4] for r in table]
+    sB = [vals[iB] for iB in range(4)]
+    sA = [vals[iA * 4] * vals[0] for iA in range(4)]
+    assert all(vals[a * 4 + b] == sA[a] * sB[b] for a in range(4) for b in range(4)), "weights do not factorise"
+    lamp = [table[iB][2] for iB in range(4)]
+    nup = [table[iB][3] for iB in range(4)]
+    for iB in range(4):  # involution: the pair whose lambda' is nu'(iB) has nu' = lambda'(iB)
+        assert nup[lamp.index(nup[iB])] == lamp[iB], "source pairing is not an involution"
+    sink = [(table[iA * 4][0], table[iA * 4][1], sA[iA]) for iA in range(4)]
+    lanes = []
+    for l in range(16):
+        x, y = l >> 2, l & 3
+        iA1, iB1 = lamp.index(y), nup.index(y)
+        iA2, iB2 = lamp.index(x), nup.index(x)
+        sN = next((sB[i] for i in range(4) if (nup[i], lamp[i]) == (x, y)), 0)
+        sL = next((sB[i] for i in range(4) if (lamp[i], nup[i]) == (x, y)), 0)
+        lanes.append((nup[iA1], sB[iA1], sB[iB1], nup[iA2], sB[iA2], sB[iB2], sN, sL))
+    return sink, lanes
+
+
 def levi_civita():
     """The six colour permutations (a, b, c) and their signs, even ones first:
     the cyclic rotations of (0,1,2), then the transpositions (0<->2), (1<->2),
@@ -209,6 +242,8 @@ def header_text() -> str:
            _c_array("kNucVal", "int", [r[4] for r in nuc]),
            _c_array("kDeltaIdx", "int", [[r[:4] for r in t] for t in dl]),
            _c_array("kDeltaVal", "int", [[r[4] for r in t] for t in dl]),
+           _c_array("kDeltaSink", "int", [diquark_lane_tables(t)[0] for t in dl]),
+           _c_array("kDeltaLane", "int", [diquark_lane_tables(t)[1] for t in dl]),
            _c_array("kEps", "int", eps),
            _c_array("kEpsSign", "int", sgn),
            "}  // namespace p2\n"]

@@ -146,3 +146,19 @@ def test_invalid_requests_return_status(ctx_small):
     # the context stays usable after errors
     (u2,) = device_props(ctx, [(2, 0)], t0=0)
     run(ctx, [u2, u2], (0, 0, 0, 0), 8, NUC, q2max=0)
+
+
+def test_delta_all_isospins_plain():
+    """Delta C g_k, k = 1..3, isospin 1/2 and 3/2, both datasets, with the
+    nucleon and the 16x16 mesons in the same request (the batched
+    configuration's contraction set, K = 480)."""
+    ctx = p2.Context((4, 3, 5, 6))
+    bufs = device_props(ctx, [(41, 0), (41, 1)], t0=2)
+    what = NUC | p2.DELTA_ISO12 | p2.DELTA_ISO32 | p2.MESON_G16
+    assert p2.components(what) == 480
+    out, moms = run(ctx, bufs, (1, 2, 3, 2), 6, what, q2max=2)
+    taus = list(range(6))
+    ref = oracle_blocks(ctx.L, bufs, (1, 2, 3, 2), moms, what, taus)
+    err = per_t_error(out, what, 6, moms, ref, taus)
+    assert err.max() < TOL, err
+    ctx.close()

@@ -89,3 +89,17 @@ def test_split_matches_plain_to_tolerance():
         scale = np.abs(ga[bit]).max(axis=(3, 4), keepdims=True)
         assert (np.abs(ga[bit] - gb[bit]) / scale).max() < 1e-5
     ctx.close()
+
+
+def test_split_delta_batched_set():
+    """Nucleon + Delta (both isospins, k = 1..3) + 16x16 mesons, K = 480:
+    four N-tiles of the tensor-core projection."""
+    ctx = p2.Context((8, 6, 4, 8))
+    bufs = device_props(ctx, [(1004, 0), (1004, 1)], t0=6)
+    what = NUC | p2.DELTA_ISO12 | p2.DELTA_ISO32 | p2.MESON_G16
+    out, moms = run(ctx, bufs, (3, 1, 2, 6), 7, what, q2max=5, mode=SPLIT)
+    taus = list(range(7))
+    ref = oracle_blocks(ctx.L, bufs, (3, 1, 2, 6), moms, what, taus)
+    err = per_t_error(out, what, 7, moms, ref, taus)
+    assert err.max() < TOL, err
+    ctx.close()
