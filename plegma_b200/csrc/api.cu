@@ -144,6 +144,81 @@ p2_status chunk_view(p2_ctx* c, const p2_prop& p, DevBuf& stage, int t_begin, in
   return P2_OK;
 }
 
+std::vector<Chunk> make_chunks(const p2_ctx* c, const std::vector<TauRun>& runs, const int* src, int tc) {
+  std::vector<Chunk> out;
+  for (const TauRun& run : runs)
+    for (int off = 0; off < run.n; off += tc) {
+      Chunk ch;
+      ch.tau0 = run.tau0 + off;
+      ch.n = std::min(tc, run.n - off);
+      ch.t_begin = (src[3] + ch.tau0) % c->T;
+      out.push_back(ch);
+    }
+  return out;
+}
+
+Uploader::Uploader(p2_ctx* ctx, const p2_prop& pu, const p2_prop& pd)
+    : c(ctx), u(pu), d(pd), host(pu.location == P2_HOST || pd.location == P2_HOST) {}
+
+p2_status Uploader::issue(int slot, const Chunk& ch) {
+  if (!host) return P2_OK;
+  if (!c->copy_stream) {
+    P2_TRY(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "copy stream");
+    for (int i = 0; i < 2; i++) {
+      P2_TRY(c, cudaEventCreateWithFlags(&c->copied[i], cudaEventDisableTiming), "copy events");
+      P2_TRY(c, cudaEventCreateWithFlags(&c->consumed[i], cudaEventDisableTiming), "copy events");
+      P2_TRY(c, cudaEventRecord(c->consumed[i], c->stream), "copy events");
+    }
+  }
+  P2_TRY(c, cudaStreamWaitEvent(c->copy_stream, c->consumed[slot], 0), "copy wait");
+  const int T = c->T;
+  for (int f = 0; f < 2; f++) {
+    const p2_prop& p = f ? d : u;
+    if (p.location != P2_HOST) continue;
+    DevBuf& stage = f ? c->stage_d2[slot] : c->stage_u2[slot];
+    const size_t esz = p.precision == P2_FP64 ? 16 : 8;
+    const int j0 = ((ch.t_begin - p.t_first) % T + T) % T;
+    P2_TRY(c, stage.ensure((size_t)144 * ch.n * c->V3 * esz), "staging alloc");
+    const size_t width = (size_t)ch.n * c->V3 * esz;
+    P2_TRY(c,
+           cudaMemcpy2DAsync(stage.p, width, (const char*)p.data + (size_t)j0 * c->V3 * esz,
+                             (size_t)p.nt * c->V3 * esz, width, 144, cudaMemcpyHostToDevice, c->copy_stream),
+           "host propagator upload");
+  }
+  P2_TRY(c, cudaEventRecord(c->copied[slot], c->copy_stream), "copy event");
+  return P2_OK;
+}
+
+p2_status Uploader::view(int slot, const Chunk& ch, p2::ContractArgs& a) {
+  for (int f = 0; f < 2; f++) {
+    const p2_prop& p = f ? d : u;
+    const void* ptr = p.data;
+    long long vol = c->V3 * p.nt;
+    int t_first = p.t_first;
+    if (p.location == P2_HOST) {
+      ptr = (f ? c->stage_d2[slot] : c->stage_u2[slot]).p;
+      vol = c->V3 * ch.n;
+      t_first = ch.t_begin;
+    }
+    if (f) {
+      a.d = ptr;
+      a.vol_d = vol;
+      a.t_first_d = t_first;
+    } else {
+      a.u = ptr;
+      a.vol_u = vol;
+      a.t_first_u = t_first;
+    }
+  }
+  if (host) P2_TRY(c, cudaStreamWaitEvent(c->stream, c->copied[slot], 0), "compute wait");
+  return P2_OK;
+}
+
+p2_status Uploader::release(int slot) {
+  if (host) P2_TRY(c, cudaEventRecord(c->consumed[slot], c->stream), "consume event");
+  return P2_OK;
+}
+
 p2_status make_plan(p2_ctx* c, const p2_request& r, Plan& pl) {
   if (r.contractions == 0 || (r.contractions & ~kAllBits))
     return c->fail(P2_ERR_INVALID_ARG, "contractions: empty or unknown bits");
@@ -202,71 +277,72 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request& r, const 
 
   const int ptiles = (pl.nmom + 63) / 64;
   const int ktiles = (pl.K + 95) / 96;
-  for (const TauRun& run : local_runs(c, u, d, r.source, r.totalT)) {
-    for (int off = 0; off < run.n; off += tc) {
-      const int n = std::min(tc, run.n - off);
-      const int tau0 = run.tau0 + off;
-      p2::ContractArgs a{};
-      const int t_begin = (r.source[3] + tau0) % c->T;
-      p2_status s = chunk_view(c, u, c->stage_u, t_begin, n, a, true);
-      if (s != P2_OK) return s;
-      s = chunk_view(c, d, c->stage_d, t_begin, n, a, false);
-      if (s != P2_OK) return s;
-      a.V3 = (int)c->V3;
-      a.T = c->T;
-      a.t0 = r.source[3];
-      a.tau0 = tau0;
-      a.ntau = n;
-      a.what = r.contractions;
-      a.K = pl.K;
-      a.k = offsets_of(r.contractions);
-      a.out = c->cbuf.p;
-      {
-        ProfScope ps(c, "contract_plain_fp64");
-        P2_TRY(c, p2::launch_contract_plain(a, c->nsm, c->stream), "contract kernel");
-      }
+  const std::vector<Chunk> chunks = make_chunks(c, local_runs(c, u, d, r.source, r.totalT), r.source, tc);
+  Uploader up(c, u, d);
+  for (size_t i = 0; i < chunks.size() && i < 2; i++) {
+    p2_status s = up.issue((int)i, chunks[i]);
+    if (s != P2_OK) return s;
+  }
+  for (size_t i = 0; i < chunks.size(); i++) {
+    const Chunk& ch = chunks[i];
+    const int slot = (int)(i & 1);
+    const int n = ch.n, tau0 = ch.tau0;
+    p2::ContractArgs a{};
+    p2_status s = up.view(slot, ch, a);
+    if (s != P2_OK) return s;
+    a.V3 = (int)c->V3;
+    a.T = c->T;
+    a.t0 = r.source[3];
+    a.tau0 = tau0;
+    a.ntau = n;
+    a.what = r.contractions;
+    a.K = pl.K;
+    a.k = offsets_of(r.contractions);
+    a.out = c->cbuf.p;
+    {
+      ProfScope ps(c, "contract_plain_fp64");
+      P2_TRY(c, p2::launch_contract_plain(a, c->nsm, c->stream), "contract kernel");
+    }
+    if ((s = up.release(slot)) != P2_OK) return s;
+    if (i + 2 < chunks.size() && (s = up.issue(slot, chunks[i + 2])) != P2_OK) return s;
 
-      p2::ProjArgs pa{};
-      pa.c = c->cbuf.p;
-      pa.sT = (long long)pl.K * c->V3;
-      pa.sK = c->V3;
-      pa.ntau = n;
-      pa.K = pl.K;
-      pa.V3 = (int)c->V3;
-      pa.nmom = pl.nmom;
-      pa.Lx = c->Ll[0];
-      pa.Ly = c->Ll[1];
-      pa.Lz = c->Ll[2];
-      pa.Lmax = pl.Lmax;
-      pa.tab = (const double*)c->tab.p;
-      int nsplit = (2 * c->nsm + ptiles * ktiles * n - 1) / (ptiles * ktiles * n);
-      nsplit = std::max(1, std::min(nsplit, (int)((c->V3 + 255) / 256)));
-      pa.chunk = (int)((((c->V3 + nsplit - 1) / nsplit) + 15) / 16 * 16);
-      pa.nsplit = (int)((c->V3 + pa.chunk - 1) / pa.chunk);
-      P2_TRY(c, c->part.ensure((size_t)n * pa.nsplit * pl.nmom * pl.K * 16), "partials alloc");
-      pa.part = (double*)c->part.p;
-      {
-        ProfScope ps(c, "project_fp64");
-        P2_TRY(c, p2::launch_project_fp64(pa, c->stream), "projection kernel");
-      }
-
-      p2::ScatterArgs sa{};
-      sa.part = (const double*)c->part.p;
-      sa.ntau = n;
-      sa.nsplit = pa.nsplit;
-      sa.nmom = pl.nmom;
-      sa.K = pl.K;
-      sa.tau0 = tau0;
-      sa.totalT = r.totalT;
-      sa.nblocks = (int)pl.blocks.size();
-      for (size_t b = 0; b < pl.blocks.size(); b++) sa.blk[b] = pl.blocks[b];
-      sa.out = dres;
-      {
-        ProfScope ps(c, "reduce_scatter");
-        P2_TRY(c, p2::launch_scatter(sa, c->stream), "reduction kernel");
-      }
-      if (u.location == P2_HOST || d.location == P2_HOST)
-        P2_TRY(c, cudaStreamSynchronize(c->stream), "staging reuse");
+    p2::ProjArgs pa{};
+    pa.c = c->cbuf.p;
+    pa.sT = (long long)pl.K * c->V3;
+    pa.sK = c->V3;
+    pa.ntau = n;
+    pa.K = pl.K;
+    pa.V3 = (int)c->V3;
+    pa.nmom = pl.nmom;
+    pa.Lx = c->Ll[0];
+    pa.Ly = c->Ll[1];
+    pa.Lz = c->Ll[2];
+    pa.Lmax = pl.Lmax;
+    pa.tab = (const double*)c->tab.p;
+    int nsplit = (2 * c->nsm + ptiles * ktiles * n - 1) / (ptiles * ktiles * n);
+    nsplit = std::max(1, std::min(nsplit, (int)((c->V3 + 255) / 256)));
+    pa.chunk = (int)((((c->V3 + nsplit - 1) / nsplit) + 15) / 16 * 16);
+    pa.nsplit = (int)((c->V3 + pa.chunk - 1) / pa.chunk);
+    P2_TRY(c, c->part.ensure((size_t)n * pa.nsplit * pl.nmom * pl.K * 16), "partials alloc");
+    pa.part = (double*)c->part.p;
+    {
+      ProfScope ps(c, "project_fp64");
+      P2_TRY(c, p2::launch_project_fp64(pa, c->stream), "projection kernel");
+    }
+    p2::ScatterArgs sa{};
+    sa.part = (const double*)c->part.p;
+    sa.ntau = n;
+    sa.nsplit = pa.nsplit;
+    sa.nmom = pl.nmom;
+    sa.K = pl.K;
+    sa.tau0 = tau0;
+    sa.totalT = r.totalT;
+    sa.nblocks = (int)pl.blocks.size();
+    for (size_t b = 0; b < pl.blocks.size(); b++) sa.blk[b] = pl.blocks[b];
+    sa.out = dres;
+    {
+      ProfScope ps(c, "reduce_scatter");
+      P2_TRY(c, p2::launch_scatter(sa, c->stream), "reduction kernel");
     }
   }
   return P2_OK;
@@ -407,6 +483,13 @@ p2_status p2_ctx_destroy(p2_ctx* c) {
   }
   cudaStreamSynchronize(c->stream);
   for (DevBuf* b : {&c->cbuf, &c->part, &c->tab, &c->res, &c->stage_u, &c->stage_d, &c->scratch}) b->release();
+  for (int i = 0; i < 2; i++) {
+    c->stage_u2[i].release();
+    c->stage_d2[i].release();
+    if (c->copied[i]) cudaEventDestroy(c->copied[i]);
+    if (c->consumed[i]) cudaEventDestroy(c->consumed[i]);
+  }
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   c->prof_collect();
   for (auto& p : c->prof)
     for (cudaEvent_t e : p.pool) cudaEventDestroy(e);

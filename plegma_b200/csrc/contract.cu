@@ -76,13 +76,20 @@ template <typename R>
 struct Writer {
   Cx<R>* out;
   long long V3;
-  int* smax;  // split form: per-component running max (float bits), or null
+  int* smax;    // split form: per-component running max (float bits), or null
+  float* rmax;  // split form: this lane's running maxima of its nucleon (2) and G16 (16) outputs
   __device__ __forceinline__ void put(int k, Cx<R> v) const {
     out[(long long)k * V3] = v;
     if (smax) {
       const float m = fmaxf(fabsf((float)v.x), fabsf((float)v.y));
       atomicMax(smax + k, __float_as_int(m));
     }
+  }
+  // Outputs whose component is fixed per lane: the maximum stays in a register
+  // (slot) and reaches shared memory once per time slice.
+  __device__ __forceinline__ void put_slot(int k, Cx<R> v, int slot) const {
+    out[(long long)k * V3] = v;
+    if (rmax) rmax[slot] = fmaxf(rmax[slot], fmaxf(fabsf((float)v.x), fabsf((float)v.y)));
   }
 };
 
@@ -116,17 +123,17 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Cx<R>
     return;
   }
   if (a.what & 1u) {
-    const Cx<R> p = nucleon_site<R>(U, D, lt, l, mask);
-    const Cx<R> n = nucleon_site<R>(D, U, lt, l, mask);
-    w.put(a.k.nuc + l, p);
-    w.put(a.k.nuc + 16 + l, n);
+    Cx<R> pn[2];
+    nucleon_site<R>(U, D, lt, l, mask, pn);
+    w.put_slot(a.k.nuc + l, pn[0], 0);
+    w.put_slot(a.k.nuc + 16 + l, pn[1], 1);
   }
   if (a.what & (8u | 16u | 32u)) {
     Cx<R> c[16];
     meson_site<R>(U, D, lt, l, mask, c);
     if (a.what & 8u) {
 #pragma unroll
-      for (int g2 = 0; g2 < 16; g2++) w.put(a.k.g16 + l * 16 + g2, c[g2]);
+      for (int g2 = 0; g2 < 16; g2++) w.put_slot(a.k.g16 + l * 16 + g2, c[g2], 2 + g2);
     }
     if (a.what & 16u) {
       if (l == 0) w.put(a.k.all34 + 0, c[0]);
@@ -186,7 +193,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
     const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + hw;
     if (x < a.V3) {
       const Cx<double>* U = st + hw * kRow;
-      Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr};
+      Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr, nullptr};
       contract_site<double, DELTA>(a, U, U + 144, lt, l, mask, w);
     }
     __syncthreads();
@@ -195,12 +202,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
   cp_async_wait<0>();
 }
 
-// Split form: FP32 arithmetic on power-of-two scaled inputs.
+// Split form: FP32 arithmetic on power-of-two scaled inputs.  One staging
+// buffer in the input precision plus an FP32 copy of the tile: the staging
+// buffer is refilled with the next tile's cp.async as soon as the current one
+// is converted, so two CTAs (16 warps) fit on an SM.
 template <typename Tin, bool DELTA>
-__global__ void __launch_bounds__(kThreads, 1) k_contract_f32(const ContractArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Cx<Tin>* sm = (Cx<Tin>*)smem_raw;
-  Cx<float>* sf = (Cx<float>*)(smem_raw + 2 * kStage * sizeof(Cx<Tin>));
+  Cx<Tin>* st = (Cx<Tin>*)smem_raw;
+  Cx<float>* sf = (Cx<float>*)(smem_raw + kStage * sizeof(Cx<Tin>));
   int* smax = (int*)(sf + kStage);
   const int tid = threadIdx.x;
   const int hw = tid >> 4, l = tid & 15;
@@ -212,14 +222,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_f32(const ContractArgs
   long long tile = blockIdx.x;
   for (int k = tid; k < a.K; k += kThreads) smax[k] = 0;
 
-  issue_tile<Tin>(a, sm, tile, ntiles, tiles_per_tau);
-  issue_tile<Tin>(a, sm + kStage, tile + gridDim.x, ntiles, tiles_per_tau);
+  issue_tile<Tin>(a, st, tile, ntiles, tiles_per_tau);
 
   int cur = -1;  // slice whose maxima smax holds
-  for (int it = 0; tile < ntiles; tile += gridDim.x, it++) {
-    Cx<Tin>* st = sm + (it & 1) * kStage;
+  float rmax[18];
+#pragma unroll
+  for (int i = 0; i < 18; i++) rmax[i] = 0.f;
+  // lane maxima -> shared (the two half-warps of a warp own the same components)
+  auto flush_lane = [&]() {
+#pragma unroll
+    for (int i = 0; i < 18; i++) {
+      const float m = fmaxf(rmax[i], __shfl_xor_sync(0xffffffffu, rmax[i], 16));
+      rmax[i] = 0.f;
+      if (!(tid & 16)) {
+        int k = -1;
+        if (i < 2 && (a.what & 1u)) k = a.k.nuc + 16 * i + l;
+        if (i >= 2 && (a.what & 8u)) k = a.k.g16 + l * 16 + (i - 2);
+        if (k >= 0) atomicMax(smax + k, __float_as_int(m));
+      }
+    }
+  };
+  for (; tile < ntiles; tile += gridDim.x) {
     const int tl = (int)(tile / tiles_per_tau);
-    cp_async_wait<1>();
+    if (tl != cur && cur >= 0) flush_lane();
+    cp_async_wait<0>();
     __syncthreads();
     if (tl != cur) {
       if (cur >= 0)
@@ -231,34 +257,31 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_f32(const ContractArgs
     }
     // scale by 2^-E per flavour and convert to FP32 once per tile
     {
-      const int eu = a.exp_u[tl], ed = a.exp_d[tl];
+      // exact power-of-two scales; products are formed in double so that no
+      // intermediate leaves the representable range
+      const double su = ldexp(1.0, -a.exp_u[tl]), sd = ldexp(1.0, -a.exp_d[tl]);
       for (int i = tid; i < kSitesPerTile * 288; i += kThreads) {
         const int s = i / 288, c = i - s * 288;
         const Cx<Tin> v = st[s * kRow + c];
-        const int e = c < 144 ? eu : ed;
+        const double sc = c < 144 ? su : sd;
         Cx<float> f;
-        if (sizeof(Tin) == 8) {
-          f.x = (float)scalbn((double)v.x, -e);
-          f.y = (float)scalbn((double)v.y, -e);
-        } else {
-          f.x = scalbnf((float)v.x, -e);
-          f.y = scalbnf((float)v.y, -e);
-        }
+        f.x = (float)((double)v.x * sc);
+        f.y = (float)((double)v.y * sc);
         sf[s * kRow + c] = f;
       }
     }
     __syncthreads();
-    // the staged tile has been converted: refill this stage while contracting
-    issue_tile<Tin>(a, st, tile + 2LL * gridDim.x, ntiles, tiles_per_tau);
+    // the staged tile has been converted: refill the staging buffer while contracting
+    issue_tile<Tin>(a, st, tile + gridDim.x, ntiles, tiles_per_tau);
     const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + hw;
     if (x < a.V3) {
       const Cx<float>* U = sf + hw * kRow;
-      Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, smax};
+      Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, smax, rmax};
       contract_site<float, DELTA>(a, U, U + 144, lt, l, mask, w);
     }
-    __syncthreads();
   }
   cp_async_wait<0>();
+  if (cur >= 0) flush_lane();
   __syncthreads();
   if (cur >= 0)
     for (int k = tid; k < a.K; k += kThreads) atomicMax(a.cmax + (long long)cur * a.K + k, smax[k]);
@@ -322,7 +345,7 @@ cudaError_t launch_plain_t(const ContractArgs& a, int grid, cudaStream_t s) {
 
 template <typename Tin, bool DELTA>
 cudaError_t launch_f32_t(const ContractArgs& a, int grid, cudaStream_t s) {
-  const int smem = 2 * kStage * (int)sizeof(Cx<Tin>) + kStage * (int)sizeof(Cx<float>) + a.K * (int)sizeof(int);
+  const int smem = kStage * (int)sizeof(Cx<Tin>) + kStage * (int)sizeof(Cx<float>) + a.K * (int)sizeof(int);
   cudaError_t e = cudaFuncSetAttribute(k_contract_f32<Tin, DELTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   k_contract_f32<Tin, DELTA><<<grid, kThreads, smem, s>>>(a);

@@ -52,6 +52,11 @@ struct p2_ctx {
   bool host_only = false;  // created with device < 0
   std::string err = "no error";
   p2host::DevBuf cbuf, part, tab, res, stage_u, stage_d, scratch;
+  // host-resident propagators: two staging slots per flavour, uploaded on a
+  // copy stream while the previous chunk is contracted
+  p2host::DevBuf stage_u2[2], stage_d2[2];
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
   // split form: phase tiles, per-slice exponents, component maxima, tables, partials, error flag
   p2host::DevBuf phaseA, expb, cmaxb, momrow, kexp, fpart, rowtab, errflag;
   int project_split_smem_max = 0;  // opt-in shared memory per block of the device
@@ -116,6 +121,28 @@ struct Plan {
   std::vector<int> moms;
   std::vector<p2::ScatterBlock> blocks;
   size_t total;  // complex elements of the result
+};
+
+// A chunk of consecutive source-relative times processed by one launch sequence.
+struct Chunk {
+  int tau0, n, t_begin;
+};
+
+// Splits the local time runs of a request into chunks of at most `tc` slices.
+std::vector<Chunk> make_chunks(const p2_ctx* c, const std::vector<TauRun>& runs, const int* src, int tc);
+
+// Device views of (u, d) for each chunk.  Device propagators are used in
+// place; host propagators are uploaded into two staging slots on a copy
+// stream, so chunk i+1 crosses PCIe while chunk i is contracted.
+struct Uploader {
+  p2_ctx* c;
+  const p2_prop& u;
+  const p2_prop& d;
+  bool host;
+  Uploader(p2_ctx* ctx, const p2_prop& pu, const p2_prop& pd);
+  p2_status issue(int slot, const Chunk& ch);                    // start the upload of a chunk
+  p2_status view(int slot, const Chunk& ch, p2::ContractArgs& a);  // views for the compute stream
+  p2_status release(int slot);                                   // the chunk's kernels are queued
 };
 
 int components_of(unsigned what);

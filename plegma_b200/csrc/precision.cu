@@ -162,14 +162,18 @@ p2_status run_one(p2_ctx* c, const p2_prop* props, const p2_request& r) {
   P2_TRY(c, c->expb.ensure((size_t)2 * tc * sizeof(int)), "exponent alloc");
   P2_TRY(c, c->cmaxb.ensure((size_t)tc * K * sizeof(int)), "maxima alloc");
 
-  for (const TauRun& run : local_runs(c, u, d, r.source, r.totalT)) {
-    for (int off = 0; off < run.n; off += tc) {
-      const int n = std::min(tc, run.n - off);
-      const int tau0 = run.tau0 + off;
-      const int t_begin = (r.source[3] + tau0) % c->T;
+  const std::vector<Chunk> chunks = make_chunks(c, local_runs(c, u, d, r.source, r.totalT), r.source, tc);
+  Uploader up(c, u, d);
+  for (size_t i = 0; i < chunks.size() && i < 2; i++)
+    if ((st = up.issue((int)i, chunks[i])) != P2_OK) return st;
+  for (size_t ci = 0; ci < chunks.size(); ci++) {
+    {
+      const Chunk& ch = chunks[ci];
+      const int slot = (int)(ci & 1);
+      const int n = ch.n;
+      const int tau0 = ch.tau0;
       p2::ContractArgs a{};
-      if ((st = chunk_view(c, u, c->stage_u, t_begin, n, a, true)) != P2_OK) return st;
-      if ((st = chunk_view(c, d, c->stage_d, t_begin, n, a, false)) != P2_OK) return st;
+      if ((st = up.view(slot, ch, a)) != P2_OK) return st;
       int* eu = (int*)c->expb.p;
       int* ed = eu + tc;
       {
@@ -194,8 +198,10 @@ p2_status run_one(p2_ctx* c, const p2_prop* props, const p2_request& r) {
       a.cmax = (int*)c->cmaxb.p;
       {
         ProfScope ps(c, "contract_f32");
-        P2_TRY(c, p2::launch_contract_f32(a, fp32_in, c->nsm, c->stream), "contract kernel");
+        P2_TRY(c, p2::launch_contract_f32(a, fp32_in, 2 * c->nsm, c->stream), "contract kernel");
       }
+      if ((st = up.release(slot)) != P2_OK) return st;
+      if (ci + 2 < chunks.size() && (st = up.issue(slot, chunks[ci + 2])) != P2_OK) return st;
       // projection GEMM: enough CTAs for about two waves
       const int per = ntile * nmtile * n;
       int nsplit = std::max(1, (2 * c->nsm + per - 1) / per);
@@ -246,8 +252,6 @@ p2_status run_one(p2_ctx* c, const p2_prop* props, const p2_request& r) {
         ProfScope ps(c, "split_reduce");
         P2_TRY(c, p2::launch_split_reduce(rd, c->stream), "split reduction");
       }
-      if (u.location == P2_HOST || d.location == P2_HOST)
-        P2_TRY(c, cudaStreamSynchronize(c->stream), "staging reuse");
     }
   }
   if (r.out_location == P2_HOST) {

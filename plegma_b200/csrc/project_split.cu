@@ -34,7 +34,7 @@ namespace p2 {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;  // 16 warps: producers of B (all), TMA/MMA issue (thread 0), epilogue
 constexpr int kKS = 64;                   // sites per k-step
 constexpr int kATile = 128 * kKS * 2;     // bytes of one 128 x 64 FP16 tile
 
@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
   constexpr int NM = NR / NH;
   constexpr uint32_t IDESC = tc::idesc_f16_f32(128, NM);
   constexpr int TCOLS = tmem_cols(NT);
-  constexpr int JN = NT / 8;                 // components per producer thread
+  constexpr int JN = NT / 16;                // components per producer thread
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // the dynamic window is only guaranteed 16-byte aligned: round up to 1024
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -115,12 +115,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
   tc::tc_fence_after();
   const uint32_t tmem = *tslot;
 
-  // producer role: site pair sp (sites 2sp, 2sp+1 of the k-step), components kg + 8j
+  // producer role: site pair sp (sites 2sp, 2sp+1 of the k-step), components kg + 16j
   const int sp = tid & 31, kg = tid >> 5;
   float sc[JN];
 #pragma unroll
   for (int j = 0; j < JN; j++) {
-    const int k = k0 + kg + 8 * j;
+    const int k = k0 + kg + 16 * j;
     sc[j] = 0.f;
     if (k < a.K) {
       const float mx = __int_as_float(a.cmax[(long long)tau * a.K + k]);
@@ -134,9 +134,29 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
 
   int issued = -1;  // last k-step whose phase copy thread 0 issued
   bool failed = false;
+  // B values of the current k-step and the next one (register double buffer:
+  // the global loads of step i+1 are in flight while step i is split and fed
+  // to the tensor cores)
+  Cx<float> cur[JN][2], nxt[JN][2];
+  auto load_b = [&](int ks, Cx<float> (&r)[JN][2]) {
+    const long long x = (long long)ks * kKS + 2 * sp;
+#pragma unroll
+    for (int j = 0; j < JN; j++) {
+      const int k = k0 + kg + 16 * j;
+      r[j][0] = czero<float>();
+      r[j][1] = czero<float>();
+      if (k < a.K) {
+        const Cx<float>* src = cb + (long long)k * a.V3 + x;
+        if (x < a.V3) r[j][0] = src[0];
+        if (x + 1 < a.V3) r[j][1] = src[1];
+      }
+    }
+  };
+  if (nk > 0) load_b(ks0, cur);
   for (int i = 0; i < nk; i++) {
     const int s = i & 1;
     unsigned char* st = smem + s * ST;
+    if (i + 1 < nk) load_b(ks0 + i + 1, nxt);
     bool bad = false;
     if (i >= 2) bad = !tc::mbar_wait(&done[s], ((i >> 1) - 1) & 1);
     if (__syncthreads_or(bad || *flag)) {
@@ -152,17 +172,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
     // B: split c into hi/lo FP16, Re and Im rows per component
     unsigned char* Bh = st + 2 * kATile;
     unsigned char* Bl = Bh + BT;
-    const long long x = (long long)ks * kKS + 2 * sp;
 #pragma unroll
     for (int j = 0; j < JN; j++) {
-      const int kk = kg + 8 * j;
-      const int k = k0 + kk;
-      Cx<float> v0 = czero<float>(), v1 = czero<float>();
-      if (k < a.K) {
-        const Cx<float>* src = cb + (long long)k * a.V3 + x;
-        if (x < a.V3) v0 = src[0];
-        if (x + 1 < a.V3) v1 = src[1];
-      }
+      const int kk = kg + 16 * j;
+      const Cx<float> v0 = cur[j][0], v1 = cur[j][1];
       const float r0 = v0.x * sc[j], i0 = v0.y * sc[j], r1 = v1.x * sc[j], i1 = v1.y * sc[j];
       const __half2 hr = __floats2half2_rn(r0, r1);
       const __half2 hi_ = __floats2half2_rn(i0, i1);
@@ -175,6 +188,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
       *(__half2*)(Bh + oim) = hi_;
       *(__half2*)(Bl + ore) = lr;
       *(__half2*)(Bl + oim) = li;
+    }
+#pragma unroll
+    for (int j = 0; j < JN; j++) {
+      cur[j][0] = nxt[j][0];
+      cur[j][1] = nxt[j][1];
     }
     tc::fence_proxy_async_smem();
     __syncthreads();
@@ -215,13 +233,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
     if (tid == 0) atomicExch(a.err, 1);
   } else {
     tc::tc_fence_after();
-    // epilogue: warps w and w+4 share TMEM lanes 32*(w%4).., half the columns each
+    // epilogue: warps w, w+4, w+8, w+12 share TMEM lanes 32*(w%4)..; 16-column
+    // chunks are dealt round-robin among them
     const int row = 32 * (warp & 3) + lane;
-    const int c0 = (warp >> 2) * (NR / 2);
     float* dst = a.part + ((((long long)tau * a.nsplit + split) * a.nmtile + mt) * 128 + row) * (long long)(a.ntile * NR) +
                  nti * NR;
 #pragma unroll 1
-    for (int c = c0; c < c0 + NR / 2; c += 16) {
+    for (int c = (warp >> 2) * 16; c < NR; c += 64) {
       float v[16];
       tc::tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c, v);
       float4* d4 = (float4*)(dst + c);

@@ -2,22 +2,28 @@
 //
 // The reference evaluates every output component of a site in one thread,
 // unfactorised (lib/kernels/PLEGMA_baryons_NtoN.cu:6-46: 16 (mu,mu') x 16 spin
-// terms x 36 colour terms; PLEGMA_mesonsAll.cuh:34-82: 9 colour products per
-// spin term per Gamma pair).  Here the same sums are regrouped so that the
-// 16 lanes of a half-warp share one site and every lane does an equal share:
+// terms x 36 colour terms; PLEGMA_baryons_deltas.cu:7-110 likewise with 8 or 6
+// Wick terms; PLEGMA_mesonsAll.cuh:34-82: 9 colour products per spin term per
+// Gamma pair).  Here the same sums are regrouped so that the 16 lanes of a
+// half-warp share one site and every lane does an equal share.
 //
-// Nucleon C g5 (per dataset, A = doubly represented flavour, B = the other):
-//   tmp[mu][mu'] = sum_idx val_idx sum_{eps eps'} B[lam lam'][b b']
-//                  ( A[nu nu'][a a'] A[mu mu'][c c'] - A[nu mu'][a c'] A[mu nu'][c a'] )
-//   direct   : Q[c][c'] = sum_idx val sum_{a,a'} eps eps' A[nu nu'][a a'] B[lam lam'][b b']
-//              (lane = idx, 36 complex products, butterfly over the 16 lanes),
-//              then T1[mu][mu'] = sum_{c c'} Q[c][c'] A[mu mu'][c c'].
-//   exchange : Z[c][a'] = sum_{(nu,lam)} val sum_{a,c'} eps eps' B[lam lam'][b b'] A[nu mu'][a c']
-//              (lane = ((lam',nu'), mu'), 144 products, no reduction), then
-//              P[mu] = sum_{c a'} Z[c][a'] A[mu nu'][c a'] and T2 = sum over the
-//              four nu' lanes (two shuffle levels).
-//   Per site and dataset: 3600 complex products instead of the reference's
-//   ~1.1e5.
+// Baryons (nucleon C g5, Delta C g_k).  Every Wick term is a product of three
+// propagator lines X[nu][s1'] Y[lam][s2'] Z[mu][s3'] with the sink diquark
+// (nu, lam) contracted with Gamma and the source spins (s1', s2', s3') a
+// permutation of (nu', lam', mu') (lam', nu' contracted with Gamma-bar).
+// Summing the sink diquark first gives, on lane (x', y') = (l >> 2, l & 3),
+//   G^{XY}[c][e] = sum_{(nu,lam)} sA sum eps_abc eps_{c1 c2 e} X[nu][x'][a][c1] Y[lam][y'][b][c2]
+// (144 complex products per lane), and every term is +-G contracted with Z:
+//   mu' on X's source slot (slot 1): P[m] = f1 sum G[c][e] Z[m][z1][c][e], summed over y'
+//   mu' on Y's source slot (slot 2): P[m] = f2 sum G[c][e] Z[m][z2][c][e], summed over x'
+//   mu' on Z (type a):                D = sum over the 16 lanes of fa G, T = sum D Z[mu][mu']
+// with f1 = -(c1A sA1 - c1B sB1), f2 = c2A sA2 - c2B sB2, fa = cN sN - cL sL from
+// per-lane descriptors (spin.diquark_lane_tables) and the Wick coefficients c.
+// Swapping the two diquark lines transposes the lanes: G^{YX}(y',x') =
+// sign G^{XY}(x',y'), sign -1 for C g5 (antisymmetric), +1 for C g_k.
+//   nucleon, per dataset: direct term = type a (cN = 1), exchange = slot 1 (c1A = -1)
+//   -> 144 + 45 products per lane for the first dataset, 45 for the second;
+//   the reference spends ~1.1e5 per site and dataset.
 //
 // Mesons, all 16 x 16 (G_sink, G_src):
 //   C[g1][g2] = sum G1[d][a] A[a][b] G2[b][z] conj(B[d][z]) over spin and colour.
@@ -29,36 +35,43 @@
 
 namespace p2 {
 
+// Source-side descriptor of a diquark table for lane (x' = l >> 2, y' = l & 3).
+struct DiquarkLane {
+  int z1, sA1, sB1, z2, sA2, sB2, sN, sL;
+};
+
 // Per-lane copies of the table entries a lane needs with a lane-dependent index.
 struct LaneTables {
-  // nucleon table entry idx = lane: (nu, lam, lam', nu') and value
-  int nu, lu, lup, nup, val;
-  // exchange stage: lane = (iB = lane >> 2, mu' = lane & 3)
-  int xlup, xnup;
-  int xval[4];  // val(iA, iB) for iA = 0..3
+  DiquarkLane nuc;  // nucleon C g5 descriptor
   // meson stage: lane = g1, row d of G_g1: column pi1(d) and value
   int gsrc[4];  // source lane pi1(d)*4 + d
   int gre[4], gim[4];
 };
 
-__constant__ int c_nuc_idx[16][4] = P2_INIT_NucIdx;
-__constant__ int c_nuc_val[16] = P2_INIT_NucVal;
 __constant__ int c_gamma_perm[16][4] = P2_INIT_GammaPerm;
 __constant__ int c_gamma_re[16][4] = P2_INIT_GammaRe;
 __constant__ int c_gamma_im[16][4] = P2_INIT_GammaIm;
+__constant__ int c_nuc_sink[4][3] = P2_INIT_NucSink;
+__constant__ int c_nuc_lane[16][8] = P2_INIT_NucLane;
+__constant__ int c_delta_sink[3][4][3] = P2_INIT_DeltaSink;
+__constant__ int c_delta_lane[3][16][8] = P2_INIT_DeltaLane;
+
+__device__ __forceinline__ DiquarkLane load_diquark_lane(const int (*t)[8], int l) {
+  DiquarkLane d;
+  d.z1 = t[l][0];
+  d.sA1 = t[l][1];
+  d.sB1 = t[l][2];
+  d.z2 = t[l][3];
+  d.sA2 = t[l][4];
+  d.sB2 = t[l][5];
+  d.sN = t[l][6];
+  d.sL = t[l][7];
+  return d;
+}
 
 __device__ __forceinline__ LaneTables load_lane_tables(int l) {
   LaneTables t;
-  t.nu = c_nuc_idx[l][0];
-  t.lu = c_nuc_idx[l][1];
-  t.lup = c_nuc_idx[l][2];
-  t.nup = c_nuc_idx[l][3];
-  t.val = c_nuc_val[l];
-  const int iB = l >> 2;
-  t.xlup = c_nuc_idx[iB][2];
-  t.xnup = c_nuc_idx[iB][3];
-#pragma unroll
-  for (int iA = 0; iA < 4; iA++) t.xval[iA] = c_nuc_val[iA * 4 + iB];
+  t.nuc = load_diquark_lane(c_nuc_lane, l);
 #pragma unroll
   for (int d = 0; d < 4; d++) {
     t.gsrc[d] = c_gamma_perm[l][d] * 4 + d;
@@ -68,108 +81,113 @@ __device__ __forceinline__ LaneTables load_lane_tables(int l) {
   return t;
 }
 
+// G^{XY} for lane (x', y') and a sink table sink[iA] = (nu, lam, sA).
 template <typename R>
-__device__ __forceinline__ Cx<R> ld(const Cx<R>* p, int i) {
-  return p[i];
-}
-
-// Nucleon C g5 for one dataset; returns tmp[lane >> 2][lane & 3].
-template <typename R>
-__device__ __forceinline__ Cx<R> nucleon_site(const Cx<R>* __restrict__ A, const Cx<R>* __restrict__ B,
-                                              const LaneTables& lt, int l, unsigned mask) {
-  // ---- direct term: Q[c][c'] ----
-  Cx<R> Q[3][3];
-  {
-    const Cx<R>* An = A + sblk(lt.nu, lt.nup);
-    const Cx<R>* Bl = B + sblk(lt.lu, lt.lup);
+__device__ __forceinline__ void diquark_G(const Cx<R>* __restrict__ X, const Cx<R>* __restrict__ Y,
+                                          const int (*sink)[3], int xp, int yp, Cx<R> q[9]) {
+#pragma unroll
+  for (int i = 0; i < 9; i++) q[i] = czero<R>();
+#pragma unroll 1
+  for (int iA = 0; iA < 4; iA++) {
+    const Cx<R>* Xb = X + sblk(sink[iA][0], xp);
+    const Cx<R>* Yb = Y + sblk(sink[iA][1], yp);
+    const R sgn = R(sink[iA][2]);
     Cx<R> a[9], b[9];
 #pragma unroll
     for (int i = 0; i < 9; i++) {
-      a[i] = An[i];
-      b[i] = Bl[i];
+      a[i] = cscale(Xb[i], sgn);
+      b[i] = Yb[i];
     }
-    const R v = R(lt.val);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
 #pragma unroll
-      for (int cp = 0; cp < 3; cp++) {
-        const int d1 = (cp + 1) % 3, d2 = (cp + 2) % 3;
-        Cx<R> q = czero<R>();
-        cmac(q, a[c1 * 3 + d1], b[c2 * 3 + d2]);
-        cmsub(q, a[c1 * 3 + d2], b[c2 * 3 + d1]);
-        cmsub(q, a[c2 * 3 + d1], b[c1 * 3 + d2]);
-        cmac(q, a[c2 * 3 + d2], b[c1 * 3 + d1]);
-        Q[c][cp] = cscale(q, v);
+      for (int e = 0; e < 3; e++) {
+        const int e1 = (e + 1) % 3, e2 = (e + 2) % 3;
+        Cx<R>& r = q[c * 3 + e];
+        cmac(r, a[c1 * 3 + e1], b[c2 * 3 + e2]);
+        cmsub(r, a[c1 * 3 + e2], b[c2 * 3 + e1]);
+        cmsub(r, a[c2 * 3 + e1], b[c1 * 3 + e2]);
+        cmac(r, a[c2 * 3 + e2], b[c1 * 3 + e1]);
       }
     }
   }
-#pragma unroll
-  for (int m = 1; m < 16; m <<= 1)
-#pragma unroll
-    for (int i = 0; i < 9; i++) Q[i / 3][i % 3] = Q[i / 3][i % 3] + shfl_xor16(Q[i / 3][i % 3], m, mask);
+}
 
+// G^{YX} from G^{XY}: move lane (y', x') to lane (x', y') with the table's sign.
+template <typename R>
+__device__ __forceinline__ void diquark_transpose(Cx<R> q[9], int l, unsigned mask, R sign) {
+  const int src = ((l & 3) << 2) | (l >> 2);
+#pragma unroll
+  for (int i = 0; i < 9; i++) q[i] = cscale(shfl_idx16(q[i], src, mask), sign);
+}
+
+// One group of Wick terms sharing G and the third line Z; returns the lane's
+// share of T[mu = l >> 2][mu' = l & 3].  S1, S2, TA select the term types present.
+template <typename R, bool S1, bool S2, bool TA>
+__device__ __forceinline__ Cx<R> diquark_eval(const Cx<R> g[9], const Cx<R>* __restrict__ Z, const DiquarkLane& dl,
+                                              int l, unsigned mask, int c1A, int c1B, int c2A, int c2B, int cN,
+                                              int cL) {
   const int mu = l >> 2, mup = l & 3;
-  Cx<R> T1 = czero<R>();
-  {
-    const Cx<R>* Am = A + sblk(mu, mup);
+  Cx<R> r = czero<R>();
+  if (S2) {
+    // slot 2 (reduce over x'): this lane's y' is mu'
+    const R f2 = R(c2A * dl.sA2 - c2B * dl.sB2);
+#pragma unroll 1
+    for (int m = 0; m < 4; m++) {
+      const Cx<R>* Z2 = Z + sblk(m, dl.z2);
+      Cx<R> p2 = czero<R>();
 #pragma unroll
-    for (int i = 0; i < 9; i++) cmac(T1, Q[i / 3][i % 3], Am[i]);
-  }
-
-  // ---- exchange term: lane = (iB, mu'') with mu'' = l & 3 ----
-  Cx<R> Z[9];
-#pragma unroll
-  for (int i = 0; i < 9; i++) Z[i] = czero<R>();
-  {
-    constexpr int NI[16][4] = P2_INIT_NucIdx;
-    const int mpp = l & 3;
-#pragma unroll
-    for (int iA = 0; iA < 4; iA++) {
-      const int nu = NI[iA * 4][0], lu = NI[iA * 4][1];
-      const Cx<R>* Bq = B + sblk(lu, lt.xlup);
-      const Cx<R>* Aq = A + sblk(nu, mpp);
-      Cx<R> a[9], b[9];
-#pragma unroll
-      for (int i = 0; i < 9; i++) {
-        a[i] = Aq[i];
-        b[i] = cscale(Bq[i], R(lt.xval[iA]));
-      }
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
-#pragma unroll
-        for (int ap = 0; ap < 3; ap++) {
-          const int e1 = (ap + 1) % 3, e2 = (ap + 2) % 3;
-          Cx<R>& z = Z[c * 3 + ap];
-          cmac(z, a[c1 * 3 + e2], b[c2 * 3 + e1]);
-          cmsub(z, a[c1 * 3 + e1], b[c2 * 3 + e2]);
-          cmsub(z, a[c2 * 3 + e2], b[c1 * 3 + e1]);
-          cmac(z, a[c2 * 3 + e1], b[c1 * 3 + e2]);
-        }
-      }
+      for (int i = 0; i < 9; i++) cmac(p2, g[i], Z2[i]);
+      p2 = cscale(p2, f2);
+      p2 = p2 + shfl_xor16(p2, 4, mask);
+      p2 = p2 + shfl_xor16(p2, 8, mask);
+      if (m == mu) r = r + p2;
     }
   }
-  Cx<R> P[4];
+  if (S1) {
+    // slot 1 (reduce over y'): T[.][mu'] sits on lane (x' = mu', y' = 0)
+    const R f1 = R(-(c1A * dl.sA1 - c1B * dl.sB1));
+    const int src = mup << 2;
+#pragma unroll 1
+    for (int m = 0; m < 4; m++) {
+      const Cx<R>* Z1 = Z + sblk(m, dl.z1);
+      Cx<R> p1 = czero<R>();
 #pragma unroll
-  for (int m = 0; m < 4; m++) {
-    const Cx<R>* Am = A + sblk(m, lt.xnup);
-    Cx<R> p = czero<R>();
-#pragma unroll
-    for (int i = 0; i < 9; i++) cmac(p, Z[i], Am[i]);
-    P[m] = p;
+      for (int i = 0; i < 9; i++) cmac(p1, g[i], Z1[i]);
+      p1 = cscale(p1, f1);
+      p1 = p1 + shfl_xor16(p1, 1, mask);
+      p1 = p1 + shfl_xor16(p1, 2, mask);
+      const Cx<R> v = shfl_idx16(p1, src, mask);
+      if (m == mu) r = r + v;
+    }
   }
+  if (TA) {
+    const R fa = R(cN * dl.sN - cL * dl.sL);
+    const Cx<R>* Zm = Z + sblk(mu, mup);
 #pragma unroll
-  for (int m = 0; m < 4; m++) {
-    P[m] = P[m] + shfl_xor16(P[m], 4, mask);
-    P[m] = P[m] + shfl_xor16(P[m], 8, mask);
+    for (int i = 0; i < 9; i++) {
+      Cx<R> d = cscale(g[i], fa);
+      d = d + shfl_xor16(d, 1, mask);
+      d = d + shfl_xor16(d, 2, mask);
+      d = d + shfl_xor16(d, 4, mask);
+      d = d + shfl_xor16(d, 8, mask);
+      cmac(r, d, Zm[i]);
+    }
   }
-  // lane (mu = l >> 2, mu' = l & 3) holds T2[m][mu'] for all m; pick m = mu.
-  Cx<R> T2 = P[0];
-  T2 = (mu == 1) ? P[1] : T2;
-  T2 = (mu == 2) ? P[2] : T2;
-  T2 = (mu == 3) ? P[3] : T2;
-  return T1 - T2;
+  return r;
+}
+
+// Nucleon C g5, both datasets: out[0] = proton (u u d), out[1] = neutron (d d u),
+// for lane (mu = l >> 2, mu' = l & 3).
+template <typename R>
+__device__ __forceinline__ void nucleon_site(const Cx<R>* __restrict__ U, const Cx<R>* __restrict__ D,
+                                             const LaneTables& lt, int l, unsigned mask, Cx<R> out[2]) {
+  Cx<R> g[9];
+  diquark_G<R>(U, D, c_nuc_sink, l >> 2, l & 3, g);  // G^{ud}
+  out[0] = diquark_eval<R, true, false, true>(g, U, lt.nuc, l, mask, -1, 0, 0, 0, 1, 0);
+  diquark_transpose<R>(g, l, mask, R(-1));  // G^{du}
+  out[1] = diquark_eval<R, true, false, true>(g, D, lt.nuc, l, mask, -1, 0, 0, 0, 1, 0);
 }
 
 // Generic meson block: lane g1 gets C[g1][g2] for g2 = 0..15 in out[].
@@ -215,153 +233,38 @@ __device__ __forceinline__ void meson_site(const Cx<R>* __restrict__ A, const Cx
 }
 
 // ---- Delta C g_k (PLEGMA_baryons_deltas.cu:7-110) ------------------------------
-//
-// All 14 Wick terms (8 of isospin 1/2, 6 of isospin 3/2) are products
-//   X[nu][s1'] Y[lam][s2'] Z[mu][s3']  (colours a, b, c at the sink; the source
-//   colour of a line follows its source spin slot),
-// with Gamma = C g_k on (nu, lam) and Gamma-bar on (lam', nu').  Summing the
-// sink diquark first gives, for the lane's source spins (x', y'),
-//   G^{XY}[c][e] = sum_{(nu,lam)} sA sum eps_abc eps_{c1 c2 e} X[nu][x'][a][c1] Y[lam][y'][b][c2]
-// (the same cofactor form as the nucleon's direct term), and every term is
-// +-G contracted with the third line:
-//   mu' on X's source slot (slot 1):  P[m] = f1 sum G[c][e] Z[m][z1][c][e], summed over y'
-//   mu' on Y's source slot (slot 2):  P[m] = f2 sum G[c][e] Z[m][z2][c][e], summed over x'
-//   mu' on Z (type a):                 D = sum over the 16 lanes of fa G, T = sum D Z[mu][mu']
-// with f1 = -(c1A sA1 - c1B sB1), f2 = c2A sA2 - c2B sB2, fa = cN sN - cL sL from the
-// per-lane descriptors (spin.diquark_lane_tables) and the Wick coefficients c.
-struct DeltaLane {
-  int z1, sA1, sB1, z2, sA2, sB2, sN, sL;
-};
-
-__constant__ int c_delta_lane[3][16][8] = P2_INIT_DeltaLane;
-
-__device__ __forceinline__ DeltaLane load_delta_lane(int g, int l) {
-  DeltaLane d;
-  d.z1 = c_delta_lane[g][l][0];
-  d.sA1 = c_delta_lane[g][l][1];
-  d.sB1 = c_delta_lane[g][l][2];
-  d.z2 = c_delta_lane[g][l][3];
-  d.sA2 = c_delta_lane[g][l][4];
-  d.sB2 = c_delta_lane[g][l][5];
-  d.sN = c_delta_lane[g][l][6];
-  d.sL = c_delta_lane[g][l][7];
-  return d;
-}
-
-__constant__ int c_delta_sink[3][4][3] = P2_INIT_DeltaSink;
-
-// G^{XY} for lane (x' = l >> 2, y' = l & 3) and table g (k = g + 1).
-template <typename R>
-__device__ __forceinline__ void delta_G(const Cx<R>* __restrict__ X, const Cx<R>* __restrict__ Y, int g, int xp,
-                                        int yp, Cx<R> q[9]) {
-#pragma unroll
-  for (int i = 0; i < 9; i++) q[i] = czero<R>();
-#pragma unroll 1
-  for (int iA = 0; iA < 4; iA++) {
-    const Cx<R>* Xb = X + sblk(c_delta_sink[g][iA][0], xp);
-    const Cx<R>* Yb = Y + sblk(c_delta_sink[g][iA][1], yp);
-    const R s = R(c_delta_sink[g][iA][2]);
-    Cx<R> a[9], b[9];
-#pragma unroll
-    for (int i = 0; i < 9; i++) {
-      a[i] = cscale(Xb[i], s);
-      b[i] = Yb[i];
-    }
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
-#pragma unroll
-      for (int e = 0; e < 3; e++) {
-        const int e1 = (e + 1) % 3, e2 = (e + 2) % 3;
-        Cx<R>& r = q[c * 3 + e];
-        cmac(r, a[c1 * 3 + e1], b[c2 * 3 + e2]);
-        cmsub(r, a[c1 * 3 + e2], b[c2 * 3 + e1]);
-        cmsub(r, a[c2 * 3 + e1], b[c1 * 3 + e2]);
-        cmac(r, a[c2 * 3 + e2], b[c1 * 3 + e1]);
-      }
-    }
-  }
-}
-
-// One group of Wick terms sharing G and the third line Z; returns the lane's
-// share of T[mu = l >> 2][mu' = l & 3].
-template <typename R>
-__device__ __forceinline__ Cx<R> delta_eval(const Cx<R> g[9], const Cx<R>* __restrict__ Z, const DeltaLane& dl, int l,
-                                            unsigned mask, int c1A, int c1B, int c2A, int c2B, int cN, int cL) {
-  const R f1 = R(-(c1A * dl.sA1 - c1B * dl.sB1));
-  const R f2 = R(c2A * dl.sA2 - c2B * dl.sB2);
-  const R fa = R(cN * dl.sN - cL * dl.sL);
-  const int mu = l >> 2, mup = l & 3;
-  Cx<R> r = czero<R>();
-  // slot 2 (reduce over x'): this lane's y' is mu'
-#pragma unroll 1
-  for (int m = 0; m < 4; m++) {
-    const Cx<R>* Z2 = Z + sblk(m, dl.z2);
-    Cx<R> p2 = czero<R>();
-#pragma unroll
-    for (int i = 0; i < 9; i++) cmac(p2, g[i], Z2[i]);
-    p2 = cscale(p2, f2);
-    p2 = p2 + shfl_xor16(p2, 4, mask);
-    p2 = p2 + shfl_xor16(p2, 8, mask);
-    if (m == mu) r = r + p2;
-  }
-  // slot 1 (reduce over y'): T[.][mu'] sits on lane (x' = mu', y' = 0)
-  const int src = mup << 2;
-#pragma unroll 1
-  for (int m = 0; m < 4; m++) {
-    const Cx<R>* Z1 = Z + sblk(m, dl.z1);
-    Cx<R> p1 = czero<R>();
-#pragma unroll
-    for (int i = 0; i < 9; i++) cmac(p1, g[i], Z1[i]);
-    p1 = cscale(p1, f1);
-    p1 = p1 + shfl_xor16(p1, 1, mask);
-    p1 = p1 + shfl_xor16(p1, 2, mask);
-    const Cx<R> v = shfl_idx16(p1, src, mask);
-    if (m == mu) r = r + v;
-  }
-  // type a
-  const Cx<R>* Zm = Z + sblk(mu, mup);
-#pragma unroll
-  for (int i = 0; i < 9; i++) {
-    Cx<R> d = cscale(g[i], fa);
-    d = d + shfl_xor16(d, 1, mask);
-    d = d + shfl_xor16(d, 2, mask);
-    d = d + shfl_xor16(d, 4, mask);
-    d = d + shfl_xor16(d, 8, mask);
-    cmac(r, d, Zm[i]);
-  }
-  return r;
-}
-
-// Delta C g_k, k = g + 1: out = {iso-1/2 Delta+ (u,u,d), iso-1/2 Delta0 (d,d,u),
-// iso-3/2 Delta++ (u,u,u), iso-3/2 Delta- (d,d,d)} for lane (mu, mu').
+// Wick coefficients (c1A, c1B, c2A, c2B, cN, cL) per G, read off the reference's
+// terms: with A the doubly represented flavour,
+//   isospin 1/2, G^{AA}, Z = B: (0, 2, 0, -2, 1, -1)        x 1/3
+//   isospin 1/2, G^{AB}, Z = A: (-4, 0, 2, -2, 4, 0)        x 1/3
+//   isospin 3/2, G^{AA}, Z = A: (-1, 1, 1, -1, 1, -1)
+// out = {iso-1/2 Delta+ (u,u,d), iso-1/2 Delta0 (d,d,u), iso-3/2 Delta++ (u,u,u),
+// iso-3/2 Delta- (d,d,d)} for table g (k = g + 1) and lane (mu, mu').
 template <typename R>
 __device__ __forceinline__ void delta_site(const Cx<R>* __restrict__ U, const Cx<R>* __restrict__ D, int g, int l,
                                            unsigned mask, Cx<R> out[4]) {
-  const DeltaLane dl = load_delta_lane(g, l);
-  const int xp = l >> 2, yp = l & 3;
+  const DiquarkLane dl = load_diquark_lane(c_delta_lane[g], l);
   const R third = R(1) / R(3);
 #pragma unroll
   for (int i = 0; i < 4; i++) out[i] = czero<R>();
-  // flavour pairs (X, Y) of the two diquark lines: uu, dd, ud, du
+  // G^{uu}, G^{dd}: isospin 1/2 with the other flavour on the third line, isospin 3/2 with the same
 #pragma unroll 1
-  for (int pair = 0; pair < 4; pair++) {
-    const Cx<R>* X = (pair == 0 || pair == 2) ? U : D;
-    const Cx<R>* Y = (pair == 0 || pair == 3) ? U : D;
+  for (int pair = 0; pair < 2; pair++) {
+    const Cx<R>* X = pair == 0 ? U : D;
+    const Cx<R>* O = pair == 0 ? D : U;
     Cx<R> q[9];
-    delta_G<R>(X, Y, g, xp, yp, q);
-    if (pair < 2) {
-      // G^{AA}: isospin 1/2 with the other flavour on the third line, isospin 3/2 with the same
-      const Cx<R> a = delta_eval<R>(q, pair == 0 ? D : U, dl, l, mask, 0, 2, 0, -2, 1, -1);
-      const Cx<R> b = delta_eval<R>(q, pair == 0 ? U : D, dl, l, mask, -1, 1, 1, -1, 1, -1);
-      out[pair] = out[pair] + cscale(a, third);
-      out[2 + pair] = out[2 + pair] + b;
-    } else {
-      // G^{AB}: isospin 1/2 with A on the third line
-      const Cx<R> a = delta_eval<R>(q, pair == 2 ? U : D, dl, l, mask, -4, 0, 2, -2, 4, 0);
-      out[pair - 2] = out[pair - 2] + cscale(a, third);
-    }
+    diquark_G<R>(X, X, c_delta_sink[g], l >> 2, l & 3, q);
+    const Cx<R> a = diquark_eval<R, true, true, true>(q, O, dl, l, mask, 0, 2, 0, -2, 1, -1);
+    const Cx<R> b = diquark_eval<R, true, true, true>(q, X, dl, l, mask, -1, 1, 1, -1, 1, -1);
+    out[pair] = out[pair] + cscale(a, third);
+    out[2 + pair] = out[2 + pair] + b;
   }
+  // G^{ud} (A = u) and its lane transpose G^{du} (A = d; C g_k is symmetric)
+  Cx<R> q[9];
+  diquark_G<R>(U, D, c_delta_sink[g], l >> 2, l & 3, q);
+  out[0] = out[0] + cscale(diquark_eval<R, true, true, true>(q, U, dl, l, mask, -4, 0, 2, -2, 4, 0), third);
+  diquark_transpose<R>(q, l, mask, R(1));
+  out[1] = out[1] + cscale(diquark_eval<R, true, true, true>(q, D, dl, l, mask, -4, 0, 2, -2, 4, 0), third);
 }
 
 }  // namespace p2

@@ -131,6 +131,16 @@ def nucleon_table():
     return diquark_table(CG5)
 
 
+def transpose_sign(gamma: np.ndarray) -> int:
+    """G^{YX} on lane (y', x') equals sign * G^{XY} on lane (x', y'): -1 for an
+    antisymmetric diquark matrix (C g5), +1 for a symmetric one (C g_k)."""
+    if np.allclose(gamma, gamma.T):
+        return 1
+    if np.allclose(gamma, -gamma.T):
+        return -1
+    raise ValueError("diquark matrix is neither symmetric nor antisymmetric")
+
+
 def delta_tables():
     return [diquark_table(c) for c in CGK]
 
@@ -242,6 +252,8 @@ def header_text() -> str:
            _c_array("kNucVal", "int", [r[4] for r in nuc]),
            _c_array("kDeltaIdx", "int", [[r[:4] for r in t] for t in dl]),
            _c_array("kDeltaVal", "int", [[r[4] for r in t] for t in dl]),
+           _c_array("kNucSink", "int", diquark_lane_tables(nuc)[0]),
+           _c_array("kNucLane", "int", diquark_lane_tables(nuc)[1]),
            _c_array("kDeltaSink", "int", [diquark_lane_tables(t)[0] for t in dl]),
            _c_array("kDeltaLane", "int", [diquark_lane_tables(t)[1] for t in dl]),
            _c_array("kEps", "int", eps),
