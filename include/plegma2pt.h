@@ -170,6 +170,22 @@ p2_status p2_contract_position(p2_ctx* ctx, const p2_prop* props, int nprops, co
 p2_status p2_ft_apply(p2_ctx* ctx, const double* field, int dof, int nt, const int* moms, int nmom, int sign,
                       double* out, int out_location);
 
+/* Allocation-free variant of p2_ft_apply (no counterpart in the reference).
+ * For callers that cannot allocate device memory at call time, e.g. a host
+ * framework that reserves all device memory for its own pool up front, or a
+ * caller with a fixed device-memory budget: its scratch (momenta, phase
+ * tables, partial sums) lives in a 32 MiB file-scope device array that every
+ * GPU loading the library holds until exit; no cudaMalloc/cudaFree or other
+ * allocating routine is called.  `out` is a device pointer ([nt][dof][nmom]
+ * complex double).  Requests needing more than the scratch
+ * (3*nmom*4 + 3*nmom*L*16 + nt*nmom*dof*16 bytes, each part rounded up to
+ * 256) are rejected with P2_ERR_INVALID_ARG.  The first call on a device
+ * looks up the array's address with that device current; make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race. */
+p2_status p2_ft_apply_noalloc(p2_ctx* ctx, const double* field, int dof, int nt, const int* moms, int nmom,
+                              int sign, double* out);
+
 /* ---- memory ------------------------------------------------------------ */
 /* Field storage for callers that do not link the CUDA runtime themselves
  * (PLEGMA_Field::create_device / create_host, lib/PLEGMA_Field.cu:226-235):

@@ -70,7 +70,8 @@ class P2KernelTime(C.Structure):
 #: Every entry point declared in include/plegma2pt.h.
 EXPORTS = ["p2_ctx_create", "p2_ctx_destroy", "p2_last_error", "p2_sync", "p2_set_stream", "p2_components",
            "p2_mom_list", "p2_block_info", "p2_contract_project", "p2_contract_position", "p2_ft_apply",
-           "p2_synth_propagator", "p2_profile_enable", "p2_profile_read", "p2_alloc", "p2_free", "p2_copy"]
+           "p2_synth_propagator", "p2_profile_enable", "p2_profile_read", "p2_alloc", "p2_free", "p2_copy",
+           "p2_ft_apply_noalloc"]
 
 _lib = None
 
@@ -97,6 +98,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
                                 C.c_void_p, C.c_int]
     lib.p2_synth_propagator.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int,
                                         C.c_double, C.c_int, C.c_int]
+    lib.p2_ft_apply_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int,
+                                        C.c_int, C.c_void_p]
     lib.p2_alloc.argtypes = [C.c_void_p, C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]
     lib.p2_free.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
     lib.p2_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]
@@ -227,6 +230,13 @@ class Context:
         buf = (P2KernelTime * 64)()
         n = self.lib.p2_profile_read(self.h, buf, 64, int(reset))
         return {buf[i].name.decode(): (buf[i].launches, buf[i].ms) for i in range(min(n, 64))}
+
+    def ft_apply_noalloc(self, field_ptr: int, dof: int, nt: int, moms: np.ndarray, sign: int, out_ptr: int):
+        """p2_ft_apply_noalloc: device output, scratch in the library's static device array."""
+        m = np.ascontiguousarray(moms, dtype=np.int32)
+        self.check(self.lib.p2_ft_apply_noalloc(self.h, C.c_void_p(field_ptr), dof, nt,
+                                                m.ctypes.data_as(C.POINTER(C.c_int)), len(m), sign,
+                                                C.c_void_p(out_ptr)))
 
     def ft_apply(self, field_ptr: int, dof: int, nt: int, moms: np.ndarray, sign: int, out_ptr: int,
                  out_location=P2_DEVICE):
