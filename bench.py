@@ -273,7 +273,7 @@ def main():
         need = 2 * u.numel() * 16 + (8 << 30)
         if avail > need:
             hu = torch.empty(u.numel(), dtype=torch.complex128, pin_memory=True)
-            hd = torch.empty_like(hu)
+            hd = torch.empty(u.numel(), dtype=torch.complex128, pin_memory=True)  # empty_like does not pin
             hu.copy_(u)
             hd.copy_(d)
             del u, d
@@ -287,14 +287,19 @@ def main():
                                                           mode=forms[head], q2max=Q2MAX)])
             estep()
             torch.cuda.synchronize()
+            ctx.profile(True)
+            ctx.profile_read(reset=True)
             t = time.perf_counter()
             n_e = max(1, min(args.steps, 3))
             for _ in range(n_e):
                 estep()
             torch.cuda.synchronize()
             el = (time.perf_counter() - t) / n_e
+            eprof = ctx.profile_read(reset=True)
+            ctx.profile(False)
             e2e = {"value": sites * world / el, "unit": "sites/s", "h2d_bytes_per_step": 2 * hu.numel() * 16,
-                   "d2h_bytes_per_step": total * 16, "steps": n_e, "timer": "host wall clock around the C-ABI call"}
+                   "d2h_bytes_per_step": total * 16, "steps": n_e, "timer": "host wall clock around the C-ABI call",
+                   "device_ms_per_step": {k: v[1] / n_e for k, v in eprof.items()}}
         else:
             e2e = {"value": None, "unit": "sites/s", "note": f"host memory {avail >> 30} GiB < {need >> 30} GiB"}
 

@@ -345,7 +345,7 @@ class PLEGMA_Correlator {
       r.out_location = P2_HOST;
       Runtime::check(p2_contract_position(c, props, 2, &r), "contract");
       // reference position-space layout: [group*dataset][t][x3][comp] for baryons
-      // (PLEGMA_baryons.cuh:208-212), [t][x3][site] otherwise
+      // (PLEGMA_baryons.cuh:157-161,200-201), [t][x3][site] otherwise
       buf.assign(getTotalSize() * 2, Float(0));
       size_t total = 0;
       p2_block blocks[8];

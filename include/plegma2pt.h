@@ -135,6 +135,12 @@ const char* p2_last_error(const p2_ctx* ctx);
 p2_status p2_sync(p2_ctx* ctx);
 /* Work is issued on `stream` (a cudaStream_t; NULL = the context's own). */
 p2_status p2_set_stream(p2_ctx* ctx, void* stream);
+/* Upper bound on the context's per-chunk position-space buffer (time slices
+ * are contracted and projected in chunks that fit it; default min(8 GiB,
+ * free/4)).  Smaller values cut memory and make more, shorter launches; the
+ * result does not depend on it beyond rounding.  No counterpart in the
+ * reference (it allocates per call, lib/kernels/PLEGMA_baryons.cuh:122). */
+p2_status p2_set_workspace(p2_ctx* ctx, size_t bytes);
 
 /* ---- shapes ----------------------------------------------------------- */
 /* Components per site of a contraction set (sum over blocks of groups*datasets*comps). */
@@ -149,9 +155,9 @@ int p2_block_info(unsigned contractions, int totalT, int nmom, p2_block* blocks,
 /* ---- the hot path ------------------------------------------------------ */
 /* Contraction + projection of nreq requests over the given propagators.
  * Replaces contract_baryons / contract_mesons_all / contract_mesons_new /
- * contract_mesons (lib/kernels/PLEGMA_baryons.cuh:169-206,
- * PLEGMA_mesonsAll.cuh:161-192, PLEGMA_mesonsNew.cuh:140-157,
- * PLEGMA_mesons.cuh:134-165) including their host block sums and spatial
+ * contract_mesons (lib/kernels/PLEGMA_baryons.cuh:99-206,
+ * PLEGMA_mesonsAll.cuh:98-192, PLEGMA_mesonsNew.cuh:63-157,
+ * PLEGMA_mesons.cuh:68-165) including their host block sums and spatial
  * all-reduce (one GPU holds the full spatial volume).  Asynchronous on the
  * context's stream when all outputs are on the device; synchronous when a
  * result or a propagator lives on the host. */

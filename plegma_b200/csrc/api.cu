@@ -51,15 +51,17 @@ std::vector<int> createMom(int q2max) {
 }
 
 // Per-dimension phase tables [3][nmom][Lmax] complex double:
-// exp(sign * i * 2 pi * n_d * (x_d - src_d) / L_d) for the local coordinates x_d.
-std::vector<double> phase_tables(const p2_ctx* c, const int* moms, int nmom, const int* src, int sign, int Lmax) {
+// exp(sign * i * 2 pi * n_d * x_d / L_d) for the global coordinates x_d of
+// the local sites (origin 0; the source's phase is applied per slice after
+// the site sum).
+std::vector<double> phase_tables(const p2_ctx* c, const int* moms, int nmom, int sign, int Lmax) {
   std::vector<double> t((size_t)3 * nmom * Lmax * 2, 0.0);
   for (int d = 0; d < 3; d++)
     for (int p = 0; p < nmom; p++)
       for (int xl = 0; xl < c->Ll[d]; xl++) {
         const long long xg = (long long)xl + (long long)c->g.coords[d] * c->Ll[d];
-        // reduce n*(x - x0) mod L exactly in integers before the division
-        long long num = ((long long)moms[3 * p + d] * (xg - src[d])) % c->g.L[d];
+        // reduce n*x mod L exactly in integers before the division
+        long long num = ((long long)moms[3 * p + d] * xg) % c->g.L[d];
         if (num < 0) num += c->g.L[d];
         const double ph = 2.0 * M_PI * (double)num / (double)c->g.L[d];
         const size_t i = ((size_t)(d * nmom + p) * Lmax + xl) * 2;
@@ -69,31 +71,15 @@ std::vector<double> phase_tables(const p2_ctx* c, const int* moms, int nmom, con
   return t;
 }
 
-std::vector<TauRun> local_runs(const p2_ctx* c, const p2_prop& u, const p2_prop& d, const int* src, int totalT) {
-  std::vector<TauRun> runs;
-  const int T = c->T;
-  const int tl0 = c->g.coords[3] * c->Ll[3];
-  int prev_ju = -2, prev_jd = -2;
-  for (int tau = 0; tau < totalT; tau++) {
-    const int t = (src[3] + tau) % T;
-    if (t < tl0 || t >= tl0 + c->Ll[3]) {
-      prev_ju = prev_jd = -2;
-      continue;
-    }
-    const int ju = ((t - u.t_first) % T + T) % T, jd = ((t - d.t_first) % T + T) % T;
-    if (ju >= u.nt || jd >= d.nt) {
-      prev_ju = prev_jd = -2;
-      continue;
-    }
-    if (!runs.empty() && ju == prev_ju + 1 && jd == prev_jd + 1 && runs.back().tau0 + runs.back().n == tau)
-      runs.back().n++;
-    else
-      runs.push_back({tau, 1});
-    prev_ju = ju;
-    prev_jd = jd;
-  }
-  return runs;
+p2_status upload_async(p2_ctx* c, DevBuf& b, const void* src, size_t bytes, const char* what) {
+  P2_TRY(c, b.ensure(std::max<size_t>(bytes, 16)), what);
+  P2_TRY(c, cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, c->stream), what);
+  return P2_OK;
 }
+
+}  // namespace p2host
+
+namespace {
 
 p2_status check_prop(p2_ctx* c, const p2_prop& p, const char* name) {
   if (!p.data) return c->fail(P2_ERR_INVALID_ARG, std::string(name) + ": null data");
@@ -107,115 +93,176 @@ p2_status check_prop(p2_ctx* c, const p2_prop& p, const char* name) {
   return P2_OK;
 }
 
-// Device views for one chunk of time slices: device propagators are used in
-// place; host propagators are copied slice-range by slice-range into the
-// context's staging buffers (2-D copies over the 144 component rows).
-p2_status chunk_view(p2_ctx* c, const p2_prop& p, DevBuf& stage, int t_begin, int n, p2::ContractArgs& a, bool is_u) {
-  const size_t esz = p.precision == P2_FP64 ? 16 : 8;
+}  // namespace
+
+namespace p2host {
+
+Work make_work(const p2_ctx* c, const p2_prop* props, const p2_request* reqs, const int* idx, int nidx, int tc) {
+  Work w;
   const int T = c->T;
-  if (p.location == P2_DEVICE) {
-    if (is_u) {
-      a.u = p.data;
-      a.vol_u = c->V3 * p.nt;
-      a.t_first_u = p.t_first;
-    } else {
-      a.d = p.data;
-      a.vol_d = c->V3 * p.nt;
-      a.t_first_d = p.t_first;
+  const int tl0 = c->g.coords[3] * c->Ll[3];
+  for (int q = 0; q < nidx; q++) {
+    const int ri = idx ? idx[q] : q;
+    const p2_request& r = reqs[ri];
+    const p2_prop& u = props[r.prop_u];
+    const p2_prop& d = props[r.prop_d];
+    for (int tau = 0; tau < r.totalT; tau++) {
+      const int t = (r.source[3] + tau) % T;
+      if (t < tl0 || t >= tl0 + c->Ll[3]) continue;  // another rank's time slab
+      const int ju = ((t - u.t_first) % T + T) % T, jd = ((t - d.t_first) % T + T) % T;
+      if (ju >= u.nt || jd >= d.nt) continue;  // not stored in the views
+      w.sl.push_back({ri, tau, ju, jd});
     }
-    return P2_OK;
   }
-  const int j0 = ((t_begin - p.t_first) % T + T) % T;
-  P2_TRY(c, stage.ensure((size_t)144 * n * c->V3 * esz), "staging alloc");
-  const size_t width = (size_t)n * c->V3 * esz;
-  P2_TRY(c,
-         cudaMemcpy2DAsync(stage.p, width, (const char*)p.data + (size_t)j0 * c->V3 * esz,
-                           (size_t)p.nt * c->V3 * esz, width, 144, cudaMemcpyHostToDevice, c->stream),
-         "host propagator upload");
-  if (is_u) {
-    a.u = stage.p;
-    a.vol_u = c->V3 * n;
-    a.t_first_u = t_begin;
-  } else {
-    a.d = stage.p;
-    a.vol_d = c->V3 * n;
-    a.t_first_d = t_begin;
+  const int n = (int)w.sl.size();
+  tc = std::max(1, tc);
+  // equal chunks: ceil(n / tc) of them, sizes differing by at most one
+  const int nch = (n + tc - 1) / tc;
+  for (int i = 0, s0 = 0; i < nch; i++) {
+    const int len = n / nch + (i < n % nch ? 1 : 0);
+    w.chunks.push_back({s0, len});
+    w.max_n = std::max(w.max_n, len);
+    s0 += len;
   }
+  return w;
+}
+
+Stager::Stager(p2_ctx* ctx, const p2_prop* pp, const p2_request* rr, const Work& work)
+    : c(ctx), props(pp), reqs(rr), w(work) {
+  for (const SliceRef& s : w.sl) {
+    const p2_request& r = reqs[s.req];
+    host |= props[r.prop_u].location == P2_HOST || props[r.prop_d].location == P2_HOST;
+  }
+}
+
+namespace {
+size_t esz_of(const p2_prop& p) { return p.precision == P2_FP64 ? 16 : 8; }
+}  // namespace
+
+p2_status Stager::prepare(double* const* outs) {
+  if (w.sl.empty()) return P2_OK;
+  size_t esz_max[2] = {0, 0};
+  for (const SliceRef& s : w.sl) {
+    const p2_request& r = reqs[s.req];
+    for (int f = 0; f < 2; f++) {
+      const p2_prop& p = props[f ? r.prop_d : r.prop_u];
+      if (p.location == P2_HOST) esz_max[f] = std::max(esz_max[f], esz_of(p));
+    }
+  }
+  if (host) {
+    if (c->capturing) return c->fail(P2_ERR_UNSUPPORTED, "graphs need device-resident propagators");
+    for (int slot = 0; slot < 2; slot++)
+      for (int f = 0; f < 2; f++)
+        if (esz_max[f])
+          P2_TRY(c, (f ? c->stage_d2[slot] : c->stage_u2[slot]).ensure((size_t)144 * w.max_n * c->V3 * esz_max[f]),
+                 "staging alloc");
+    if (!c->copy_stream) {
+      P2_TRY(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "copy stream");
+      for (int i = 0; i < 2; i++) {
+        P2_TRY(c, cudaEventCreateWithFlags(&c->copied[i], cudaEventDisableTiming), "copy events");
+        P2_TRY(c, cudaEventCreateWithFlags(&c->consumed[i], cudaEventDisableTiming), "copy events");
+      }
+    }
+    for (int i = 0; i < 2; i++) P2_TRY(c, cudaEventRecord(c->consumed[i], c->stream), "copy events");
+  }
+  // descriptors of every slice, in chunk order
+  const size_t bytes = w.sl.size() * sizeof(p2::SliceDesc);
+  if (!c->sdesc_copied)
+    P2_TRY(c, cudaEventCreateWithFlags(&c->sdesc_copied, cudaEventDisableTiming), "descriptor event");
+  else if (!c->capturing)
+    P2_TRY(c, cudaEventSynchronize(c->sdesc_copied), "descriptor mirror");
+  if (c->sdesc_host_n < bytes) {
+    if (c->sdesc_host) cudaFreeHost(c->sdesc_host);
+    c->sdesc_host = nullptr;
+    c->sdesc_host_n = 0;
+    P2_TRY(c, cudaMallocHost(&c->sdesc_host, bytes), "descriptor mirror");
+    c->sdesc_host_n = bytes;
+  }
+  p2::SliceDesc* h = (p2::SliceDesc*)c->sdesc_host;
+  for (size_t ci = 0; ci < w.chunks.size(); ci++) {
+    const Chunk& ch = w.chunks[ci];
+    const int slot = (int)(ci & 1);
+    for (int i = 0; i < ch.n; i++) {
+      const SliceRef& s = w.sl[ch.s0 + i];
+      const p2_request& r = reqs[s.req];
+      p2::SliceDesc& sd = h[ch.s0 + i];
+      std::memset(&sd, 0, sizeof(sd));
+      for (int f = 0; f < 2; f++) {
+        const p2_prop& p = props[f ? r.prop_d : r.prop_u];
+        const void* ptr = p.data;
+        long long vol = c->V3 * p.nt, off = (long long)(f ? s.jd : s.ju) * c->V3;
+        if (p.location == P2_HOST) {
+          ptr = (f ? c->stage_d2[slot] : c->stage_u2[slot]).p;
+          vol = c->V3 * ch.n;
+          off = (long long)i * c->V3;
+        }
+        (f ? sd.d : sd.u) = ptr;
+        (f ? sd.vol_d : sd.vol_u) = vol;
+        (f ? sd.off_d : sd.off_u) = off;
+      }
+      sd.out = outs[s.req];
+      sd.tau = s.tau;
+      sd.totalT = r.totalT;
+      for (int d = 0; d < 3; d++) sd.x0[d] = r.source[d];
+    }
+  }
+  P2_TRY(c, c->sdesc.ensure(bytes), "descriptor alloc");
+  P2_TRY(c, cudaMemcpyAsync(c->sdesc.p, h, bytes, cudaMemcpyHostToDevice, c->stream), "descriptor upload");
+  if (!c->capturing) P2_TRY(c, cudaEventRecord(c->sdesc_copied, c->stream), "descriptor event");
+  dsl = (p2::SliceDesc*)c->sdesc.p;
   return P2_OK;
 }
 
-std::vector<Chunk> make_chunks(const p2_ctx* c, const std::vector<TauRun>& runs, const int* src, int tc) {
-  std::vector<Chunk> out;
-  for (const TauRun& run : runs)
-    for (int off = 0; off < run.n; off += tc) {
-      Chunk ch;
-      ch.tau0 = run.tau0 + off;
-      ch.n = std::min(tc, run.n - off);
-      ch.t_begin = (src[3] + ch.tau0) % c->T;
-      out.push_back(ch);
-    }
-  return out;
-}
-
-Uploader::Uploader(p2_ctx* ctx, const p2_prop& pu, const p2_prop& pd)
-    : c(ctx), u(pu), d(pd), host(pu.location == P2_HOST || pd.location == P2_HOST) {}
-
-p2_status Uploader::issue(int slot, const Chunk& ch) {
-  if (!host) return P2_OK;
-  if (!c->copy_stream) {
-    P2_TRY(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "copy stream");
-    for (int i = 0; i < 2; i++) {
-      P2_TRY(c, cudaEventCreateWithFlags(&c->copied[i], cudaEventDisableTiming), "copy events");
-      P2_TRY(c, cudaEventCreateWithFlags(&c->consumed[i], cudaEventDisableTiming), "copy events");
-      P2_TRY(c, cudaEventRecord(c->consumed[i], c->stream), "copy events");
-    }
-  }
+p2_status Stager::issue(int ci) {
+  if (!host || ci >= (int)w.chunks.size()) return P2_OK;
+  const int slot = ci & 1;
+  const Chunk& ch = w.chunks[ci];
   P2_TRY(c, cudaStreamWaitEvent(c->copy_stream, c->consumed[slot], 0), "copy wait");
-  const int T = c->T;
+  ProfScope ps(c, "h2d_upload", c->copy_stream);
   for (int f = 0; f < 2; f++) {
-    const p2_prop& p = f ? d : u;
-    if (p.location != P2_HOST) continue;
-    DevBuf& stage = f ? c->stage_d2[slot] : c->stage_u2[slot];
-    const size_t esz = p.precision == P2_FP64 ? 16 : 8;
-    const int j0 = ((ch.t_begin - p.t_first) % T + T) % T;
-    P2_TRY(c, stage.ensure((size_t)144 * ch.n * c->V3 * esz), "staging alloc");
-    const size_t width = (size_t)ch.n * c->V3 * esz;
-    P2_TRY(c,
-           cudaMemcpy2DAsync(stage.p, width, (const char*)p.data + (size_t)j0 * c->V3 * esz,
-                             (size_t)p.nt * c->V3 * esz, width, 144, cudaMemcpyHostToDevice, c->copy_stream),
-           "host propagator upload");
+    // runs of slices that are consecutive in one host view: one contiguous
+    // copy per component row and run (a strided 2-D copy of this shape runs
+    // at a third of the link's bandwidth)
+    int i = 0;
+    while (i < ch.n) {
+      const SliceRef& s = w.sl[ch.s0 + i];
+      const p2_request& r = reqs[s.req];
+      const int pi = f ? r.prop_d : r.prop_u;
+      const p2_prop& p = props[pi];
+      const int j0 = f ? s.jd : s.ju;
+      int len = 1;
+      while (i + len < ch.n) {
+        const SliceRef& s2 = w.sl[ch.s0 + i + len];
+        const p2_request& r2 = reqs[s2.req];
+        if ((f ? r2.prop_d : r2.prop_u) != pi || (f ? s2.jd : s2.ju) != j0 + len) break;
+        len++;
+      }
+      if (p.location == P2_HOST) {
+        const size_t esz = esz_of(p);
+        char* dst = (char*)(f ? c->stage_d2[slot] : c->stage_u2[slot]).p + (size_t)i * c->V3 * esz;
+        const char* src = (const char*)p.data + (size_t)j0 * c->V3 * esz;
+        const size_t width = (size_t)len * c->V3 * esz;
+        const size_t spitch = (size_t)p.nt * c->V3 * esz, dpitch = (size_t)ch.n * c->V3 * esz;
+        for (int comp = 0; comp < 144; comp++)
+          P2_TRY(c,
+                 cudaMemcpyAsync(dst + comp * dpitch, src + comp * spitch, width, cudaMemcpyHostToDevice,
+                                 c->copy_stream),
+                 "host propagator upload");
+      }
+      i += len;
+    }
   }
   P2_TRY(c, cudaEventRecord(c->copied[slot], c->copy_stream), "copy event");
   return P2_OK;
 }
 
-p2_status Uploader::view(int slot, const Chunk& ch, p2::ContractArgs& a) {
-  for (int f = 0; f < 2; f++) {
-    const p2_prop& p = f ? d : u;
-    const void* ptr = p.data;
-    long long vol = c->V3 * p.nt;
-    int t_first = p.t_first;
-    if (p.location == P2_HOST) {
-      ptr = (f ? c->stage_d2[slot] : c->stage_u2[slot]).p;
-      vol = c->V3 * ch.n;
-      t_first = ch.t_begin;
-    }
-    if (f) {
-      a.d = ptr;
-      a.vol_d = vol;
-      a.t_first_d = t_first;
-    } else {
-      a.u = ptr;
-      a.vol_u = vol;
-      a.t_first_u = t_first;
-    }
-  }
-  if (host) P2_TRY(c, cudaStreamWaitEvent(c->stream, c->copied[slot], 0), "compute wait");
+p2_status Stager::wait(int ci) {
+  if (host) P2_TRY(c, cudaStreamWaitEvent(c->stream, c->copied[ci & 1], 0), "compute wait");
   return P2_OK;
 }
 
-p2_status Uploader::release(int slot) {
-  if (host) P2_TRY(c, cudaEventRecord(c->consumed[slot], c->stream), "consume event");
+p2_status Stager::release(int ci) {
+  if (host) P2_TRY(c, cudaEventRecord(c->consumed[ci & 1], c->stream), "consume event");
   return P2_OK;
 }
 
@@ -237,7 +284,6 @@ p2_status make_plan(p2_ctx* c, const p2_request& r, Plan& pl) {
   pl.Lmax = std::max(c->Ll[0], std::max(c->Ll[1], c->Ll[2]));
   pl.totalT = r.totalT;
   pl.blocks.clear();
-  size_t off = 0;
   int k = 0;
   for (const auto& b : kBlocks)
     if (r.contractions & b.bit) {
@@ -246,14 +292,17 @@ p2_status make_plan(p2_ctx* c, const p2_request& r, Plan& pl) {
       sb.groups = b.groups;
       sb.datasets = b.datasets;
       sb.comps = b.comps;
-      sb.base = (long long)off;
+      sb.base = k;  // the blocks before this one hold k components per (time, momentum)
       pl.blocks.push_back(sb);
       k += b.groups * b.datasets * b.comps;
-      off += (size_t)b.groups * b.datasets * b.comps * r.totalT * pl.nmom;
     }
-  pl.total = off;
+  pl.total = (size_t)k * r.totalT * pl.nmom;
   return P2_OK;
 }
+
+}  // namespace p2host
+
+namespace {
 
 int chunk_slices(p2_ctx* c, int K) {
   const size_t per = (size_t)K * c->V3 * 16;
@@ -261,50 +310,49 @@ int chunk_slices(p2_ctx* c, int K) {
   return (int)std::max<size_t>(1, std::min<size_t>(n, (size_t)c->T));
 }
 
-p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request& r, const Plan& pl, double* dres) {
-  const p2_prop& u = props[r.prop_u];
-  const p2_prop& d = props[r.prop_d];
-  if (u.precision != P2_FP64 || d.precision != P2_FP64)
-    return c->fail(P2_ERR_UNSUPPORTED, "the plain FP64 form needs FP64 propagators");
-
-  std::vector<double> tabh = phase_tables(c, pl.moms.data(), pl.nmom, r.source, -1, pl.Lmax);
-  P2_TRY(c, c->tab.ensure(tabh.size() * sizeof(double)), "phase table alloc");
-  P2_TRY(c, cudaMemcpyAsync(c->tab.p, tabh.data(), tabh.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream),
-         "phase table upload");
+// Plain FP64 form for requests reqs[idx[..]] that share contractions and
+// momenta: FP64 site contraction, FP64 projection, deterministic reduction.
+p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request* reqs, const int* idx, int nidx,
+                    const Plan& pl, double* const* outs) {
+  for (int q = 0; q < nidx; q++) {
+    const p2_request& r = reqs[idx[q]];
+    if (props[r.prop_u].precision != P2_FP64 || props[r.prop_d].precision != P2_FP64)
+      return c->fail(P2_ERR_UNSUPPORTED, "the plain FP64 form needs FP64 propagators");
+  }
+  const unsigned what = reqs[idx[0]].contractions;
+  std::vector<double> tabh = phase_tables(c, pl.moms.data(), pl.nmom, -1, pl.Lmax);
+  p2_status st;
+  if ((st = upload_async(c, c->tab, tabh.data(), tabh.size() * sizeof(double), "phase table")) != P2_OK) return st;
+  if ((st = upload_async(c, c->moms, pl.moms.data(), pl.moms.size() * sizeof(int), "momenta")) != P2_OK) return st;
 
   const int tc = chunk_slices(c, pl.K);
-  P2_TRY(c, c->cbuf.ensure((size_t)tc * pl.K * c->V3 * 16), "position buffer alloc");
+  const Work w = make_work(c, props, reqs, idx, nidx, tc);
+  if (w.sl.empty()) return P2_OK;
+  P2_TRY(c, c->cbuf.ensure((size_t)w.max_n * pl.K * c->V3 * 16), "position buffer alloc");
+  Stager sg(c, props, reqs, w);
+  if ((st = sg.prepare(outs)) != P2_OK) return st;
 
   const int ptiles = (pl.nmom + 63) / 64;
   const int ktiles = (pl.K + 95) / 96;
-  const std::vector<Chunk> chunks = make_chunks(c, local_runs(c, u, d, r.source, r.totalT), r.source, tc);
-  Uploader up(c, u, d);
-  for (size_t i = 0; i < chunks.size() && i < 2; i++) {
-    p2_status s = up.issue((int)i, chunks[i]);
-    if (s != P2_OK) return s;
-  }
-  for (size_t i = 0; i < chunks.size(); i++) {
-    const Chunk& ch = chunks[i];
-    const int slot = (int)(i & 1);
-    const int n = ch.n, tau0 = ch.tau0;
+  for (int i = 0; i < 2; i++)
+    if ((st = sg.issue(i)) != P2_OK) return st;
+  for (size_t ci = 0; ci < w.chunks.size(); ci++) {
+    const int n = w.chunks[ci].n;
+    if ((st = sg.wait((int)ci)) != P2_OK) return st;
     p2::ContractArgs a{};
-    p2_status s = up.view(slot, ch, a);
-    if (s != P2_OK) return s;
+    a.sl = sg.desc((int)ci);
     a.V3 = (int)c->V3;
-    a.T = c->T;
-    a.t0 = r.source[3];
-    a.tau0 = tau0;
     a.ntau = n;
-    a.what = r.contractions;
+    a.what = what;
     a.K = pl.K;
-    a.k = offsets_of(r.contractions);
+    a.k = offsets_of(what);
     a.out = c->cbuf.p;
     {
       ProfScope ps(c, "contract_plain_fp64");
       P2_TRY(c, p2::launch_contract_plain(a, c->nsm, c->stream), "contract kernel");
     }
-    if ((s = up.release(slot)) != P2_OK) return s;
-    if (i + 2 < chunks.size() && (s = up.issue(slot, chunks[i + 2])) != P2_OK) return s;
+    if ((st = sg.release((int)ci)) != P2_OK) return st;
+    if ((st = sg.issue((int)ci + 2)) != P2_OK) return st;
 
     p2::ProjArgs pa{};
     pa.c = c->cbuf.p;
@@ -323,7 +371,7 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request& r, const 
     nsplit = std::max(1, std::min(nsplit, (int)((c->V3 + 255) / 256)));
     pa.chunk = (int)((((c->V3 + nsplit - 1) / nsplit) + 15) / 16 * 16);
     pa.nsplit = (int)((c->V3 + pa.chunk - 1) / pa.chunk);
-    P2_TRY(c, c->part.ensure((size_t)n * pa.nsplit * pl.nmom * pl.K * 16), "partials alloc");
+    P2_TRY(c, c->part.ensure((size_t)w.max_n * pa.nsplit * pl.nmom * pl.K * 16), "partials alloc");
     pa.part = (double*)c->part.p;
     {
       ProfScope ps(c, "project_fp64");
@@ -335,11 +383,11 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request& r, const 
     sa.nsplit = pa.nsplit;
     sa.nmom = pl.nmom;
     sa.K = pl.K;
-    sa.tau0 = tau0;
-    sa.totalT = r.totalT;
     sa.nblocks = (int)pl.blocks.size();
     for (size_t b = 0; b < pl.blocks.size(); b++) sa.blk[b] = pl.blocks[b];
-    sa.out = dres;
+    sa.sl = sg.desc((int)ci);
+    sa.moms = (const int*)c->moms.p;
+    for (int d = 0; d < 3; d++) sa.L[d] = c->g.L[d];
     {
       ProfScope ps(c, "reduce_scatter");
       P2_TRY(c, p2::launch_scatter(sa, c->stream), "reduction kernel");
@@ -350,7 +398,7 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request& r, const 
 
 }  // namespace
 
-cudaEvent_t p2_ctx::prof_begin(const char* name, int& slot) {
+cudaEvent_t p2_ctx::prof_begin(const char* name, int& slot, cudaStream_t on) {
   slot = -1;
   for (size_t i = 0; i < prof.size(); i++)
     if (prof[i].name == name) slot = (int)i;
@@ -368,11 +416,11 @@ cudaEvent_t p2_ctx::prof_begin(const char* name, int& slot) {
     cudaGetLastError();
     return nullptr;
   }
-  cudaEventRecord(e, stream);
+  cudaEventRecord(e, on ? on : stream);
   return e;
 }
 
-void p2_ctx::prof_end(int slot, cudaEvent_t start) {
+void p2_ctx::prof_end(int slot, cudaEvent_t start, cudaStream_t on) {
   cudaEvent_t e = nullptr;
   Prof& p = prof[slot];
   if (!p.pool.empty()) {
@@ -383,7 +431,7 @@ void p2_ctx::prof_end(int slot, cudaEvent_t start) {
     p.pool.push_back(start);
     return;
   }
-  cudaEventRecord(e, stream);
+  cudaEventRecord(e, on ? on : stream);
   p.pending.emplace_back(start, e);
 }
 
@@ -482,7 +530,9 @@ p2_status p2_ctx_destroy(p2_ctx* c) {
     return P2_OK;
   }
   cudaStreamSynchronize(c->stream);
-  for (DevBuf* b : {&c->cbuf, &c->part, &c->tab, &c->res, &c->stage_u, &c->stage_d, &c->scratch}) b->release();
+  for (DevBuf* b : {&c->cbuf, &c->part, &c->tab, &c->res, &c->moms, &c->sdesc}) b->release();
+  if (c->sdesc_host) cudaFreeHost(c->sdesc_host);
+  if (c->sdesc_copied) cudaEventDestroy(c->sdesc_copied);
   for (int i = 0; i < 2; i++) {
     c->stage_u2[i].release();
     c->stage_d2[i].release();
@@ -531,6 +581,13 @@ p2_status p2_set_stream(p2_ctx* c, void* s) {
       return c->fail(P2_ERR_CUDA, "stream create");
     c->own_stream = true;
   }
+  return P2_OK;
+}
+
+p2_status p2_set_workspace(p2_ctx* c, size_t bytes) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  if (bytes == 0) return c->fail(P2_ERR_INVALID_ARG, "p2_set_workspace: zero bytes");
+  c->ws_budget = bytes;
   return P2_OK;
 }
 
@@ -583,25 +640,54 @@ p2_status p2_contract_project(p2_ctx* c, const p2_prop* props, int nprops, const
     if (s != P2_OK) return s;
   }
   if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
-  if (nreq > 1 && reqs[0].mode == P2_SPLIT_FP16) {
-    bool all = true;
-    for (int i = 0; i < nreq; i++) all &= reqs[i].mode == P2_SPLIT_FP16;
-    if (all) return p2::precision_run_batch(c, props, nprops, reqs, nreq);
-  }
+  if (c->capturing)
+    for (int i = 0; i < nreq; i++)
+      if (reqs[i].out_location != P2_DEVICE) return c->fail(P2_ERR_UNSUPPORTED, "graphs need device-resident results");
+
+  // requests that share form, contractions, momenta and input precision run as
+  // one batch: each kernel launches once per chunk of slices from all of them
+  std::vector<char> done(nreq, 0);
   for (int i = 0; i < nreq; i++) {
-    const p2_request& r = reqs[i];
-    const Plan& pl = plans[i];
-    double* dres = r.out;
-    if (r.out_location == P2_HOST) {
-      P2_TRY(c, c->res.ensure(pl.total * 16), "result alloc");
-      P2_TRY(c, cudaMemsetAsync(c->res.p, 0, pl.total * 16, c->stream), "result clear");
-      dres = (double*)c->res.p;
+    if (done[i]) continue;
+    std::vector<int> idx;
+    const p2_request& ri = reqs[i];
+    for (int j = i; j < nreq; j++) {
+      const p2_request& rj = reqs[j];
+      if (done[j] || rj.mode != ri.mode || rj.contractions != ri.contractions || plans[j].moms != plans[i].moms ||
+          props[rj.prop_u].precision != props[ri.prop_u].precision ||
+          props[rj.prop_d].precision != props[ri.prop_d].precision)
+        continue;
+      done[j] = 1;
+      idx.push_back(j);
     }
-    p2_status s = r.mode == P2_PLAIN_FP64 ? run_plain(c, props, r, pl, dres)
-                                          : p2::precision_run_batch(c, props, nprops, &r, 1);
+    // device result of each request; host results go through one device buffer
+    std::vector<double*> outs(nreq, nullptr);
+    size_t host_total = 0;
+    for (int j : idx)
+      if (reqs[j].out_location == P2_HOST) host_total += plans[j].total;
+    if (host_total) {
+      P2_TRY(c, c->res.ensure(host_total * 16), "result alloc");
+      P2_TRY(c, cudaMemsetAsync(c->res.p, 0, host_total * 16, c->stream), "result clear");
+    }
+    size_t off = 0;
+    for (int j : idx) {
+      if (reqs[j].out_location == P2_HOST) {
+        outs[j] = (double*)c->res.p + 2 * off;
+        off += plans[j].total;
+      } else {
+        outs[j] = reqs[j].out;
+      }
+    }
+    p2_status s = ri.mode == P2_PLAIN_FP64
+                      ? run_plain(c, props, reqs, idx.data(), (int)idx.size(), plans[i], outs.data())
+                      : p2::precision_run_batch(c, props, reqs, idx.data(), (int)idx.size(), plans[i], outs.data());
     if (s != P2_OK) return s;
-    if (r.out_location == P2_HOST && r.mode == P2_PLAIN_FP64) {
-      P2_TRY(c, cudaMemcpyAsync(r.out, dres, pl.total * 16, cudaMemcpyDeviceToHost, c->stream), "result download");
+    if (host_total) {
+      for (int j : idx)
+        if (reqs[j].out_location == P2_HOST)
+          P2_TRY(c,
+                 cudaMemcpyAsync(reqs[j].out, outs[j], plans[j].total * 16, cudaMemcpyDeviceToHost, c->stream),
+                 "result download");
       P2_TRY(c, cudaStreamSynchronize(c->stream), "result download");
     }
   }
@@ -621,47 +707,52 @@ p2_status p2_contract_position(p2_ctx* c, const p2_prop* props, int nprops, cons
   if (r->contractions == 0 || (r->contractions & ~kAllBits))
     return c->fail(P2_ERR_INVALID_ARG, "contractions: empty or unknown bits");
   if (r->totalT < 1 || r->totalT > c->T) return c->fail(P2_ERR_INVALID_ARG, "totalT out of range");
+  if (r->out_location != P2_DEVICE && r->out_location != P2_HOST)
+    return c->fail(P2_ERR_INVALID_ARG, "bad out_location");
   const p2_prop& u = props[r->prop_u];
   const p2_prop& d = props[r->prop_d];
   if (u.precision != P2_FP64 || d.precision != P2_FP64)
     return c->fail(P2_ERR_UNSUPPORTED, "position-space output needs FP64 propagators");
   if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
   const int K = components_of(r->contractions);
-  const size_t slice = (size_t)K * c->V3;
-  for (const TauRun& run : local_runs(c, u, d, r->source, r->totalT)) {
+  const size_t slice = (size_t)K * c->V3;  // complex elements of one time slice
+  const Work w = make_work(c, props, r, nullptr, 1, chunk_slices(c, K));
+  if (w.sl.empty()) return P2_OK;
+  P2_TRY(c, c->cbuf.ensure((size_t)w.max_n * slice * 16), "position buffer alloc");
+  Stager sg(c, props, r, w);
+  double* outs[1] = {r->out};
+  p2_status st;
+  if ((st = sg.prepare(outs)) != P2_OK) return st;
+  for (int i = 0; i < 2; i++)
+    if ((st = sg.issue(i)) != P2_OK) return st;
+  for (size_t ci = 0; ci < w.chunks.size(); ci++) {
+    const Chunk& ch = w.chunks[ci];
+    if ((st = sg.wait((int)ci)) != P2_OK) return st;
+    // slices of consecutive times go straight into a device result
+    bool direct = r->out_location == P2_DEVICE;
+    for (int i = 1; i < ch.n && direct; i++) direct = w.sl[ch.s0 + i].tau == w.sl[ch.s0].tau + i;
     p2::ContractArgs a{};
-    const int t_begin = (r->source[3] + run.tau0) % c->T;
-    p2_status s = chunk_view(c, u, c->stage_u, t_begin, run.n, a, true);
-    if (s != P2_OK) return s;
-    s = chunk_view(c, d, c->stage_d, t_begin, run.n, a, false);
-    if (s != P2_OK) return s;
+    a.sl = sg.desc((int)ci);
     a.V3 = (int)c->V3;
-    a.T = c->T;
-    a.t0 = r->source[3];
-    a.tau0 = run.tau0;
-    a.ntau = run.n;
+    a.ntau = ch.n;
     a.what = r->contractions;
     a.K = K;
     a.k = offsets_of(r->contractions);
-    double* dst = r->out + 2 * slice * run.tau0;
-    if (r->out_location == P2_HOST) {
-      P2_TRY(c, c->cbuf.ensure(slice * run.n * 16), "position buffer alloc");
-      a.out = c->cbuf.p;
-    } else {
-      a.out = dst;
-    }
+    a.out = direct ? (void*)(r->out + 2 * slice * w.sl[ch.s0].tau) : c->cbuf.p;
     {
-        ProfScope ps(c, "contract_plain_fp64");
-        P2_TRY(c, p2::launch_contract_plain(a, c->nsm, c->stream), "contract kernel");
-      }
-    if (r->out_location == P2_HOST) {
-      P2_TRY(c, cudaMemcpyAsync(dst, c->cbuf.p, slice * run.n * 16, cudaMemcpyDeviceToHost, c->stream),
-             "position download");
-      P2_TRY(c, cudaStreamSynchronize(c->stream), "position download");
-    } else if (u.location == P2_HOST || d.location == P2_HOST) {
-      P2_TRY(c, cudaStreamSynchronize(c->stream), "staging reuse");
+      ProfScope ps(c, "contract_plain_fp64");
+      P2_TRY(c, p2::launch_contract_plain(a, c->nsm, c->stream), "contract kernel");
     }
+    if ((st = sg.release((int)ci)) != P2_OK) return st;
+    if ((st = sg.issue((int)ci + 2)) != P2_OK) return st;
+    if (!direct)
+      for (int i = 0; i < ch.n; i++)
+        P2_TRY(c,
+               cudaMemcpyAsync(r->out + 2 * slice * w.sl[ch.s0 + i].tau, (const double*)c->cbuf.p + 2 * slice * i,
+                               slice * 16, cudaMemcpyDefault, c->stream),
+               "position copy");
   }
+  if (r->out_location == P2_HOST) P2_TRY(c, cudaStreamSynchronize(c->stream), "position download");
   return P2_OK;
 }
 
@@ -673,8 +764,7 @@ p2_status p2_ft_apply(p2_ctx* c, const double* field, int dof, int nt, const int
   if (sign != 1 && sign != -1) return c->fail(P2_ERR_INVALID_ARG, "p2_ft_apply: sign must be +1 or -1");
   if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
   const int Lmax = std::max(c->Ll[0], std::max(c->Ll[1], c->Ll[2]));
-  const int origin[4] = {0, 0, 0, 0};
-  std::vector<double> tabh = phase_tables(c, moms, nmom, origin, sign, Lmax);
+  std::vector<double> tabh = phase_tables(c, moms, nmom, sign, Lmax);
   P2_TRY(c, c->tab.ensure(tabh.size() * sizeof(double)), "phase table alloc");
   P2_TRY(c, cudaMemcpyAsync(c->tab.p, tabh.data(), tabh.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream),
          "phase table upload");
@@ -715,7 +805,6 @@ p2_status p2_ft_apply(p2_ctx* c, const double* field, int dof, int nt, const int
   sa.nmom = nmom;
   sa.K = dof;
   sa.tau0 = 0;
-  sa.totalT = nt;
   sa.nblocks = 0;
   sa.oT = (long long)dof * nmom;
   sa.oK = nmom;

@@ -3,7 +3,7 @@
 // projection kernels consume.
 //
 // Replaces the per-site part of contract_baryons_device / contract_NtoN_kernel
-// (lib/kernels/PLEGMA_baryons.cuh:82-147, PLEGMA_baryons_NtoN.cu:6-46) and
+// (lib/kernels/PLEGMA_baryons.cuh:31-96, PLEGMA_baryons_NtoN.cu:6-46) and
 // contract_mesons_{all,new,}_device (PLEGMA_mesonsAll.cuh:7-95,
 // PLEGMA_mesonsNew.cuh:5-56, PLEGMA_mesons.cuh:10-65).
 //
@@ -40,31 +40,30 @@ __device__ __forceinline__ void issue_tile(const ContractArgs& a, Cx<Tin>* st, l
                                            int tiles_per_tau) {
   if (tile < ntiles) {
     const int tl = (int)(tile / tiles_per_tau);
-    const int x0 = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile;
-    const int t = (a.t0 + a.tau0 + tl) % a.T;
-    const long long ju = (long long)((t - a.t_first_u + a.T) % a.T) * a.V3;
-    const long long jd = (long long)((t - a.t_first_d + a.T) % a.T) * a.V3;
-    const Cx<Tin>* U = (const Cx<Tin>*)a.u;
-    const Cx<Tin>* D = (const Cx<Tin>*)a.d;
-#pragma unroll 2
-    for (int r = 0; r < (2 * 144 * kSitesPerTile) / kThreads; r++) {
-      const int i = threadIdx.x + r * kThreads;
-      const int s = i & (kSitesPerTile - 1);
-      const int rest = i >> 4;
-      const int f = rest >= 144;
-      const int comp = rest - 144 * f;
-      const int x = x0 + s;
-      const bool ok = x < a.V3;
-      const Cx<Tin>* src = f ? D + (long long)comp * a.vol_d + jd + (ok ? x : 0)
-                             : U + (long long)comp * a.vol_u + ju + (ok ? x : 0);
-      if (sizeof(Tin) == 8)
-        cp_async16(st + s * kRow + rest, src, ok ? 16 : 0);
-      else
-        cp_async8(st + s * kRow + rest, src, ok ? 8 : 0);
+    const int s = threadIdx.x & (kSitesPerTile - 1);
+    const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + s;
+    const bool ok = x < a.V3;
+    const SliceDesc* sd = a.sl + tl;
+    // thread i copies component i/16 + 16 r of site i%16; with 256 threads
+    // rows r < 9 are the u view's 144 components and r >= 9 the d view's
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      const Cx<Tin>* src = (const Cx<Tin>*)(f ? sd->d : sd->u) + (f ? sd->off_d : sd->off_u) + (ok ? x : 0);
+      const long long vol = f ? sd->vol_d : sd->vol_u;
+#pragma unroll 3
+      for (int r = 0; r < 9; r++) {
+        const int comp = (threadIdx.x >> 4) + 16 * r;
+        Cx<Tin>* dst = st + s * kRow + 144 * f + comp;
+        if (sizeof(Tin) == 8)
+          cp_async16(dst, src + comp * vol, ok ? 16 : 0);
+        else
+          cp_async8(dst, src + comp * vol, ok ? 8 : 0);
+      }
     }
   }
   cp_async_commit();
 }
+static_assert(kThreads == 256 && kSitesPerTile == 16, "issue_tile maps 256 threads onto 16 sites x 16 components");
 
 // Index of a diagonal structure in the 10-structure list (1, g5, g1..g4,
 // g5g1..g5g4) of contractMesons / contractMesonsNew, or -1.
@@ -259,7 +258,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
     {
       // exact power-of-two scales; products are formed in double so that no
       // intermediate leaves the representable range
-      const double su = ldexp(1.0, -a.exp_u[tl]), sd = ldexp(1.0, -a.exp_d[tl]);
+      const double su = ldexp(1.0, -a.exps[2 * tl]), sd = ldexp(1.0, -a.exps[2 * tl + 1]);
       for (int i = tid; i < kSitesPerTile * 288; i += kThreads) {
         const int s = i / 288, c = i - s * 288;
         const Cx<Tin> v = st[s * kRow + c];
@@ -293,21 +292,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
 // so FP64 entries far below FP32's range are handled exactly.
 __global__ void k_sample_exponents(const SampleArgs a) {
   __shared__ int red[256];
-  const int tl = blockIdx.x;
-  const int t = (a.t0 + a.tau0 + tl) % a.T;
-  const long long j = (long long)((t - a.t_first + a.T) % a.T) * a.V3;
+  const int tl = blockIdx.x, f = blockIdx.y;
+  const SliceDesc& sd = a.sl[tl];
+  const void* p = f ? sd.d : sd.u;
+  const long long vol = f ? sd.vol_d : sd.vol_u;
+  const long long j = f ? sd.off_d : sd.off_u;
   int emax = -100000;
   for (int i = threadIdx.x; i < 21 * 1024; i += blockDim.x) {
     const int comp = (i % 21) * 7;
     const long long x = ((long long)(i / 21) * 97) % a.V3;
-    const long long idx = (long long)comp * a.vol + j + x;
+    const long long idx = (long long)comp * vol + j + x;
     double re, im;
     if (a.fp32) {
-      const float2 v = ((const float2*)a.p)[idx];
+      const float2 v = ((const float2*)p)[idx];
       re = v.x;
       im = v.y;
     } else {
-      const double2 v = ((const double2*)a.p)[idx];
+      const double2 v = ((const double2*)p)[idx];
       re = v.x;
       im = v.y;
     }
@@ -327,7 +328,7 @@ __global__ void k_sample_exponents(const SampleArgs a) {
     if (threadIdx.x < s) red[threadIdx.x] = max(red[threadIdx.x], red[threadIdx.x + s]);
     __syncthreads();
   }
-  if (threadIdx.x == 0) a.exp_out[tl] = red[0] == -100000 ? 0 : red[0];
+  if (threadIdx.x == 0) a.exp_out[2 * tl + f] = red[0] == -100000 ? 0 : red[0];
 }
 
 }  // namespace
@@ -371,7 +372,7 @@ cudaError_t launch_contract_f32(const ContractArgs& a, int fp32_in, int grid, cu
 }
 
 cudaError_t launch_sample_exponents(const SampleArgs& a, cudaStream_t s) {
-  k_sample_exponents<<<a.ntau, 256, 0, s>>>(a);
+  k_sample_exponents<<<dim3(a.ntau, 2), 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -51,7 +51,13 @@ struct p2_ctx {
   bool own_stream = false;
   bool host_only = false;  // created with device < 0
   std::string err = "no error";
-  p2host::DevBuf cbuf, part, tab, res, stage_u, stage_d, scratch;
+  p2host::DevBuf cbuf, part, tab, res, moms;
+  // slice descriptors of the current call and their pinned host mirror
+  p2host::DevBuf sdesc;
+  void* sdesc_host = nullptr;
+  size_t sdesc_host_n = 0;
+  cudaEvent_t sdesc_copied = nullptr;  // the mirror may be rewritten once this completes
+  bool capturing = false;              // recording a graph: no host synchronisation
   // host-resident propagators: two staging slots per flavour, uploaded on a
   // copy stream while the previous chunk is contracted
   p2host::DevBuf stage_u2[2], stage_d2[2];
@@ -59,6 +65,8 @@ struct p2_ctx {
   cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
   // split form: phase tiles, per-slice exponents, component maxima, tables, partials, error flag
   p2host::DevBuf phaseA, expb, cmaxb, momrow, kexp, fpart, rowtab, errflag;
+  std::vector<int> split_moms_key;  // momentum list the phase tiles and rows were built for
+  unsigned split_what_key = 0;      // contraction set of the component exponents
   int project_split_smem_max = 0;  // opt-in shared memory per block of the device
   size_t ws_budget = 0;
 
@@ -72,8 +80,8 @@ struct p2_ctx {
   };
   bool profiling = false;
   std::vector<Prof> prof;
-  cudaEvent_t prof_begin(const char* name, int& slot);
-  void prof_end(int slot, cudaEvent_t start);
+  cudaEvent_t prof_begin(const char* name, int& slot, cudaStream_t on = nullptr);
+  void prof_end(int slot, cudaEvent_t start, cudaStream_t on = nullptr);
   void prof_collect();
   void prof_clear();
 
@@ -92,13 +100,14 @@ struct p2_ctx {
 // Brackets one kernel launch with events when profiling is on.
 struct ProfScope {
   p2_ctx* c;
+  cudaStream_t on;
   int slot = -1;
   cudaEvent_t start = nullptr;
-  ProfScope(p2_ctx* ctx, const char* name) : c(ctx) {
-    if (c->profiling) start = c->prof_begin(name, slot);
+  ProfScope(p2_ctx* ctx, const char* name, cudaStream_t s = nullptr) : c(ctx), on(s) {
+    if (c->profiling) start = c->prof_begin(name, slot, on);
   }
   ~ProfScope() {
-    if (start) c->prof_end(slot, start);
+    if (start) c->prof_end(slot, start, on);
   }
 };
 
@@ -111,51 +120,68 @@ struct ProfScope {
 
 namespace p2host {
 
-// Consecutive source-relative times whose slices are stored contiguously in both views.
-struct TauRun {
-  int tau0, n;
-};
-
 struct Plan {
   int K, nmom, Lmax, totalT;
   std::vector<int> moms;
-  std::vector<p2::ScatterBlock> blocks;
+  std::vector<p2::ScatterBlock> blocks;  // base = block offset per unit of (totalT * nmom)
   size_t total;  // complex elements of the result
 };
 
-// A chunk of consecutive source-relative times processed by one launch sequence.
-struct Chunk {
-  int tau0, n, t_begin;
+// One local time slice of one request: its source-relative time and the
+// slice's index in the request's u and d views.
+struct SliceRef {
+  int req, tau, ju, jd;
 };
 
-// Splits the local time runs of a request into chunks of at most `tc` slices.
-std::vector<Chunk> make_chunks(const p2_ctx* c, const std::vector<TauRun>& runs, const int* src, int tc);
+// Slices [s0, s0 + n) of a work list, processed by one launch sequence.
+struct Chunk {
+  int s0, n;
+};
 
-// Device views of (u, d) for each chunk.  Device propagators are used in
-// place; host propagators are uploaded into two staging slots on a copy
-// stream, so chunk i+1 crosses PCIe while chunk i is contracted.
-struct Uploader {
+struct Work {
+  std::vector<SliceRef> sl;
+  std::vector<Chunk> chunks;
+  int max_n = 0;
+};
+
+// The local slices of requests reqs[idx[0..nidx)] in request order, cut into
+// chunks of at most tc slices.
+Work make_work(const p2_ctx* c, const p2_prop* props, const p2_request* reqs, const int* idx, int nidx, int tc);
+
+// Device views and slice descriptors of a work list.  Device propagators are
+// read in place; host propagators are uploaded chunk by chunk into two
+// staging slots on a copy stream, so chunk i+1 crosses PCIe while chunk i is
+// contracted.  All descriptors go to the device in one copy (prepare).
+struct Stager {
   p2_ctx* c;
-  const p2_prop& u;
-  const p2_prop& d;
-  bool host;
-  Uploader(p2_ctx* ctx, const p2_prop& pu, const p2_prop& pd);
-  p2_status issue(int slot, const Chunk& ch);                    // start the upload of a chunk
-  p2_status view(int slot, const Chunk& ch, p2::ContractArgs& a);  // views for the compute stream
-  p2_status release(int slot);                                   // the chunk's kernels are queued
+  const p2_prop* props;
+  const p2_request* reqs;
+  const Work& w;
+  bool host = false;
+  p2::SliceDesc* dsl = nullptr;
+  Stager(p2_ctx* ctx, const p2_prop* pp, const p2_request* rr, const Work& work);
+  // outs[req]: device result pointer of each request (indexed like reqs)
+  p2_status prepare(double* const* outs);
+  p2_status issue(int ci);    // start the upload of chunk ci
+  p2_status wait(int ci);     // the compute stream waits for chunk ci's upload
+  p2_status release(int ci);  // chunk ci's kernels are queued; its slot may be refilled
+  const p2::SliceDesc* desc(int ci) const { return dsl + w.chunks[ci].s0; }
 };
 
 int components_of(unsigned what);
 p2::CompOffsets offsets_of(unsigned what);
-std::vector<double> phase_tables(const p2_ctx* c, const int* moms, int nmom, const int* src, int sign, int Lmax);
-std::vector<TauRun> local_runs(const p2_ctx* c, const p2_prop& u, const p2_prop& d, const int* src, int totalT);
+// [3][nmom][Lmax] complex exp(sign i 2 pi n_d x_d / L_d), x_d the global coordinate of local xl
+std::vector<double> phase_tables(const p2_ctx* c, const int* moms, int nmom, int sign, int Lmax);
 p2_status make_plan(p2_ctx* c, const p2_request& r, Plan& pl);
-p2_status chunk_view(p2_ctx* c, const p2_prop& p, DevBuf& stage, int t_begin, int n, p2::ContractArgs& a, bool is_u);
+p2_status upload_async(p2_ctx* c, DevBuf& b, const void* src, size_t bytes, const char* what);
 
 }  // namespace p2host
 
 namespace p2 {
 // split-FP16 path (precision.cu)
-p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, int nprops, const p2_request* reqs, int nreq);
+// requests reqs[idx[..]] share contractions, momenta (pl) and input precision;
+// outs[j] is the device result of request j
+p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request* reqs, const int* idx, int nidx,
+                              const p2host::Plan& pl, double* const* outs);
 void precision_release(p2_ctx* c);
 }  // namespace p2

@@ -13,32 +13,40 @@ struct CompOffsets {
   int nuc, diso12, diso32, g16, all34, new10, diag10;
 };
 
-struct ContractArgs {
-  const void* u;
+// One time slice of one request, as the kernels see it.  A launch covers an
+// array of slices, possibly from many sources with different windows.
+struct SliceDesc {
+  const void* u;           // propagator views (SoA [144][vol])
   const void* d;
-  long long vol_u, vol_d;  // component stride of the views (V3 * nt)
-  int t_first_u, t_first_d;
-  int V3, T;
-  int t0;
-  int tau0, ntau;  // source-relative times of this chunk
+  long long vol_u, vol_d;  // component strides of the views
+  long long off_u, off_d;  // element offset of this slice inside the views (j * V3)
+  double* out;             // result of the slice's request
+  int tau;                 // source-relative time of the slice
+  int totalT;              // window of the request (result layout)
+  int x0[3];               // spatial source position of the request
+  int pad;
+};
+
+struct ContractArgs {
+  const SliceDesc* sl;  // [ntau] slices of this launch
+  int ntau;
+  int V3;
   unsigned what;
   int K;
   CompOffsets k;
   void* out;  // [ntau][K][V3] complex (double for the plain form, float for the split form)
-  // split form only: power-of-two scale exponents per chunk slice (input x 2^-E),
-  // and the running max |Re|,|Im| per (slice, component) as float bits
-  const int* exp_u;
-  const int* exp_d;
+  // split form only: power-of-two scale exponents per slice and flavour
+  // (input x 2^-E, exps[2 s + f]), and max(|Re|,|Im|) per (slice, component) as float bits
+  const int* exps;
   int* cmax;  // [ntau][K]
 };
 
-// Per-slice magnitude exponents of a propagator view, from a strided sample.
+// Per-slice magnitude exponents of the u and d views, from a strided sample.
 struct SampleArgs {
-  const void* p;
+  const SliceDesc* sl;
   int fp32;
-  long long vol;
-  int t_first, V3, T, t0, tau0, ntau;
-  int* exp_out;  // [ntau]
+  int V3, ntau;
+  int* exp_out;  // [ntau][2]
 };
 
 struct ProjArgs {
@@ -46,7 +54,7 @@ struct ProjArgs {
   long long sT, sK;
   int ntau, K, V3, nmom;
   int Lx, Ly, Lz, Lmax;
-  const double* tab;        // [3][nmom][Lmax] complex: exp(sign i 2 pi n_d (x_d - x0_d) / L_d)
+  const double* tab;        // [3][nmom][Lmax] complex: exp(sign i 2 pi n_d x_d / L_d)
   int nsplit, chunk;        // site range per split (multiple of 16)
   double* part;             // [ntau][nsplit][nmom][K] complex
 };
@@ -60,21 +68,27 @@ struct ScatterBlock {
 struct ScatterArgs {
   const double* part;  // [ntau][nsplit][nmom][K]
   int ntau, nsplit, nmom, K;
-  int tau0, totalT;
+  // block layout (nblocks > 0): slice tl goes to sl[tl].out at time sl[tl].tau
+  // and is multiplied by the source phase exp(i p.x0) (phases have origin 0)
   int nblocks;
-  ScatterBlock blk[kMaxBlocks];
+  ScatterBlock blk[kMaxBlocks];  // base = block offset per unit of (totalT * nmom)
+  const SliceDesc* sl;
+  const int* moms;  // [nmom][3]
+  int L[3];
   // generic [t][dof][mom] layout when nblocks == 0: out[(tau0+tau)*oT + k*oK + p]
+  int tau0;
   long long oT, oK;
   double* out;
 };
 
 // ---- split-FP16 projection ------------------------------------------------
 // Phase rows: for every representative momentum h of a +-h pair, a cos row and
-// (h != 0) a sin row; cos(h.(x-x0)) and sin(h.(x-x0)) over the sites, stored
+// (h != 0) a sin row; cos(h.x) and sin(h.x) over the sites (origin 0; the
+// source's phase exp(i p.x0) is applied in the FP64 reduction), stored
 // as hi+lo FP16 tiles of 128 rows x 64 sites in the tensor core's 128-byte
 // swizzled K-major layout: A[mtile][kstep][hi, lo][128 x 64].
 struct PhaseBuildArgs {
-  const double* tab;  // [3][nh][Lmax] complex, exp(-i 2 pi h_d (x_d - x0_d) / L_d)
+  const double* tab;  // [3][nh][Lmax] complex, exp(-i 2 pi h_d x_d / L_d)
   const int* row_h;   // [nrows] representative of each row
   const int* row_sin; // [nrows] 0 = cos row, 1 = sin row
   int nrows, nmtile, nkstep, V3, Lx, Ly, Lmax, nh;
@@ -84,7 +98,7 @@ struct PhaseBuildArgs {
 struct SplitGemmArgs {
   const void* c;     // complex float [ntau][K][V3]
   const int* cmax;   // [ntau][K] max(|Re|,|Im|) as float bits
-  const void* A;     // phase tiles
+  const void* A;     // phase tiles (origin x = 0, shared by all sources)
   int ntau, K, V3, nkstep, nmtile;
   int NT, ntile;     // components per N-tile (multiple of 16, <= 144), N-tiles
   int ks_per_split, nsplit;
@@ -96,15 +110,14 @@ struct SplitReduceArgs {
   const float* part;
   int ntau, nsplit, nmtile, ncols, NT;
   int nmom, K;
-  const int* mom_row;  // [nmom][3]: cos row, sin row (-1 for h = 0), sign (+1: p = h, -1: p = -h)
+  const int* mom_row;  // [nmom][6]: cos row, sin row (-1 for h = 0), sign (+1: p = h, -1: p = -h), p
+  int L[3];            // global spatial extents (source phase exp(i p.x0))
   const int* cmax;     // [ntau][K]
-  const int* exp_u;    // [ntau]
-  const int* exp_d;    // [ntau]
+  const int* exps;     // [ntau][2]
   const int* kexp;     // [K][2]: powers of the u and d scales in component k
-  int tau0, totalT;
+  const SliceDesc* sl; // result location of each slice
   int nblocks;
-  ScatterBlock blk[kMaxBlocks];
-  double* out;
+  ScatterBlock blk[kMaxBlocks];  // base = block offset per unit of (totalT * nmom)
 };
 
 cudaError_t launch_build_phases(const PhaseBuildArgs& a, cudaStream_t s);

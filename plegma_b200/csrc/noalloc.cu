@@ -134,7 +134,6 @@ extern "C" p2_status p2_ft_apply_noalloc(p2_ctx* c, const double* field, int dof
   sa.nmom = nmom;
   sa.K = dof;
   sa.tau0 = 0;
-  sa.totalT = nt;
   sa.nblocks = 0;
   sa.oT = (long long)dof * nmom;
   sa.oK = nmom;

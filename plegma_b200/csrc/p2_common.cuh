@@ -101,4 +101,19 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+// exp(i 2 pi sum_d p_d x0_d / L_d): the phase that moves a projection with
+// origin 0 to the source x0; each p_d x0_d is reduced mod L_d in integers.
+__device__ __forceinline__ Cx<double> source_phase(const int* p, const int* x0, const int* L) {
+  double frac = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    int m = (int)(((long long)p[d] * x0[d]) % L[d]);
+    if (m < 0) m += L[d];
+    frac += (double)m / (double)L[d];
+  }
+  double sn, cs;
+  sincospi(2.0 * frac, &sn, &cs);
+  return cx<double>(cs, sn);
+}
+
 }  // namespace p2

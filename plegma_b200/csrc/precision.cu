@@ -1,13 +1,14 @@
 // Split-FP16 form: orchestration of the FP32 site contraction and the
 // tensor-core projection (project_split.cu) for one or more requests.
 //
-// Per chunk of time slices:
+// Per chunk of time slices (from one or many requests):
 //   1. per-slice exponents E_u, E_d from a strided sample of each propagator;
 //   2. FP32 contraction of the inputs scaled by 2^-E, plus max |c_k| per slice;
 //   3. hi+lo FP16 projection GEMM on tcgen05 with FP32 accumulation in TMEM;
 //   4. FP64 reduction over site splits, pair recombination
-//        C(+-h) = (Cc_re +- Cs_im) + i (Cc_im -+ Cs_re),
-//      and exact un-scaling by 2^(n_u E_u + n_d E_d - s_k).
+//        S(+-h) = (Cc_re +- Cs_im) + i (Cc_im -+ Cs_re),
+//      exact un-scaling by 2^(n_u E_u + n_d E_d - s_k), and the source phase
+//      C(p) = exp(i p.x0) S(p).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -96,36 +97,24 @@ PhaseRows phase_rows(const std::vector<int>& moms) {
   return pr;
 }
 
-template <typename T>
-p2_status upload(p2_ctx* c, DevBuf& b, const std::vector<T>& v, const char* what) {
-  P2_TRY(c, b.ensure(std::max<size_t>(v.size() * sizeof(T), 16)), what);
-  P2_TRY(c, cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream), what);
-  return P2_OK;
-}
-
-p2_status run_one(p2_ctx* c, const p2_prop* props, const p2_request& r) {
-  Plan pl;
-  p2_status st = make_plan(c, r, pl);
-  if (st != P2_OK) return st;
-  const p2_prop& u = props[r.prop_u];
-  const p2_prop& d = props[r.prop_d];
-  if (u.precision != d.precision) return c->fail(P2_ERR_UNSUPPORTED, "u and d must share a precision");
-  const int fp32_in = u.precision == P2_FP32;
-  const int K = pl.K;
-
-  // phase rows of the +-p pairs and their hi/lo FP16 tiles
+// Phase tiles, momentum rows and component exponents, rebuilt only when the
+// momentum list or the contraction set changes (the tiles have origin 0, so
+// every source shares them).
+p2_status prepare_tables(p2_ctx* c, const Plan& pl, unsigned what, int& nmtile, int& nkstep) {
   PhaseRows pr = phase_rows(pl.moms);
   const int nh = (int)pr.reps.size() / 3;
   const int nrows = (int)pr.row_h.size();
-  const int nmtile = (nrows + 127) / 128;
-  const int nkstep = (int)((c->V3 + 63) / 64);
-  std::vector<double> tabh = phase_tables(c, pr.reps.data(), nh, r.source, -1, pl.Lmax);
-  if ((st = upload(c, c->tab, tabh, "phase table")) != P2_OK) return st;
-  std::vector<int> rows(pr.row_h);
-  rows.insert(rows.end(), pr.row_sin.begin(), pr.row_sin.end());
-  if ((st = upload(c, c->rowtab, rows, "phase rows")) != P2_OK) return st;
-  P2_TRY(c, c->phaseA.ensure((size_t)nmtile * nkstep * 2 * 128 * 64 * 2), "phase tiles alloc");
-  {
+  nmtile = (nrows + 127) / 128;
+  nkstep = (int)((c->V3 + 63) / 64);
+  p2_status st;
+  if (c->split_moms_key != pl.moms) {
+    c->split_moms_key.clear();
+    std::vector<double> tabh = phase_tables(c, pr.reps.data(), nh, -1, pl.Lmax);
+    if ((st = upload_async(c, c->tab, tabh.data(), tabh.size() * sizeof(double), "phase table")) != P2_OK) return st;
+    std::vector<int> rows(pr.row_h);
+    rows.insert(rows.end(), pr.row_sin.begin(), pr.row_sin.end());
+    if ((st = upload_async(c, c->rowtab, rows.data(), rows.size() * sizeof(int), "phase rows")) != P2_OK) return st;
+    P2_TRY(c, c->phaseA.ensure((size_t)nmtile * nkstep * 2 * 128 * 64 * 2), "phase tiles alloc");
     p2::PhaseBuildArgs b{};
     b.tab = (const double*)c->tab.p;
     b.row_h = (const int*)c->rowtab.p;
@@ -139,124 +128,23 @@ p2_status run_one(p2_ctx* c, const p2_prop* props, const p2_request& r) {
     b.Lmax = pl.Lmax;
     b.nh = nh;
     b.A = c->phaseA.p;
-    ProfScope ps(c, "build_phase_tiles");
-    P2_TRY(c, p2::launch_build_phases(b, c->stream), "phase tiles");
-  }
-  if ((st = upload(c, c->momrow, pr.mom_row, "momentum rows")) != P2_OK) return st;
-  if ((st = upload(c, c->kexp, component_exponents(r.contractions), "component exponents")) != P2_OK) return st;
-
-  double* dres = r.out;
-  if (r.out_location == P2_HOST) {
-    P2_TRY(c, c->res.ensure(pl.total * 16), "result alloc");
-    P2_TRY(c, cudaMemsetAsync(c->res.p, 0, pl.total * 16, c->stream), "result clear");
-    dres = (double*)c->res.p;
-  }
-
-  // N tiling: at most 144 components (288 TMEM columns) per CTA
-  const int ntile = (K + 143) / 144;
-  const int NT = ((K + ntile - 1) / ntile + 15) / 16 * 16;
-  // chunk of slices: FP32 position buffer within the workspace budget
-  const size_t per_slice = (size_t)K * c->V3 * 8;
-  const int tc = (int)std::max<size_t>(1, std::min<size_t>(c->ws_budget / std::max<size_t>(per_slice, 1), c->T));
-  P2_TRY(c, c->cbuf.ensure((size_t)tc * per_slice), "position buffer alloc");
-  P2_TRY(c, c->expb.ensure((size_t)2 * tc * sizeof(int)), "exponent alloc");
-  P2_TRY(c, c->cmaxb.ensure((size_t)tc * K * sizeof(int)), "maxima alloc");
-
-  const std::vector<Chunk> chunks = make_chunks(c, local_runs(c, u, d, r.source, r.totalT), r.source, tc);
-  Uploader up(c, u, d);
-  for (size_t i = 0; i < chunks.size() && i < 2; i++)
-    if ((st = up.issue((int)i, chunks[i])) != P2_OK) return st;
-  for (size_t ci = 0; ci < chunks.size(); ci++) {
     {
-      const Chunk& ch = chunks[ci];
-      const int slot = (int)(ci & 1);
-      const int n = ch.n;
-      const int tau0 = ch.tau0;
-      p2::ContractArgs a{};
-      if ((st = up.view(slot, ch, a)) != P2_OK) return st;
-      int* eu = (int*)c->expb.p;
-      int* ed = eu + tc;
-      {
-        ProfScope ps(c, "sample_exponents");
-        p2::SampleArgs sa{a.u, fp32_in, a.vol_u, a.t_first_u, (int)c->V3, c->T, r.source[3], tau0, n, eu};
-        P2_TRY(c, p2::launch_sample_exponents(sa, c->stream), "exponent sample");
-        p2::SampleArgs sd{a.d, fp32_in, a.vol_d, a.t_first_d, (int)c->V3, c->T, r.source[3], tau0, n, ed};
-        P2_TRY(c, p2::launch_sample_exponents(sd, c->stream), "exponent sample");
-      }
-      P2_TRY(c, cudaMemsetAsync(c->cmaxb.p, 0, (size_t)n * K * sizeof(int), c->stream), "maxima clear");
-      a.V3 = (int)c->V3;
-      a.T = c->T;
-      a.t0 = r.source[3];
-      a.tau0 = tau0;
-      a.ntau = n;
-      a.what = r.contractions;
-      a.K = K;
-      a.k = offsets_of(r.contractions);
-      a.out = c->cbuf.p;
-      a.exp_u = eu;
-      a.exp_d = ed;
-      a.cmax = (int*)c->cmaxb.p;
-      {
-        ProfScope ps(c, "contract_f32");
-        P2_TRY(c, p2::launch_contract_f32(a, fp32_in, 2 * c->nsm, c->stream), "contract kernel");
-      }
-      if ((st = up.release(slot)) != P2_OK) return st;
-      if (ci + 2 < chunks.size() && (st = up.issue(slot, chunks[ci + 2])) != P2_OK) return st;
-      // projection GEMM: enough CTAs for about two waves
-      const int per = ntile * nmtile * n;
-      int nsplit = std::max(1, (2 * c->nsm + per - 1) / per);
-      nsplit = std::min(nsplit, nkstep);
-      const int ks_per = (nkstep + nsplit - 1) / nsplit;
-      nsplit = (nkstep + ks_per - 1) / ks_per;
-      const int ncols = ntile * 2 * NT;
-      P2_TRY(c, c->fpart.ensure((size_t)n * nsplit * nmtile * 128 * ncols * sizeof(float)), "partials alloc");
-      p2::SplitGemmArgs g{};
-      g.c = c->cbuf.p;
-      g.cmax = (const int*)c->cmaxb.p;
-      g.A = c->phaseA.p;
-      g.ntau = n;
-      g.K = K;
-      g.V3 = (int)c->V3;
-      g.nkstep = nkstep;
-      g.nmtile = nmtile;
-      g.NT = NT;
-      g.ntile = ntile;
-      g.ks_per_split = ks_per;
-      g.nsplit = nsplit;
-      g.part = (float*)c->fpart.p;
-      g.err = (int*)c->errflag.p;
-      {
-        ProfScope ps(c, "project_split_tc");
-        P2_TRY(c, p2::launch_project_split(g, c->stream), "tensor-core projection");
-      }
-      p2::SplitReduceArgs rd{};
-      rd.part = (const float*)c->fpart.p;
-      rd.ntau = n;
-      rd.nsplit = nsplit;
-      rd.nmtile = nmtile;
-      rd.ncols = ncols;
-      rd.NT = NT;
-      rd.nmom = pl.nmom;
-      rd.K = K;
-      rd.mom_row = (const int*)c->momrow.p;
-      rd.cmax = (const int*)c->cmaxb.p;
-      rd.exp_u = eu;
-      rd.exp_d = ed;
-      rd.kexp = (const int*)c->kexp.p;
-      rd.tau0 = tau0;
-      rd.totalT = r.totalT;
-      rd.nblocks = (int)pl.blocks.size();
-      for (size_t b = 0; b < pl.blocks.size(); b++) rd.blk[b] = pl.blocks[b];
-      rd.out = dres;
-      {
-        ProfScope ps(c, "split_reduce");
-        P2_TRY(c, p2::launch_split_reduce(rd, c->stream), "split reduction");
-      }
+      ProfScope ps(c, "build_phase_tiles");
+      P2_TRY(c, p2::launch_build_phases(b, c->stream), "phase tiles");
     }
+    // [nmom][6]: cos row, sin row, sign, p
+    std::vector<int> mr;
+    for (int p = 0; p < pl.nmom; p++) {
+      for (int q = 0; q < 3; q++) mr.push_back(pr.mom_row[3 * p + q]);
+      for (int q = 0; q < 3; q++) mr.push_back(pl.moms[3 * p + q]);
+    }
+    if ((st = upload_async(c, c->momrow, mr.data(), mr.size() * sizeof(int), "momentum rows")) != P2_OK) return st;
+    c->split_moms_key = pl.moms;
   }
-  if (r.out_location == P2_HOST) {
-    P2_TRY(c, cudaMemcpyAsync(r.out, dres, pl.total * 16, cudaMemcpyDeviceToHost, c->stream), "result download");
-    P2_TRY(c, cudaStreamSynchronize(c->stream), "result download");
+  if (c->split_what_key != what) {
+    std::vector<int> ke = component_exponents(what);
+    if ((st = upload_async(c, c->kexp, ke.data(), ke.size() * sizeof(int), "component exponents")) != P2_OK) return st;
+    c->split_what_key = what;
   }
   return P2_OK;
 }
@@ -265,17 +153,118 @@ p2_status run_one(p2_ctx* c, const p2_prop* props, const p2_request& r) {
 
 namespace p2 {
 
-p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, int nprops, const p2_request* reqs, int nreq) {
-  (void)nprops;
+p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request* reqs, const int* idx, int nidx,
+                              const Plan& pl, double* const* outs) {
   if (!c->errflag.p) {
     P2_TRY(c, c->errflag.ensure(16), "error flag alloc");
     P2_TRY(c, cudaMemsetAsync(c->errflag.p, 0, 16, c->stream), "error flag clear");
   }
   if (c->project_split_smem_max < p2::project_split_smem_bytes(144))
     return c->fail(P2_ERR_UNSUPPORTED, "device shared memory per block too small for the tensor-core projection");
-  for (int i = 0; i < nreq; i++) {
-    p2_status s = run_one(c, props, reqs[i]);
-    if (s != P2_OK) return s;
+  const p2_request& r0 = reqs[idx[0]];
+  const unsigned what = r0.contractions;
+  for (int q = 0; q < nidx; q++) {
+    const p2_request& r = reqs[idx[q]];
+    if (props[r.prop_u].precision != props[r.prop_d].precision)
+      return c->fail(P2_ERR_UNSUPPORTED, "u and d must share a precision");
+  }
+  const int fp32_in = props[r0.prop_u].precision == P2_FP32;
+  const int K = pl.K;
+  int nmtile = 0, nkstep = 0;
+  p2_status st = prepare_tables(c, pl, what, nmtile, nkstep);
+  if (st != P2_OK) return st;
+
+  // N tiling: at most 144 components (288 TMEM columns) per CTA
+  const int ntile = (K + 143) / 144;
+  const int NT = ((K + ntile - 1) / ntile + 15) / 16 * 16;
+  // chunk of slices: FP32 position buffer within the workspace budget
+  const size_t per_slice = (size_t)K * c->V3 * 8;
+  const int tc = (int)std::max<size_t>(1, std::min<size_t>(c->ws_budget / std::max<size_t>(per_slice, 1), c->T));
+  const Work w = make_work(c, props, reqs, idx, nidx, tc);
+  if (w.sl.empty()) return P2_OK;
+  const int mx = w.max_n;
+  P2_TRY(c, c->cbuf.ensure((size_t)mx * per_slice), "position buffer alloc");
+  P2_TRY(c, c->expb.ensure((size_t)2 * mx * sizeof(int)), "exponent alloc");
+  P2_TRY(c, c->cmaxb.ensure((size_t)mx * K * sizeof(int)), "maxima alloc");
+  Stager sg(c, props, reqs, w);
+  if ((st = sg.prepare(outs)) != P2_OK) return st;
+
+  for (int i = 0; i < 2; i++)
+    if ((st = sg.issue(i)) != P2_OK) return st;
+  for (size_t ci = 0; ci < w.chunks.size(); ci++) {
+    const int n = w.chunks[ci].n;
+    const SliceDesc* dsl = sg.desc((int)ci);
+    if ((st = sg.wait((int)ci)) != P2_OK) return st;
+    {
+      ProfScope ps(c, "sample_exponents");
+      p2::SampleArgs sa{dsl, fp32_in, (int)c->V3, n, (int*)c->expb.p};
+      P2_TRY(c, p2::launch_sample_exponents(sa, c->stream), "exponent sample");
+    }
+    P2_TRY(c, cudaMemsetAsync(c->cmaxb.p, 0, (size_t)n * K * sizeof(int), c->stream), "maxima clear");
+    p2::ContractArgs a{};
+    a.sl = dsl;
+    a.V3 = (int)c->V3;
+    a.ntau = n;
+    a.what = what;
+    a.K = K;
+    a.k = offsets_of(what);
+    a.out = c->cbuf.p;
+    a.exps = (const int*)c->expb.p;
+    a.cmax = (int*)c->cmaxb.p;
+    {
+      ProfScope ps(c, "contract_f32");
+      P2_TRY(c, p2::launch_contract_f32(a, fp32_in, 2 * c->nsm, c->stream), "contract kernel");
+    }
+    if ((st = sg.release((int)ci)) != P2_OK) return st;
+    if ((st = sg.issue((int)ci + 2)) != P2_OK) return st;
+    // projection GEMM: enough CTAs for about two waves
+    const int per = ntile * nmtile * n;
+    int nsplit = std::max(1, (2 * c->nsm + per - 1) / per);
+    nsplit = std::min(nsplit, nkstep);
+    const int ks_per = (nkstep + nsplit - 1) / nsplit;
+    nsplit = (nkstep + ks_per - 1) / ks_per;
+    const int ncols = ntile * 2 * NT;
+    P2_TRY(c, c->fpart.ensure((size_t)n * nsplit * nmtile * 128 * ncols * sizeof(float)), "partials alloc");
+    p2::SplitGemmArgs g{};
+    g.c = c->cbuf.p;
+    g.cmax = (const int*)c->cmaxb.p;
+    g.A = c->phaseA.p;
+    g.ntau = n;
+    g.K = K;
+    g.V3 = (int)c->V3;
+    g.nkstep = nkstep;
+    g.nmtile = nmtile;
+    g.NT = NT;
+    g.ntile = ntile;
+    g.ks_per_split = ks_per;
+    g.nsplit = nsplit;
+    g.part = (float*)c->fpart.p;
+    g.err = (int*)c->errflag.p;
+    {
+      ProfScope ps(c, "project_split_tc");
+      P2_TRY(c, p2::launch_project_split(g, c->stream), "tensor-core projection");
+    }
+    p2::SplitReduceArgs rd{};
+    rd.part = (const float*)c->fpart.p;
+    rd.ntau = n;
+    rd.nsplit = nsplit;
+    rd.nmtile = nmtile;
+    rd.ncols = ncols;
+    rd.NT = NT;
+    rd.nmom = pl.nmom;
+    rd.K = K;
+    rd.mom_row = (const int*)c->momrow.p;
+    for (int d = 0; d < 3; d++) rd.L[d] = c->g.L[d];
+    rd.cmax = (const int*)c->cmaxb.p;
+    rd.exps = (const int*)c->expb.p;
+    rd.kexp = (const int*)c->kexp.p;
+    rd.sl = dsl;
+    rd.nblocks = (int)pl.blocks.size();
+    for (size_t b = 0; b < pl.blocks.size(); b++) rd.blk[b] = pl.blocks[b];
+    {
+      ProfScope ps(c, "split_reduce");
+      P2_TRY(c, p2::launch_split_reduce(rd, c->stream), "split reduction");
+    }
   }
   return P2_OK;
 }
@@ -283,6 +272,8 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, int nprops, const
 void precision_release(p2_ctx* c) {
   for (DevBuf* b : {&c->phaseA, &c->expb, &c->cmaxb, &c->momrow, &c->kexp, &c->fpart, &c->rowtab, &c->errflag})
     b->release();
+  c->split_moms_key.clear();
+  c->split_what_key = 0;
 }
 
 }  // namespace p2

@@ -2,7 +2,7 @@
 //
 // C(t, p, k) = sum_x c_k(x, t) exp(sign * i p.(x - x0)), the reference's
 // fourier_transform_3D (lib/kernels/PLEGMA_kernel_utils.cuh:820-860) and the
-// host block sum after it (PLEGMA_baryons.cuh:197-206, PLEGMA_mesons*.cuh).
+// host block sum after it (PLEGMA_baryons.cuh:146-155,198, PLEGMA_mesons*.cuh).
 // Per time slice this is a complex [nmom x V3] . [V3 x K] product; the phase
 // matrix is never stored: each entry is the product of three per-dimension
 // phase tables (p.x = sum_d n_d x_d), built on the host in double precision.
@@ -112,21 +112,23 @@ __global__ void k_scatter(const ScatterArgs a) {
     const Cx<double>* src = (const Cx<double>*)a.part + ((long long)tau * a.nsplit * a.nmom + p) * a.K + k;
     Cx<double> s = czero<double>();
     for (int sp = 0; sp < a.nsplit; sp++) s = s + src[(long long)sp * a.nmom * a.K];
-    long long o = -1;
     if (a.nblocks == 0) {
-      o = (long long)(a.tau0 + tau) * a.oT + (long long)k * a.oK + p;
-    } else {
-      for (int b = 0; b < a.nblocks; b++) {
-        const ScatterBlock& B = a.blk[b];
-        const int rel = k - B.k0;
-        if (rel >= 0 && rel < B.groups * B.datasets * B.comps) {
-          const int comp = rel % B.comps;
-          const int gd = rel / B.comps;  // group * datasets + dataset
-          o = B.base + (((long long)gd * a.totalT + a.tau0 + tau) * a.nmom + p) * B.comps + comp;
-        }
+      ((Cx<double>*)a.out)[(long long)(a.tau0 + tau) * a.oT + (long long)k * a.oK + p] = s;
+      continue;
+    }
+    const SliceDesc& sd = a.sl[tau];
+    s = cmul(s, source_phase(a.moms + 3 * p, sd.x0, a.L));
+    for (int b = 0; b < a.nblocks; b++) {
+      const ScatterBlock& B = a.blk[b];
+      const int rel = k - B.k0;
+      if (rel >= 0 && rel < B.groups * B.datasets * B.comps) {
+        const int comp = rel % B.comps;
+        const int gd = rel / B.comps;  // group * datasets + dataset
+        const long long o = B.base * sd.totalT * a.nmom +
+                            (((long long)gd * sd.totalT + sd.tau) * a.nmom + p) * B.comps + comp;
+        ((Cx<double>*)sd.out)[o] = s;
       }
     }
-    if (o >= 0) ((Cx<double>*)a.out)[o] = s;
   }
 }
 

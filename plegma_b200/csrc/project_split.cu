@@ -6,9 +6,10 @@
 // lib/kernels/PLEGMA_kernel_utils.cuh:820-860).  Here it runs as a real GEMM
 //
 //   D[row][n] = sum_x A[row][x] B[n][x]
-//   rows: cos(h.(x-x0)) and sin(h.(x-x0)) for one representative h of every
-//         +-p pair (123 momenta -> 123 rows, one M=128 tile), so each pair
-//         costs two real rows instead of two complex rows;
+//   rows: cos(h.x) and sin(h.x) for one representative h of every +-p pair
+//         (123 momenta -> 123 rows, one M=128 tile), so each pair costs two
+//         real rows instead of two complex rows; the rows have origin 0, so
+//         every source shares them and the reduction applies exp(i p.x0);
 //   n:    Re and Im of every component (2K columns).
 //
 // Both operands are split into FP16 hi + lo parts (hi = fp16(v), lo =
@@ -257,12 +258,13 @@ __global__ void k_split_reduce(const SplitReduceArgs a) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int k = (int)(i % a.K);
     const int p = (int)((i / a.K) % a.nmom);
-    const int tau = (int)(i / ((long long)a.K * a.nmom));
-    const int rc = a.mom_row[3 * p], rs = a.mom_row[3 * p + 1], sg = a.mom_row[3 * p + 2];
+    const int tl = (int)(i / ((long long)a.K * a.nmom));
+    const int* mr = a.mom_row + 6 * p;
+    const int rc = mr[0], rs = mr[1], sg = mr[2];
     const int col = (k / a.NT) * 2 * a.NT + 2 * (k % a.NT);
     double cr = 0, ci = 0, sr = 0, si = 0;
     for (int sp = 0; sp < a.nsplit; sp++) {
-      const float* base = a.part + ((long long)tau * a.nsplit + sp) * a.nmtile * 128 * (long long)a.ncols;
+      const float* base = a.part + ((long long)tl * a.nsplit + sp) * a.nmtile * 128 * (long long)a.ncols;
       const float* pc = base + (long long)rc * a.ncols + col;
       cr += (double)pc[0];
       ci += (double)pc[1];
@@ -272,20 +274,24 @@ __global__ void k_split_reduce(const SplitReduceArgs a) {
         si += (double)ps[1];
       }
     }
-    const float mx = __int_as_float(a.cmax[(long long)tau * a.K + k]);
+    const float mx = __int_as_float(a.cmax[(long long)tl * a.K + k]);
     int e = 0;
     if (mx > 0.f) frexpf(mx, &e);
-    const int pw = a.kexp[2 * k] * a.exp_u[tau] + a.kexp[2 * k + 1] * a.exp_d[tau] - (14 - e);
+    const int pw = a.kexp[2 * k] * a.exps[2 * tl] + a.kexp[2 * k + 1] * a.exps[2 * tl + 1] - (14 - e);
     const double f = ldexp(1.0, pw);
-    Cx<double> v = cx<double>((cr + sg * si) * f, (ci - sg * sr) * f);
+    // S(p) = sum_x c e^{-i p.x}; the source phase: C(p) = e^{i p.x0} S(p), with
+    // p.x0 / L reduced exactly in integers per dimension
+    const SliceDesc& sd = a.sl[tl];
+    const Cx<double> v = cmul(cx<double>((cr + sg * si) * f, (ci - sg * sr) * f), source_phase(mr + 3, sd.x0, a.L));
     for (int b = 0; b < a.nblocks; b++) {
       const ScatterBlock& B = a.blk[b];
       const int rel = k - B.k0;
       if (rel >= 0 && rel < B.groups * B.datasets * B.comps) {
         const int comp = rel % B.comps;
         const int gd = rel / B.comps;
-        const long long o = B.base + (((long long)gd * a.totalT + a.tau0 + tau) * a.nmom + p) * B.comps + comp;
-        ((Cx<double>*)a.out)[o] = v;
+        const long long o = B.base * sd.totalT * a.nmom +
+                            (((long long)gd * sd.totalT + sd.tau) * a.nmom + p) * B.comps + comp;
+        ((Cx<double>*)sd.out)[o] = v;
       }
     }
   }

@@ -71,7 +71,7 @@ class P2KernelTime(C.Structure):
 EXPORTS = ["p2_ctx_create", "p2_ctx_destroy", "p2_last_error", "p2_sync", "p2_set_stream", "p2_components",
            "p2_mom_list", "p2_block_info", "p2_contract_project", "p2_contract_position", "p2_ft_apply",
            "p2_synth_propagator", "p2_profile_enable", "p2_profile_read", "p2_alloc", "p2_free", "p2_copy",
-           "p2_ft_apply_noalloc"]
+           "p2_ft_apply_noalloc", "p2_set_workspace"]
 
 _lib = None
 
@@ -89,6 +89,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.p2_last_error.restype = C.c_char_p
     lib.p2_sync.argtypes = [C.c_void_p]
     lib.p2_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    lib.p2_set_workspace.argtypes = [C.c_void_p, C.c_size_t]
     lib.p2_components.argtypes = [C.c_uint]
     lib.p2_mom_list.argtypes = [C.c_int, C.POINTER(C.c_int)]
     lib.p2_block_info.argtypes = [C.c_uint, C.c_int, C.c_int, C.POINTER(P2Block), C.c_int, C.POINTER(C.c_size_t)]
@@ -172,6 +173,10 @@ class Context:
     def sync(self):
         self.check(self.lib.p2_sync(self.h))
 
+    def set_workspace(self, nbytes: int):
+        """p2_set_workspace: cap on the per-chunk position-space buffer."""
+        self.check(self.lib.p2_set_workspace(self.h, nbytes))
+
     def set_stream(self, stream_ptr: Optional[int]):
         self.check(self.lib.p2_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
 
@@ -181,8 +186,9 @@ class Context:
         self.check(self.lib.p2_synth_propagator(self.h, C.c_void_p(ptr), int(on_device), precision, seed, flavour,
                                                 t0, decay, t_first, nt))
 
-    @staticmethod
-    def prop(ptr: int, precision=P2_FP64, location=P2_DEVICE, t_first=0, nt=None) -> P2Prop:
+    def prop(self, ptr: int, precision=P2_FP64, location=P2_DEVICE, t_first=0, nt=None) -> P2Prop:
+        """A propagator view; nt defaults to the local time extent."""
+        nt = self.Ll[3] if nt is None else nt
         p = P2Prop()
         p.data = ptr
         p.precision = precision
