@@ -192,6 +192,39 @@ p2_status p2_ft_apply(p2_ctx* ctx, const double* field, int dof, int nt, const i
 p2_status p2_ft_apply_noalloc(p2_ctx* ctx, const double* field, int dof, int nt, const int* moms, int nmom,
                               int sign, double* out);
 
+/* ---- CUDA graphs -------------------------------------------------------- */
+/* The whole launch sequence of p2_contract_project(props, reqs) recorded once
+ * and replayed with one cudaGraphLaunch: batched sources in one submission,
+ * no per-call host work.  Creation runs the requests once eagerly (results
+ * are written), then records them; the graph keeps its own workspaces, so
+ * other calls on the context may run between replays.  Propagator and result
+ * pointers are those given at creation: refill the propagator buffers in place
+ * between launches.  Device-resident propagators and results only.  Errors
+ * are reported on the parent context.  No counterpart in the reference (it
+ * launches each kernel from the host and synchronises after each,
+ * lib/kernels/PLEGMA_baryons.cuh:134-164). */
+typedef struct p2_graph p2_graph;
+p2_status p2_graph_create(p2_ctx* ctx, const p2_prop* props, int nprops, const p2_request* reqs, int nreq,
+                          p2_graph** graph);
+/* Enqueue one replay on `stream` (a cudaStream_t; NULL = the context's stream). */
+p2_status p2_graph_launch(p2_graph* graph, void* stream);
+/* Wait for the last replay and check its device-side error flag. */
+p2_status p2_graph_sync(p2_graph* graph);
+p2_status p2_graph_destroy(p2_graph* graph);
+
+/* ---- autotuning -------------------------------------------------------- */
+/* With tuning on, the first call with a new shape times the candidate launch
+ * shapes of the tunable kernels (tensor-core projection: N-tile width and
+ * site splits; FP64 projection: component tile and site splits) and keeps the
+ * fastest.  Choices are cached per (kernel, shape) for the context and its
+ * graphs, and, when cache_path is not NULL, in that tab-separated file (read
+ * now, rewritten after each new entry; "key<TAB>params<TAB>ms" per line).
+ * Cached choices are used even with tuning off.  The reference's counterpart
+ * is tuneAndRun with QUDA's tune cache (lib/kernels/PLEGMA_kernel_tuner.cuh). */
+p2_status p2_tune_enable(p2_ctx* ctx, int on, const char* cache_path);
+/* Entries in the context's tuning cache. */
+int p2_tune_count(p2_ctx* ctx);
+
 /* ---- memory ------------------------------------------------------------ */
 /* Field storage for callers that do not link the CUDA runtime themselves
  * (PLEGMA_Field::create_device / create_host, lib/PLEGMA_Field.cu:226-235):

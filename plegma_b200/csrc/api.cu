@@ -320,10 +320,14 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request* reqs, con
       return c->fail(P2_ERR_UNSUPPORTED, "the plain FP64 form needs FP64 propagators");
   }
   const unsigned what = reqs[idx[0]].contractions;
-  std::vector<double> tabh = phase_tables(c, pl.moms.data(), pl.nmom, -1, pl.Lmax);
   p2_status st;
-  if ((st = upload_async(c, c->tab, tabh.data(), tabh.size() * sizeof(double), "phase table")) != P2_OK) return st;
-  if ((st = upload_async(c, c->moms, pl.moms.data(), pl.moms.size() * sizeof(int), "momenta")) != P2_OK) return st;
+  if (c->plain_moms_key != pl.moms) {  // phase tables have origin 0: one set per momentum list
+    c->plain_moms_key.clear();
+    std::vector<double> tabh = phase_tables(c, pl.moms.data(), pl.nmom, -1, pl.Lmax);
+    if ((st = upload_async(c, c->ptab, tabh.data(), tabh.size() * sizeof(double), "phase table")) != P2_OK) return st;
+    if ((st = upload_async(c, c->moms, pl.moms.data(), pl.moms.size() * sizeof(int), "momenta")) != P2_OK) return st;
+    c->plain_moms_key = pl.moms;
+  }
 
   const int tc = chunk_slices(c, pl.K);
   const Work w = make_work(c, props, reqs, idx, nidx, tc);
@@ -333,7 +337,6 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request* reqs, con
   if ((st = sg.prepare(outs)) != P2_OK) return st;
 
   const int ptiles = (pl.nmom + 63) / 64;
-  const int ktiles = (pl.K + 95) / 96;
   for (int i = 0; i < 2; i++)
     if ((st = sg.issue(i)) != P2_OK) return st;
   for (size_t ci = 0; ci < w.chunks.size(); ci++) {
@@ -366,13 +369,41 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request* reqs, con
     pa.Ly = c->Ll[1];
     pa.Lz = c->Ll[2];
     pa.Lmax = pl.Lmax;
-    pa.tab = (const double*)c->tab.p;
-    int nsplit = (2 * c->nsm + ptiles * ktiles * n - 1) / (ptiles * ktiles * n);
-    nsplit = std::max(1, std::min(nsplit, (int)((c->V3 + 255) / 256)));
-    pa.chunk = (int)((((c->V3 + nsplit - 1) / nsplit) + 15) / 16 * 16);
-    pa.nsplit = (int)((c->V3 + pa.chunk - 1) / pa.chunk);
-    P2_TRY(c, c->part.ensure((size_t)w.max_n * pa.nsplit * pl.nmom * pl.K * 16), "partials alloc");
+    pa.tab = (const double*)c->ptab.p;
+    // candidates (component tile, site splits): the least-waste tile at ~2
+    // waves first, then other tiles at 1, 2 and 4 waves
+    std::vector<std::vector<int>> cands;
+    const int tk0 = p2::project_fp64_tk(pl.K, 0);
+    for (int tk : {tk0, 8, 6, 4, 2})
+      for (int waves : {2, 1, 4}) {
+        const int ktiles = (pl.K + 16 * tk - 1) / (16 * tk);
+        int nsplit = (waves * c->nsm + ptiles * ktiles * n - 1) / (ptiles * ktiles * n);
+        nsplit = std::max(1, std::min(nsplit, (int)((c->V3 + 255) / 256)));
+        const int chunk = (int)((((c->V3 + nsplit - 1) / nsplit) + 15) / 16 * 16);
+        std::vector<int> v{tk, (int)((c->V3 + chunk - 1) / chunk), chunk};
+        if (std::find(cands.begin(), cands.end(), v) == cands.end()) cands.push_back(v);
+      }
+    int maxsplit = 0;
+    for (const auto& v : cands) maxsplit = std::max(maxsplit, v[1]);
+    P2_TRY(c, c->part.ensure((size_t)w.max_n * maxsplit * pl.nmom * pl.K * 16), "partials alloc");
     pa.part = (double*)c->part.p;
+    char key[160];
+    std::snprintf(key, sizeof(key), "project_fp64 V3=%lld K=%d nmom=%d n=%d", c->V3, pl.K, pl.nmom, n);
+    std::vector<int> pick;
+    P2_TRY(c,
+           tune_choose(c->tuner.get(), key, cands, c->stream, !c->capturing,
+                       [&](const std::vector<int>& v) {
+                         p2::ProjArgs q = pa;
+                         q.tk = v[0];
+                         q.nsplit = v[1];
+                         q.chunk = v[2];
+                         return p2::launch_project_fp64(q, c->stream);
+                       },
+                       pick),
+           "projection tuning");
+    pa.tk = pick[0];
+    pa.nsplit = pick[1];
+    pa.chunk = pick[2];
     {
       ProfScope ps(c, "project_fp64");
       P2_TRY(c, p2::launch_project_fp64(pa, c->stream), "projection kernel");
@@ -530,7 +561,7 @@ p2_status p2_ctx_destroy(p2_ctx* c) {
     return P2_OK;
   }
   cudaStreamSynchronize(c->stream);
-  for (DevBuf* b : {&c->cbuf, &c->part, &c->tab, &c->res, &c->moms, &c->sdesc}) b->release();
+  for (DevBuf* b : {&c->cbuf, &c->part, &c->tab, &c->res, &c->moms, &c->sdesc, &c->ptab}) b->release();
   if (c->sdesc_host) cudaFreeHost(c->sdesc_host);
   if (c->sdesc_copied) cudaEventDestroy(c->sdesc_copied);
   for (int i = 0; i < 2; i++) {

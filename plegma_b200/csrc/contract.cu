@@ -24,6 +24,7 @@
 //  - two stages: tile i+1's copies are in flight while tile i is contracted;
 //  - half-warp h contracts site h of the tile (site_contract.cuh).
 #include "kernels.cuh"
+#include "launch_util.h"
 #include "site_contract.cuh"
 
 namespace p2 {
@@ -338,7 +339,7 @@ int contract_plain_smem_bytes() { return 2 * kStage * (int)sizeof(Cx<double>); }
 template <bool DELTA>
 cudaError_t launch_plain_t(const ContractArgs& a, int grid, cudaStream_t s) {
   const int smem = contract_plain_smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(k_contract_plain<DELTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = ensure_smem((const void*)k_contract_plain<DELTA>, smem);
   if (e != cudaSuccess) return e;
   k_contract_plain<DELTA><<<grid, kThreads, smem, s>>>(a);
   return cudaGetLastError();
@@ -347,7 +348,7 @@ cudaError_t launch_plain_t(const ContractArgs& a, int grid, cudaStream_t s) {
 template <typename Tin, bool DELTA>
 cudaError_t launch_f32_t(const ContractArgs& a, int grid, cudaStream_t s) {
   const int smem = kStage * (int)sizeof(Cx<Tin>) + kStage * (int)sizeof(Cx<float>) + a.K * (int)sizeof(int);
-  cudaError_t e = cudaFuncSetAttribute(k_contract_f32<Tin, DELTA>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = ensure_smem((const void*)k_contract_f32<Tin, DELTA>, smem);
   if (e != cudaSuccess) return e;
   k_contract_f32<Tin, DELTA><<<grid, kThreads, smem, s>>>(a);
   return cudaGetLastError();

@@ -1,11 +1,13 @@
 // Context of the C ABI and the helpers shared by the plain (api.cu) and the
 // split-FP16 (precision.cu) paths.
 #pragma once
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "../../include/plegma2pt.h"
 #include "kernels.cuh"
+#include "tuner.h"
 
 namespace p2host {
 
@@ -69,6 +71,11 @@ struct p2_ctx {
   unsigned split_what_key = 0;      // contraction set of the component exponents
   int project_split_smem_max = 0;  // opt-in shared memory per block of the device
   size_t ws_budget = 0;
+  // plain form: phase tables and momentum list, rebuilt when the momentum list changes
+  p2host::DevBuf ptab;
+  std::vector<int> plain_moms_key;
+  // launch-shape autotuner (shared with the context's graphs)
+  std::shared_ptr<p2host::Tuner> tuner = std::make_shared<p2host::Tuner>();
 
   // kernel timing (p2_profile_enable)
   struct Prof {

@@ -57,6 +57,7 @@ struct ProjArgs {
   const double* tab;        // [3][nmom][Lmax] complex: exp(sign i 2 pi n_d x_d / L_d)
   int nsplit, chunk;        // site range per split (multiple of 16)
   double* part;             // [ntau][nsplit][nmom][K] complex
+  int tk;                   // component tile 16*tk (2, 4, 6 or 8); 0: the one that wastes least
 };
 
 struct ScatterBlock {
@@ -130,6 +131,7 @@ cudaError_t launch_contract_plain(const ContractArgs& a, int grid, cudaStream_t 
 cudaError_t launch_contract_f32(const ContractArgs& a, int fp32_in, int grid, cudaStream_t s);
 cudaError_t launch_sample_exponents(const SampleArgs& a, cudaStream_t s);
 cudaError_t launch_project_fp64(const ProjArgs& a, cudaStream_t s);
+int project_fp64_tk(int K, int tk);  // component tile factor a launch with ProjArgs::tk uses
 cudaError_t launch_scatter(const ScatterArgs& a, cudaStream_t s);
 cudaError_t launch_synth(void* dst, int fp32, uint64_t seed, int flavour, int t0, double decay, int t_first, int nt,
                          const int* L, const int* Ll, const int* coords, cudaStream_t s);

@@ -11,6 +11,7 @@
 //      C(p) = exp(i p.x0) S(p).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -174,9 +175,6 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
   p2_status st = prepare_tables(c, pl, what, nmtile, nkstep);
   if (st != P2_OK) return st;
 
-  // N tiling: at most 144 components (288 TMEM columns) per CTA
-  const int ntile = (K + 143) / 144;
-  const int NT = ((K + ntile - 1) / ntile + 15) / 16 * 16;
   // chunk of slices: FP32 position buffer within the workspace budget
   const size_t per_slice = (size_t)K * c->V3 * 8;
   const int tc = (int)std::max<size_t>(1, std::min<size_t>(c->ws_budget / std::max<size_t>(per_slice, 1), c->T));
@@ -217,14 +215,26 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
     }
     if ((st = sg.release((int)ci)) != P2_OK) return st;
     if ((st = sg.issue((int)ci + 2)) != P2_OK) return st;
-    // projection GEMM: enough CTAs for about two waves
-    const int per = ntile * nmtile * n;
-    int nsplit = std::max(1, (2 * c->nsm + per - 1) / per);
-    nsplit = std::min(nsplit, nkstep);
-    const int ks_per = (nkstep + nsplit - 1) / nsplit;
-    nsplit = (nkstep + ks_per - 1) / ks_per;
-    const int ncols = ntile * 2 * NT;
-    P2_TRY(c, c->fpart.ensure((size_t)n * nsplit * nmtile * 128 * ncols * sizeof(float)), "partials alloc");
+    // projection GEMM candidates (N-tile width NT <= 144 components = 288
+    // TMEM columns, number of N-tiles, site splits, k-steps per split): the
+    // fewest N-tiles at ~2 waves first, then up to two more N-tiles at 1, 2
+    // and 4 waves
+    std::vector<std::vector<int>> cands;
+    for (int ntile = (K + 143) / 144, extra = 0; extra < 3; ntile++, extra++) {
+      const int NT = ((K + ntile - 1) / ntile + 15) / 16 * 16;
+      if ((ntile - 1) * NT >= K) continue;  // an empty N-tile
+      for (int waves : {2, 1, 4}) {
+        const int per = ntile * nmtile * n;
+        int nsplit = std::min(std::max(1, (waves * c->nsm + per - 1) / per), nkstep);
+        const int ks_per = (nkstep + nsplit - 1) / nsplit;
+        nsplit = (nkstep + ks_per - 1) / ks_per;
+        std::vector<int> v{NT, ntile, nsplit, ks_per};
+        if (std::find(cands.begin(), cands.end(), v) == cands.end()) cands.push_back(v);
+      }
+    }
+    size_t maxpart = 0;
+    for (const auto& v : cands) maxpart = std::max(maxpart, (size_t)v[2] * v[1] * 2 * v[0]);
+    P2_TRY(c, c->fpart.ensure((size_t)n * nmtile * 128 * maxpart * sizeof(float)), "partials alloc");
     p2::SplitGemmArgs g{};
     g.c = c->cbuf.p;
     g.cmax = (const int*)c->cmaxb.p;
@@ -234,12 +244,29 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
     g.V3 = (int)c->V3;
     g.nkstep = nkstep;
     g.nmtile = nmtile;
-    g.NT = NT;
-    g.ntile = ntile;
-    g.ks_per_split = ks_per;
-    g.nsplit = nsplit;
     g.part = (float*)c->fpart.p;
     g.err = (int*)c->errflag.p;
+    auto set = [&](p2::SplitGemmArgs& q, const std::vector<int>& v) {
+      q.NT = v[0];
+      q.ntile = v[1];
+      q.nsplit = v[2];
+      q.ks_per_split = v[3];
+    };
+    char key[160];
+    std::snprintf(key, sizeof(key), "project_split V3=%lld K=%d rows=%d n=%d", c->V3, K, nmtile * 128, n);
+    std::vector<int> pick;
+    P2_TRY(c,
+           tune_choose(c->tuner.get(), key, cands, c->stream, !c->capturing,
+                       [&](const std::vector<int>& v) {
+                         p2::SplitGemmArgs q = g;
+                         set(q, v);
+                         return p2::launch_project_split(q, c->stream);
+                       },
+                       pick),
+           "projection tuning");
+    set(g, pick);
+    const int NT = g.NT, nsplit = g.nsplit;
+    const int ncols = g.ntile * 2 * NT;
     {
       ProfScope ps(c, "project_split_tc");
       P2_TRY(c, p2::launch_project_split(g, c->stream), "tensor-core projection");

@@ -134,18 +134,23 @@ __global__ void k_scatter(const ScatterArgs a) {
 
 }  // namespace
 
-cudaError_t launch_project_fp64(const ProjArgs& a, cudaStream_t s) {
-  int tk = 8;
-  // pick the component tile (16*TK) that wastes least
-  int best = 1 << 30;
+int project_fp64_tk(int K, int tk) {
+  if (tk == 2 || tk == 4 || tk == 6 || tk == 8) return tk;
+  // the component tile (16*TK) that wastes least
+  int best = 1 << 30, pick = 8;
   for (int cand : {8, 6, 4, 2}) {
     const int kt = 16 * cand;
-    const int waste = ((a.K + kt - 1) / kt) * kt - a.K;
+    const int waste = ((K + kt - 1) / kt) * kt - K;
     if (waste < best) {
       best = waste;
-      tk = cand;
+      pick = cand;
     }
   }
+  return pick;
+}
+
+cudaError_t launch_project_fp64(const ProjArgs& a, cudaStream_t s) {
+  const int tk = project_fp64_tk(a.K, a.tk);
   const int ptiles = (a.nmom + kPT - 1) / kPT;
   const int ktiles = (a.K + 16 * tk - 1) / (16 * tk);
   dim3 grid(ptiles * ktiles, a.nsplit, a.ntau);

@@ -28,6 +28,7 @@
 #include <cuda_fp16.h>
 
 #include "kernels.cuh"
+#include "launch_util.h"
 #include "p2_common.cuh"
 #include "tc.cuh"
 
@@ -300,7 +301,7 @@ __global__ void k_split_reduce(const SplitReduceArgs a) {
 template <int NT>
 cudaError_t launch_nt(const SplitGemmArgs& a, cudaStream_t s) {
   const int smem = stage_bytes(NT) * 2 + 64 + 1024;
-  cudaError_t e = cudaFuncSetAttribute(k_project_split<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = ensure_smem((const void*)k_project_split<NT>, smem);
   if (e != cudaSuccess) return e;
   dim3 grid(a.ntile * a.nmtile, a.nsplit, a.ntau);
   k_project_split<NT><<<grid, kThreads, smem, s>>>(a);

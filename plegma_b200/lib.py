@@ -7,6 +7,7 @@ missing, `load()` raises.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 import os
 from typing import Optional, Sequence
 
@@ -71,7 +72,8 @@ class P2KernelTime(C.Structure):
 EXPORTS = ["p2_ctx_create", "p2_ctx_destroy", "p2_last_error", "p2_sync", "p2_set_stream", "p2_components",
            "p2_mom_list", "p2_block_info", "p2_contract_project", "p2_contract_position", "p2_ft_apply",
            "p2_synth_propagator", "p2_profile_enable", "p2_profile_read", "p2_alloc", "p2_free", "p2_copy",
-           "p2_ft_apply_noalloc", "p2_set_workspace"]
+           "p2_ft_apply_noalloc", "p2_set_workspace", "p2_graph_create", "p2_graph_launch", "p2_graph_sync",
+           "p2_graph_destroy", "p2_tune_enable", "p2_tune_count"]
 
 _lib = None
 
@@ -90,6 +92,13 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.p2_sync.argtypes = [C.c_void_p]
     lib.p2_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     lib.p2_set_workspace.argtypes = [C.c_void_p, C.c_size_t]
+    lib.p2_graph_create.argtypes = [C.c_void_p, C.POINTER(P2Prop), C.c_int, C.POINTER(P2Request), C.c_int,
+                                    C.POINTER(C.c_void_p)]
+    lib.p2_graph_launch.argtypes = [C.c_void_p, C.c_void_p]
+    lib.p2_graph_sync.argtypes = [C.c_void_p]
+    lib.p2_graph_destroy.argtypes = [C.c_void_p]
+    lib.p2_tune_enable.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
+    lib.p2_tune_count.argtypes = [C.c_void_p]
     lib.p2_components.argtypes = [C.c_uint]
     lib.p2_mom_list.argtypes = [C.c_int, C.POINTER(C.c_int)]
     lib.p2_block_info.argtypes = [C.c_uint, C.c_int, C.c_int, C.POINTER(P2Block), C.c_int, C.POINTER(C.c_size_t)]
@@ -154,9 +163,14 @@ class Context:
         if st != P2_OK:
             raise P2Error(st, "p2_ctx_create failed")
         self.h = h
+        self._graphs = []  # weak references: graphs are destroyed before their context
 
     def close(self):
         if self.h:
+            for ref in self._graphs:
+                g = ref()
+                if g is not None:
+                    g.close()
             self.lib.p2_ctx_destroy(self.h)
             self.h = None
 
@@ -228,6 +242,17 @@ class Context:
         pa = (P2Prop * len(props))(*props)
         self.check(self.lib.p2_contract_position(self.h, pa, len(props), C.byref(req)))
 
+    def graph(self, props: Sequence[P2Prop], reqs: Sequence[P2Request]) -> "Graph":
+        """p2_graph_create: record the launch sequence of contract_project(props, reqs)."""
+        return Graph(self, props, reqs)
+
+    def tune(self, on: bool = True, cache_path: Optional[str] = None):
+        """p2_tune_enable: time candidate launch shapes for new (kernel, shape) keys."""
+        self.check(self.lib.p2_tune_enable(self.h, int(on), cache_path.encode() if cache_path else None))
+
+    def tune_count(self) -> int:
+        return self.lib.p2_tune_count(self.h)
+
     def profile(self, on: bool = True):
         self.check(self.lib.p2_profile_enable(self.h, int(on)))
 
@@ -250,6 +275,38 @@ class Context:
         self.check(self.lib.p2_ft_apply(self.h, C.c_void_p(field_ptr), dof, nt,
                                         m.ctypes.data_as(C.POINTER(C.c_int)), len(m), sign, C.c_void_p(out_ptr),
                                         out_location))
+
+
+class Graph:
+    """A recorded batch (p2_graph_*); keeps the request arrays alive."""
+
+    def __init__(self, ctx: "Context", props: Sequence[P2Prop], reqs: Sequence[P2Request]):
+        self.ctx = ctx
+        self._props = (P2Prop * len(props))(*props)
+        self._reqs = (P2Request * len(reqs))(*reqs)
+        self._keep = list(reqs)
+        h = C.c_void_p()
+        self.h = None
+        ctx.check(ctx.lib.p2_graph_create(ctx.h, self._props, len(props), self._reqs, len(reqs), C.byref(h)))
+        self.h = h
+        ctx._graphs.append(weakref.ref(self))
+
+    def launch(self, stream_ptr: Optional[int] = None):
+        self.ctx.check(self.ctx.lib.p2_graph_launch(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def sync(self):
+        self.ctx.check(self.ctx.lib.p2_graph_sync(self.h))
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.p2_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def result_blocks(contractions: int, totalT: int, nmom: int, flat: np.ndarray):

@@ -100,3 +100,33 @@ def test_host_only_context_generator_and_validation():
         ctx.contract_project([prop, prop], [good])
     assert e.value.status == p2.P2_ERR_UNSUPPORTED
     ctx.close()
+
+
+def test_tune_cache_file_round_trip(tmp_path):
+    """The tuning cache file is read on p2_tune_enable: well-formed lines
+    become entries, malformed ones are skipped (host-only context)."""
+    path = tmp_path / "tune.tsv"
+    path.write_text("project_split V3=32768 K=288 rows=128 n=8\t144,2,37,14\t1.25\n"
+                    "project_fp64 V3=64 K=32 nmom=19 n=4\t8,1,64\t0.01\n"
+                    "garbage line without tabs\n"
+                    "project_fp64 bad\tx,y\t1\n")
+    ctx = p2.Context((4, 4, 4, 4), device=-1)
+    assert ctx.tune_count() == 0
+    ctx.tune(False, str(path))
+    assert ctx.tune_count() == 2
+    ctx.close()
+
+
+def test_graph_and_workspace_entry_points_validate_on_host_only_context():
+    ctx = p2.Context((4, 4, 4, 4), device=-1)
+    with pytest.raises(p2.P2Error) as e:
+        ctx.set_workspace(0)
+    assert e.value.status == p2.P2_ERR_INVALID_ARG
+    ctx.set_workspace(1 << 20)
+    a = np.zeros(16, dtype=np.complex128)
+    prop = ctx.prop(a.ctypes.data, location=p2.P2_DEVICE, nt=4)
+    req = ctx.request((0, 0, 0, 0), 4, p2.NUCLEON_CG5, a.ctypes.data)
+    with pytest.raises(p2.P2Error) as e:
+        ctx.graph([prop, prop], [req])
+    assert e.value.status == p2.P2_ERR_UNSUPPORTED
+    ctx.close()
