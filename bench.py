@@ -142,6 +142,91 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+BATCHED = {
+    # name: (lattice, sources, window range, |n|^2 max, propagator precision, decay, seed)
+    "batched_32x64": ((32, 32, 32, 64), 16, (8, 20), 9, "fp64", 0.5, 2024),
+    "batched_64x128": ((64, 64, 64, 128), 4, (32, 32), 16, "fp32", 0.4, 2025),
+}
+
+
+def run_batched(name, stream, steps, warmup, forms=("split",)):
+    """Many sources with uneven windows in one recorded CUDA graph per step:
+    nucleon C g5 + Delta C g_k (both isospins) + 16x16 mesons (K = 480).
+    Propagators are stored for each source's window only (t_first = t0,
+    nt = window), so 16 sources x 2 flavours fit in HBM."""
+    import torch
+    from plegma_b200 import lib as p2
+    Lb, nsrc, (wmin, wmax), q2, prec, decay, seed = BATCHED[name]
+    what = p2.NUCLEON_CG5 | p2.DELTA_ISO12 | p2.DELTA_ISO32 | p2.MESON_G16
+    K = p2.components(what)
+    moms = p2.mom_list(q2)
+    ctx = p2.Context(Lb)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.tune(True)
+    V3 = Lb[0] * Lb[1] * Lb[2]
+    rng = np.random.default_rng(seed)
+    P = p2.P2_FP32 if prec == "fp32" else p2.P2_FP64
+    dt = torch.complex64 if prec == "fp32" else torch.complex128
+    srcs, bufs, props = [], [], []
+    for i in range(nsrc):
+        src = tuple(int(rng.integers(0, Lb[dd])) for dd in range(4))
+        W = int(rng.integers(wmin, wmax + 1))
+        for f in range(2):
+            b = torch.empty(144 * V3 * W, dtype=dt, device="cuda")
+            ctx.synth(b.data_ptr(), True, P, seed + i, f, src[3], decay, src[3], W)
+            bufs.append(b)
+            props.append(ctx.prop(b.data_ptr(), P, p2.P2_DEVICE, src[3], W))
+        srcs.append((src, W))
+    sites = sum(W for _, W in srcs) * V3
+    res = {"workload": f"{Lb[0]}^3x{Lb[3]}, {nsrc} sources, windows {wmin}-{wmax} (sum {sites // V3} slices), "
+                       f"nucleon Cg5 + Delta Cg_k (iso 1/2, 3/2) + 16x16 mesons, K={K}, |n|^2<={q2} "
+                       f"({len(moms)} momenta), {prec} propagators stored per window",
+           "sites_per_step": sites, "launch": "one CUDA graph per step (p2_graph_launch)", "forms": {}}
+    for form in forms:
+        mode = p2.P2_SPLIT_FP16 if form == "split" else p2.P2_PLAIN_FP64
+        outs, reqs = [], []
+        for i, (src, W) in enumerate(srcs):
+            _, total = p2.block_info(what, W, len(moms))
+            o = torch.zeros(total, dtype=torch.complex128, device="cuda")
+            outs.append(o)
+            reqs.append(ctx.request(src, W, what, o.data_ptr(), mode=mode, moms=moms, prop_u=2 * i,
+                                    prop_d=2 * i + 1))
+        # per-kernel device time from one eager call (graph replays are not split by kernel)
+        ctx.profile(True)
+        ctx.profile_read(reset=True)
+        ctx.contract_project(props, reqs)
+        ctx.sync()
+        prof = ctx.profile_read(reset=True)
+        ctx.profile(False)
+        g = ctx.graph(props, reqs)
+        for _ in range(warmup):
+            g.launch()
+        g.sync()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            ev0.record(stream)
+            for _ in range(steps):
+                g.launch()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        g.sync()
+        ms = ev0.elapsed_time(ev1) / steps
+        tot = sum(v[1] for v in prof.values()) or 1.0
+        res["forms"][form] = {"ms_per_step": ms, "sites_per_s": sites / (ms * 1e-3), "steps": steps,
+                              "kernels": {k: {"launches": v[0], "ms": v[1], "share": v[1] / tot}
+                                          for k, v in prof.items()},
+                              "gpu_launches_per_step": sum(v[0] for v in prof.values()),
+                              "clocks": clk.summary()}
+        g.close()
+        del outs
+    res["tuned_shapes"] = ctx.tune_count()
+    ctx.close()
+    del bufs
+    torch.cuda.empty_cache()
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -151,6 +236,7 @@ def main():
     ap.add_argument("--form", default="auto", choices=["auto", "split", "plain"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-source graph runs")
     ap.add_argument("--lattice", default=None,
                     help="Lx,Ly,Lz,Lt override for small profiling cases (not the benchmark workload)")
     args = ap.parse_args()
@@ -178,6 +264,7 @@ def main():
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
+    ctx.tune(True)  # launch shapes timed during the warm-up steps, cached in memory
 
     seed = SEED + rank
     src = source_for(seed)
@@ -310,6 +397,21 @@ def main():
         except Exception as ex:  # reported, not fatal
             cpu = {"value": None, "error": str(ex)}
 
+    ctx.close()
+    u = d = hu = hd = out = None  # release the headline's buffers before the batched runs
+    batched = None
+    if not args.no_batched and not args.lattice and world == 1:
+        import gc
+        gc.collect()
+        torch.cuda.empty_cache()
+        batched = {}
+        for name, forms_b in (("batched_32x64", ("split", "plain")), ("batched_64x128", ("split",))):
+            try:
+                batched[name] = run_batched(name, stream, max(1, min(args.steps, 3)), max(1, min(args.warmup, 2)),
+                                            forms_b)
+            except Exception as ex:  # reported, not fatal
+                batched[name] = {"error": str(ex)}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "sites/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -320,9 +422,8 @@ def main():
                 "forms": {k: {"ms_per_step": v["ms"], "sites_per_s": sites * world / (v["ms"] * 1e-3)}
                           for k, v in results.items()},
                 "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": r["clocks"]}
+                "gpu_launches": launches, "clocks": r["clocks"], "batched": batched}
         print(json.dumps(line), flush=True)
-    ctx.close()
     if dist:
         dist.destroy_process_group()
 
