@@ -142,6 +142,11 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# DRAM bytes (read + write) per site of the dominant kernel, measured with ncu
+# on the 32^3 x 16 case of the same kernel; traffic grows with the sites a
+# launch processes, so it scales to the benchmark's launches
+TRAFFIC_PER_SITE = {("contract_f32", "split"): 6916, ("contract_plain_fp64", "plain"): 9144}
+
 BATCHED = {
     # name: (lattice, sources, window range, |n|^2 max, propagator precision, decay, seed)
     "batched_32x64": ((32, 32, 32, 64), 16, (8, 20), 9, "fp64", 0.5, 2024),
@@ -343,11 +348,27 @@ def main():
     if ck:
         kname = ck[0]
         n, kms = prof[kname]
-        bytes_per_site = 2 * 144 * 16
+        bytes_per_site = 2 * 144 * 16  # algorithmic: both FP64 propagators once
+        per_launch = sites * args.steps / max(n, 1)
         ach = bytes_per_site * sites * args.steps / (kms * 1e-3) / 1e9
+        tps = TRAFFIC_PER_SITE.get((kname, head))
         roof = {"kernel": kname, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                "frac": ach / hbm, "peak_kind": peak_kind, "traffic": None,
-                "algorithmic_bytes_per_launch": bytes_per_site * sites * args.steps / max(n, 1)}
+                "frac": ach / hbm, "peak_kind": peak_kind,
+                "traffic": tps * per_launch if tps else None,
+                "traffic_note": "DRAM read+write bytes per site from the ncu capture of the 32^3x16 case, "
+                                "times the sites of one launch" if tps else None,
+                "algorithmic_bytes_per_launch": bytes_per_site * per_launch, "sites_per_launch": per_launch}
+    # the projection against the tensor (split) or FP64 (plain) roofline, algorithmic flop = 8 nmom K per site
+    roof_proj = None
+    pk = [k for k in prof if k.startswith("project")]
+    if pk:
+        n, kms = prof[pk[0]]
+        flop = 8.0 * nmom * K * sites * args.steps
+        ach = flop / (kms * 1e-3) / 1e12
+        roof_proj = {"kernel": pk[0], "bound": "tensor" if head == "split" else "fp64", "achieved": ach,
+                     "unit": "TFLOP/s", "algorithmic_flop_per_launch": flop / max(n, 1)}
+        if head == "split":
+            roof_proj.update({"peak": bf16, "frac": ach / bf16, "peak_kind": peak_kind + " dense bf16 (= fp16)"})
 
     # end to end through the C ABI with host buffers (pinned), copies inside the timed region
     e2e = None
@@ -421,7 +442,7 @@ def main():
                            "parallelism": f"source-sharded x{world}"},
                 "forms": {k: {"ms_per_step": v["ms"], "sites_per_s": sites * world / (v["ms"] * 1e-3)}
                           for k, v in results.items()},
-                "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roof, "roofline_projection": roof_proj, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": r["clocks"], "batched": batched}
         print(json.dumps(line), flush=True)
     if dist:
