@@ -36,7 +36,10 @@ constexpr int kSitesPerTile = 16;
 constexpr int kRow = 289;  // complex per site row (2 * 144 + 1 pad)
 constexpr int kStage = kSitesPerTile * kRow;
 
-template <typename Tin>
+// CM = false: site-major [site][kRow] (the plain kernel reads it directly);
+// CM = true: component-major [flavour * 144 + component][16 sites], written
+// without bank conflicts and transposed by the split kernel's conversion.
+template <typename Tin, bool CM = false>
 __device__ __forceinline__ void issue_tile(const ContractArgs& a, Cx<Tin>* st, long long tile, long long ntiles,
                                            int tiles_per_tau) {
   if (tile < ntiles) {
@@ -54,7 +57,7 @@ __device__ __forceinline__ void issue_tile(const ContractArgs& a, Cx<Tin>* st, l
 #pragma unroll 3
       for (int r = 0; r < 9; r++) {
         const int comp = (threadIdx.x >> 4) + 16 * r;
-        Cx<Tin>* dst = st + s * kRow + 144 * f + comp;
+        Cx<Tin>* dst = CM ? st + (144 * f + comp) * kSitesPerTile + s : st + s * kRow + 144 * f + comp;
         if (sizeof(Tin) == 8)
           cp_async16(dst, src + comp * vol, ok ? 16 : 0);
         else
@@ -72,17 +75,25 @@ __device__ __forceinline__ int diag10_slot(int g) {
   return g == 0 ? 0 : g == 5 ? 1 : (g >= 1 && g <= 4) ? g + 1 : (g >= 6 && g <= 9) ? g : -1;
 }
 
+// Split form: the per-component maxima of the current slice live in the spare
+// slot of each FP32 tile block (row s, block j holds components 2 (32 s + j)
+// and 2 (32 s + j) + 1), which no load of the contraction reads.
+__device__ __forceinline__ int* smax_slot(Cx<float>* sf, int k) {
+  const int p = k >> 1, s = p >> 5, j = p & 31;
+  return reinterpret_cast<int*>(sf + s * kRow32 + 2 * row32_unit(j, 4, s & 7) + 1) + (k & 1);
+}
+
 template <typename R>
 struct Writer {
   Cx<R>* out;
   long long V3;
-  int* smax;    // split form: per-component running max (float bits), or null
-  float* rmax;  // split form: this lane's running maxima of its nucleon (2) and G16 (16) outputs
+  float* rmax;          // split form: this lane's running maxima of its nucleon (2) and G16 (16) outputs
+  Cx<float>* smax_base;  // split form: tile whose spare slots hold the per-component maxima, or null
   __device__ __forceinline__ void put(int k, Cx<R> v) const {
     out[(long long)k * V3] = v;
-    if (smax) {
+    if (smax_base) {
       const float m = fmaxf(fabsf((float)v.x), fabsf((float)v.y));
-      atomicMax(smax + k, __float_as_int(m));
+      atomicMax(smax_slot(smax_base, k), __float_as_int(m));
     }
   }
   // Outputs whose component is fixed per lane: the maximum stays in a register
@@ -110,27 +121,28 @@ __device__ __forceinline__ void delta_out(const ContractArgs& a, const Writer<R>
 // block (false); a request with both runs the two instantiations over the same
 // tiles (the Delta part is ~5x the rest in arithmetic, so the second pass over
 // the propagators is hidden under its compute).
-template <typename R, bool DELTA>
-__device__ __forceinline__ void contract_site(const ContractArgs& a, const Cx<R>* U, const Cx<R>* D,
-                                              const LaneTables& lt, int l, unsigned mask, const Writer<R>& w) {
+template <bool DELTA, typename Row>
+__device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& row, const LaneTables& lt, int l,
+                                              unsigned mask, const Writer<typename Row::R>& w) {
+  typedef typename Row::R R;
   if (DELTA) {
 #pragma unroll 1
     for (int g = 0; g < 3; g++) {
       Cx<R> o[4];
-      delta_site<R>(U, D, g, l, mask, o);
+      delta_site(row, lt, g, l, mask, o);
       delta_out(a, w, l, g, o);
     }
     return;
   }
   if (a.what & 1u) {
     Cx<R> pn[2];
-    nucleon_site<R>(U, D, lt, l, mask, pn);
+    nucleon_site(row, lt, l, mask, pn);
     w.put_slot(a.k.nuc + l, pn[0], 0);
     w.put_slot(a.k.nuc + 16 + l, pn[1], 1);
   }
   if (a.what & (8u | 16u | 32u)) {
     Cx<R> c[16];
-    meson_site<R>(U, D, lt, l, mask, c);
+    meson_site(row, kU, kD, lt, l, mask, c);
     if (a.what & 8u) {
 #pragma unroll
       for (int g2 = 0; g2 < 16; g2++) w.put_slot(a.k.g16 + l * 16 + g2, c[g2], 2 + g2);
@@ -157,11 +169,11 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Cx<R>
   if (a.what & 64u) {
     const int j = diag10_slot(l);
     Cx<R> c[16];
-    meson_site<R>(U, U, lt, l, mask, c);
+    meson_site(row, kU, kU, lt, l, mask, c);
 #pragma unroll
     for (int g2 = 0; g2 < 16; g2++)
       if (g2 == l && j >= 0) w.put(a.k.diag10 + j, c[g2]);
-    meson_site<R>(D, D, lt, l, mask, c);
+    meson_site(row, kD, kD, lt, l, mask, c);
 #pragma unroll
     for (int g2 = 0; g2 < 16; g2++)
       if (g2 == l && j >= 0) w.put(a.k.diag10 + 10 + j, c[g2]);
@@ -192,9 +204,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
     const int tl = (int)(tile / tiles_per_tau);
     const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + hw;
     if (x < a.V3) {
-      const Cx<double>* U = st + hw * kRow;
-      Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr, nullptr};
-      contract_site<double, DELTA>(a, U, U + 144, lt, l, mask, w);
+      const RowF64 row{st + hw * kRow};
+      const Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr, nullptr};
+      contract_site<DELTA>(a, row, lt, l, mask, w);
     }
     __syncthreads();
     issue_tile<double>(a, st, tile + 2LL * gridDim.x, ntiles, tiles_per_tau);
@@ -203,15 +215,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
 }
 
 // Split form: FP32 arithmetic on power-of-two scaled inputs.  One staging
-// buffer in the input precision plus an FP32 copy of the tile: the staging
-// buffer is refilled with the next tile's cp.async as soon as the current one
-// is converted, so two CTAs (16 warps) fit on an SM.
+// buffer in the input precision (component-major) plus an FP32 copy of the
+// tile in the padded, swizzled row layout of RowF32: the staging buffer is
+// refilled with the next tile's cp.async as soon as the current one is
+// converted, so two CTAs (16 warps) fit on an SM.
+constexpr int kStage32 = kSitesPerTile * kRow32;
+
 template <typename Tin, bool DELTA>
 __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<Tin>* st = (Cx<Tin>*)smem_raw;
-  Cx<float>* sf = (Cx<float>*)(smem_raw + kStage * sizeof(Cx<Tin>));
-  int* smax = (int*)(sf + kStage);
+  Cx<float>* sf = (Cx<float>*)(smem_raw + kSitesPerTile * 288 * sizeof(Cx<Tin>));
   const int tid = threadIdx.x;
   const int hw = tid >> 4, l = tid & 15;
   const unsigned mask = halfwarp_mask();
@@ -220,11 +234,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
   const int tiles_per_tau = (a.V3 + kSitesPerTile - 1) / kSitesPerTile;
   const long long ntiles = (long long)a.ntau * tiles_per_tau;
   long long tile = blockIdx.x;
-  for (int k = tid; k < a.K; k += kThreads) smax[k] = 0;
+  for (int k = tid; k < a.K; k += kThreads) *smax_slot(sf, k) = 0;
 
-  issue_tile<Tin>(a, st, tile, ntiles, tiles_per_tau);
+  issue_tile<Tin, true>(a, st, tile, ntiles, tiles_per_tau);
 
-  int cur = -1;  // slice whose maxima smax holds
+  int cur = -1;  // slice whose maxima the spare slots hold
   float rmax[18];
 #pragma unroll
   for (int i = 0; i < 18; i++) rmax[i] = 0.f;
@@ -238,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
         int k = -1;
         if (i < 2 && (a.what & 1u)) k = a.k.nuc + 16 * i + l;
         if (i >= 2 && (a.what & 8u)) k = a.k.g16 + l * 16 + (i - 2);
-        if (k >= 0) atomicMax(smax + k, __float_as_int(m));
+        if (k >= 0) atomicMax(smax_slot(sf, k), __float_as_int(m));
       }
     }
   };
@@ -250,41 +264,46 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
     if (tl != cur) {
       if (cur >= 0)
         for (int k = tid; k < a.K; k += kThreads) {
-          atomicMax(a.cmax + (long long)cur * a.K + k, smax[k]);
-          smax[k] = 0;
+          int* slot = smax_slot(sf, k);
+          atomicMax(a.cmax + (long long)cur * a.K + k, *slot);
+          *slot = 0;
         }
       cur = tl;
     }
-    // scale by 2^-E per flavour and convert to FP32 once per tile
+    // scale by 2^-E per flavour and convert to FP32 once per tile: thread
+    // (site s, components c0 + 16 j) reads the component-major staging and
+    // writes the site's padded row (exact power-of-two scales; products are
+    // formed in double so that no intermediate leaves the representable range)
     {
-      // exact power-of-two scales; products are formed in double so that no
-      // intermediate leaves the representable range
       const double su = ldexp(1.0, -a.exps[2 * tl]), sd = ldexp(1.0, -a.exps[2 * tl + 1]);
-      for (int i = tid; i < kSitesPerTile * 288; i += kThreads) {
-        const int s = i / 288, c = i - s * 288;
-        const Cx<Tin> v = st[s * kRow + c];
-        const double sc = c < 144 ? su : sd;
-        Cx<float> f;
-        f.x = (float)((double)v.x * sc);
-        f.y = (float)((double)v.y * sc);
-        sf[s * kRow + c] = f;
+      const int s = tid & (kSitesPerTile - 1), c0 = tid >> 4, sw = s & 7;
+      Cx<float>* row = sf + s * kRow32;
+#pragma unroll
+      for (int j = 0; j < 18; j++) {
+        const int f = j >= 9;
+        const int cc = c0 + 16 * (j - 9 * f);  // component within the flavour
+        const int blk = cc / 9, col = cc - 9 * blk;
+        const Cx<Tin> v = st[(144 * f + cc) * kSitesPerTile + s];
+        const double sc = f ? sd : su;
+        row[2 * row32_unit(16 * f + blk, col >> 1, sw) + (col & 1)] =
+            cx<float>((float)((double)v.x * sc), (float)((double)v.y * sc));
       }
     }
     __syncthreads();
     // the staged tile has been converted: refill the staging buffer while contracting
-    issue_tile<Tin>(a, st, tile + gridDim.x, ntiles, tiles_per_tau);
+    issue_tile<Tin, true>(a, st, tile + gridDim.x, ntiles, tiles_per_tau);
     const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + hw;
     if (x < a.V3) {
-      const Cx<float>* U = sf + hw * kRow;
-      Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, smax, rmax};
-      contract_site<float, DELTA>(a, U, U + 144, lt, l, mask, w);
+      const RowF32 row{sf + hw * kRow32, hw & 7};
+      const Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, rmax, sf};
+      contract_site<DELTA>(a, row, lt, l, mask, w);
     }
   }
   cp_async_wait<0>();
   if (cur >= 0) flush_lane();
   __syncthreads();
   if (cur >= 0)
-    for (int k = tid; k < a.K; k += kThreads) atomicMax(a.cmax + (long long)cur * a.K + k, smax[k]);
+    for (int k = tid; k < a.K; k += kThreads) atomicMax(a.cmax + (long long)cur * a.K + k, *smax_slot(sf, k));
 }
 
 // Per-slice exponent E with max(|Re|,|Im|) < 2^E over a strided sample of
@@ -347,7 +366,8 @@ cudaError_t launch_plain_t(const ContractArgs& a, int grid, cudaStream_t s) {
 
 template <typename Tin, bool DELTA>
 cudaError_t launch_f32_t(const ContractArgs& a, int grid, cudaStream_t s) {
-  const int smem = kStage * (int)sizeof(Cx<Tin>) + kStage * (int)sizeof(Cx<float>) + a.K * (int)sizeof(int);
+  const int smem = kSitesPerTile * 288 * (int)sizeof(Cx<Tin>) + kStage32 * (int)sizeof(Cx<float>);
+  if (a.K > 2 * 32 * kSitesPerTile) return cudaErrorInvalidValue;  // more components than spare slots
   cudaError_t e = ensure_smem((const void*)k_contract_f32<Tin, DELTA>, smem);
   if (e != cudaSuccess) return e;
   k_contract_f32<Tin, DELTA><<<grid, kThreads, smem, s>>>(a);

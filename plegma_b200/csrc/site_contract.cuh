@@ -40,12 +40,15 @@ struct DiquarkLane {
   int z1, sA1, sB1, z2, sA2, sB2, sN, sL;
 };
 
-// Per-lane copies of the table entries a lane needs with a lane-dependent index.
+// Per-lane table entries packed into registers (the tables are indexed by
+// lane, so reading them from constant memory inside the site loop would
+// serialise the half-warp): a diquark lane descriptor as 8 fields of 4 bits
+// (value + 1), and the sink-Gamma stage of the mesons as 4 bytes (source
+// lane, Re + 1, Im + 1 of G_g1[d][pi1(d)] for d = 0..3).
 struct LaneTables {
-  DiquarkLane nuc;  // nucleon C g5 descriptor
-  // meson stage: lane = g1, row d of G_g1: column pi1(d) and value
-  int gsrc[4];  // source lane pi1(d)*4 + d
-  int gre[4], gim[4];
+  unsigned nuc;       // nucleon C g5 descriptor
+  unsigned delta[3];  // Delta C g_k descriptors, k = 1..3
+  unsigned gam;       // meson stage
 };
 
 __constant__ int c_gamma_perm[16][4] = P2_INIT_GammaPerm;
@@ -56,48 +59,103 @@ __constant__ int c_nuc_lane[16][8] = P2_INIT_NucLane;
 __constant__ int c_delta_sink[3][4][3] = P2_INIT_DeltaSink;
 __constant__ int c_delta_lane[3][16][8] = P2_INIT_DeltaLane;
 
-__device__ __forceinline__ DiquarkLane load_diquark_lane(const int (*t)[8], int l) {
+// ---- shared-memory views of one site's two propagators --------------------
+// Spin block b = mu * 4 + nu of flavour f is block 16 f + b; colour (a, b) is
+// entry a * 3 + b of the block.
+//
+// Plain FP64 tile: row of 2 x 144 complex, block at 9 * block.
+struct RowF64 {
+  typedef double R;
+  const Cx<double>* p;
+  __device__ __forceinline__ void pair(int blk, int k, Cx<double>& v0, Cx<double>& v1) const {
+    v0 = p[blk * 9 + 2 * k];
+    v1 = p[blk * 9 + 2 * k + 1];
+  }
+  __device__ __forceinline__ Cx<double> last(int blk) const { return p[blk * 9 + 8]; }
+  __device__ __forceinline__ void load9(int blk, Cx<double> v[9]) const {
+#pragma unroll
+    for (int i = 0; i < 9; i++) v[i] = p[blk * 9 + i];
+  }
+};
+
+// Split-form FP32 tile: every block padded to 10 complex = five 16-byte units
+// (colours 2k, 2k+1 in unit k, colour 8 and a spare slot in unit 4), so a
+// block is four 16-byte loads and one 8-byte load.  Units are XOR-swizzled
+// by sw = site & 7 so that the transposing writes of 16 sites spread over
+// the banks.
+constexpr int kRow32 = 320;  // complex per site row (32 blocks x 10)
+__device__ __forceinline__ int row32_unit(int blk, int k, int sw) { return (blk * 5 + k) ^ sw; }
+
+struct RowF32 {
+  typedef float R;
+  const Cx<float>* p;
+  int sw;
+  __device__ __forceinline__ void pair(int blk, int k, Cx<float>& v0, Cx<float>& v1) const {
+    const float4 q = *reinterpret_cast<const float4*>(p + 2 * row32_unit(blk, k, sw));
+    v0 = cx<float>(q.x, q.y);
+    v1 = cx<float>(q.z, q.w);
+  }
+  __device__ __forceinline__ Cx<float> last(int blk) const { return p[2 * row32_unit(blk, 4, sw)]; }
+  __device__ __forceinline__ void load9(int blk, Cx<float> v[9]) const {
+#pragma unroll
+    for (int k = 0; k < 4; k++) pair(blk, k, v[2 * k], v[2 * k + 1]);
+    v[8] = last(blk);
+  }
+};
+
+constexpr int kU = 0, kD = 16;  // block offsets of the u and d propagators in a row
+
+__device__ __forceinline__ unsigned pack_diquark_lane(const int (*t)[8], int l) {
+  unsigned v = 0;
+#pragma unroll
+  for (int f = 0; f < 8; f++) v |= (unsigned)(t[l][f] + 1) << (4 * f);
+  return v;
+}
+
+__device__ __forceinline__ DiquarkLane unpack_diquark_lane(unsigned v) {
   DiquarkLane d;
-  d.z1 = t[l][0];
-  d.sA1 = t[l][1];
-  d.sB1 = t[l][2];
-  d.z2 = t[l][3];
-  d.sA2 = t[l][4];
-  d.sB2 = t[l][5];
-  d.sN = t[l][6];
-  d.sL = t[l][7];
+  d.z1 = (int)((v >> 0) & 15u) - 1;
+  d.sA1 = (int)((v >> 4) & 15u) - 1;
+  d.sB1 = (int)((v >> 8) & 15u) - 1;
+  d.z2 = (int)((v >> 12) & 15u) - 1;
+  d.sA2 = (int)((v >> 16) & 15u) - 1;
+  d.sB2 = (int)((v >> 20) & 15u) - 1;
+  d.sN = (int)((v >> 24) & 15u) - 1;
+  d.sL = (int)((v >> 28) & 15u) - 1;
   return d;
 }
 
 __device__ __forceinline__ LaneTables load_lane_tables(int l) {
   LaneTables t;
-  t.nuc = load_diquark_lane(c_nuc_lane, l);
+  t.nuc = pack_diquark_lane(c_nuc_lane, l);
+#pragma unroll
+  for (int g = 0; g < 3; g++) t.delta[g] = pack_diquark_lane(c_delta_lane[g], l);
+  t.gam = 0;
 #pragma unroll
   for (int d = 0; d < 4; d++) {
-    t.gsrc[d] = c_gamma_perm[l][d] * 4 + d;
-    t.gre[d] = c_gamma_re[l][d];
-    t.gim[d] = c_gamma_im[l][d];
+    const unsigned src = (unsigned)(c_gamma_perm[l][d] * 4 + d);
+    const unsigned re = (unsigned)(c_gamma_re[l][d] + 1), im = (unsigned)(c_gamma_im[l][d] + 1);
+    t.gam |= (src | (re << 4) | (im << 6)) << (8 * d);
   }
   return t;
 }
 
-// G^{XY} for lane (x', y') and a sink table sink[iA] = (nu, lam, sA).
-template <typename R>
-__device__ __forceinline__ void diquark_G(const Cx<R>* __restrict__ X, const Cx<R>* __restrict__ Y,
-                                          const int (*sink)[3], int xp, int yp, Cx<R> q[9]) {
+// G^{XY} for lane (x', y') and a sink table sink[iA] = (nu, lam, sA); X and Y
+// are block offsets (kU, kD) of the two diquark lines in the site row.
+template <typename Row>
+__device__ __forceinline__ void diquark_G(const Row& row, int X, int Y, const int (*sink)[3], int xp, int yp,
+                                          Cx<typename Row::R> q[9]) {
+  typedef typename Row::R R;
 #pragma unroll
   for (int i = 0; i < 9; i++) q[i] = czero<R>();
 #pragma unroll 1
   for (int iA = 0; iA < 4; iA++) {
-    const Cx<R>* Xb = X + sblk(sink[iA][0], xp);
-    const Cx<R>* Yb = Y + sblk(sink[iA][1], yp);
     const R sgn = R(sink[iA][2]);
     Cx<R> a[9], b[9];
+    row.load9(X + sink[iA][0] * 4 + xp, a);
+    row.load9(Y + sink[iA][1] * 4 + yp, b);
 #pragma unroll
-    for (int i = 0; i < 9; i++) {
-      a[i] = cscale(Xb[i], sgn);
-      b[i] = Yb[i];
-    }
+    for (int i = 0; i < 9; i++) a[i] = cscale(a[i], sgn);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
@@ -122,12 +180,14 @@ __device__ __forceinline__ void diquark_transpose(Cx<R> q[9], int l, unsigned ma
   for (int i = 0; i < 9; i++) q[i] = cscale(shfl_idx16(q[i], src, mask), sign);
 }
 
-// One group of Wick terms sharing G and the third line Z; returns the lane's
-// share of T[mu = l >> 2][mu' = l & 3].  S1, S2, TA select the term types present.
-template <typename R, bool S1, bool S2, bool TA>
-__device__ __forceinline__ Cx<R> diquark_eval(const Cx<R> g[9], const Cx<R>* __restrict__ Z, const DiquarkLane& dl,
-                                              int l, unsigned mask, int c1A, int c1B, int c2A, int c2B, int cN,
-                                              int cL) {
+// One group of Wick terms sharing G and the third line Z (block offset in the
+// site row); returns the lane's share of T[mu = l >> 2][mu' = l & 3].  S1, S2,
+// TA select the term types present.
+template <bool S1, bool S2, bool TA, typename Row>
+__device__ __forceinline__ Cx<typename Row::R> diquark_eval(const Cx<typename Row::R> g[9], const Row& row, int Z,
+                                                            const DiquarkLane& dl, int l, unsigned mask, int c1A,
+                                                            int c1B, int c2A, int c2B, int cN, int cL) {
+  typedef typename Row::R R;
   const int mu = l >> 2, mup = l & 3;
   Cx<R> r = czero<R>();
   if (S2) {
@@ -135,10 +195,11 @@ __device__ __forceinline__ Cx<R> diquark_eval(const Cx<R> g[9], const Cx<R>* __r
     const R f2 = R(c2A * dl.sA2 - c2B * dl.sB2);
 #pragma unroll 1
     for (int m = 0; m < 4; m++) {
-      const Cx<R>* Z2 = Z + sblk(m, dl.z2);
+      Cx<R> z[9];
+      row.load9(Z + m * 4 + dl.z2, z);
       Cx<R> p2 = czero<R>();
 #pragma unroll
-      for (int i = 0; i < 9; i++) cmac(p2, g[i], Z2[i]);
+      for (int i = 0; i < 9; i++) cmac(p2, g[i], z[i]);
       p2 = cscale(p2, f2);
       p2 = p2 + shfl_xor16(p2, 4, mask);
       p2 = p2 + shfl_xor16(p2, 8, mask);
@@ -151,10 +212,11 @@ __device__ __forceinline__ Cx<R> diquark_eval(const Cx<R> g[9], const Cx<R>* __r
     const int src = mup << 2;
 #pragma unroll 1
     for (int m = 0; m < 4; m++) {
-      const Cx<R>* Z1 = Z + sblk(m, dl.z1);
+      Cx<R> z[9];
+      row.load9(Z + m * 4 + dl.z1, z);
       Cx<R> p1 = czero<R>();
 #pragma unroll
-      for (int i = 0; i < 9; i++) cmac(p1, g[i], Z1[i]);
+      for (int i = 0; i < 9; i++) cmac(p1, g[i], z[i]);
       p1 = cscale(p1, f1);
       p1 = p1 + shfl_xor16(p1, 1, mask);
       p1 = p1 + shfl_xor16(p1, 2, mask);
@@ -164,7 +226,8 @@ __device__ __forceinline__ Cx<R> diquark_eval(const Cx<R> g[9], const Cx<R>* __r
   }
   if (TA) {
     const R fa = R(cN * dl.sN - cL * dl.sL);
-    const Cx<R>* Zm = Z + sblk(mu, mup);
+    Cx<R> z[9];
+    row.load9(Z + mu * 4 + mup, z);
 #pragma unroll
     for (int i = 0; i < 9; i++) {
       Cx<R> d = cscale(g[i], fa);
@@ -172,7 +235,7 @@ __device__ __forceinline__ Cx<R> diquark_eval(const Cx<R> g[9], const Cx<R>* __r
       d = d + shfl_xor16(d, 2, mask);
       d = d + shfl_xor16(d, 4, mask);
       d = d + shfl_xor16(d, 8, mask);
-      cmac(r, d, Zm[i]);
+      cmac(r, d, z[i]);
     }
   }
   return r;
@@ -180,33 +243,52 @@ __device__ __forceinline__ Cx<R> diquark_eval(const Cx<R> g[9], const Cx<R>* __r
 
 // Nucleon C g5, both datasets: out[0] = proton (u u d), out[1] = neutron (d d u),
 // for lane (mu = l >> 2, mu' = l & 3).
-template <typename R>
-__device__ __forceinline__ void nucleon_site(const Cx<R>* __restrict__ U, const Cx<R>* __restrict__ D,
-                                             const LaneTables& lt, int l, unsigned mask, Cx<R> out[2]) {
+template <typename Row>
+__device__ __forceinline__ void nucleon_site(const Row& row, const LaneTables& lt, int l, unsigned mask,
+                                             Cx<typename Row::R> out[2]) {
+  typedef typename Row::R R;
   Cx<R> g[9];
-  diquark_G<R>(U, D, c_nuc_sink, l >> 2, l & 3, g);  // G^{ud}
-  out[0] = diquark_eval<R, true, false, true>(g, U, lt.nuc, l, mask, -1, 0, 0, 0, 1, 0);
+  diquark_G(row, kU, kD, c_nuc_sink, l >> 2, l & 3, g);  // G^{ud}
+  const DiquarkLane dl = unpack_diquark_lane(lt.nuc);
+  out[0] = diquark_eval<true, false, true>(g, row, kU, dl, l, mask, -1, 0, 0, 0, 1, 0);
   diquark_transpose<R>(g, l, mask, R(-1));  // G^{du}
-  out[1] = diquark_eval<R, true, false, true>(g, D, lt.nuc, l, mask, -1, 0, 0, 0, 1, 0);
+  out[1] = diquark_eval<true, false, true>(g, row, kD, dl, l, mask, -1, 0, 0, 0, 1, 0);
 }
 
-// Generic meson block: lane g1 gets C[g1][g2] for g2 = 0..15 in out[].
-template <typename R>
-__device__ __forceinline__ void meson_site(const Cx<R>* __restrict__ A, const Cx<R>* __restrict__ B,
-                                           const LaneTables& lt, int l, unsigned mask, Cx<R> out[16]) {
+// Generic meson block of the lines A and B (block offsets): lane g1 gets
+// C[g1][g2] for g2 = 0..15 in out[].
+template <typename Row>
+__device__ __forceinline__ void meson_site(const Row& row, int A, int B, const LaneTables& lt, int l, unsigned mask,
+                                           Cx<typename Row::R> out[16]) {
+  typedef typename Row::R R;
   const int al = l >> 2, de = l & 3;
   Cx<R> M[4][4];
 #pragma unroll
   for (int i = 0; i < 4; i++)
 #pragma unroll
     for (int j = 0; j < 4; j++) M[i][j] = czero<R>();
+  // colours in pairs (one 16-byte load per pair in the FP32 tile), then colour 8
 #pragma unroll
-  for (int ab = 0; ab < 9; ab++) {
+  for (int k = 0; k < 4; k++) {
+    Cx<R> u0[4], u1[4], d0[4], d1[4];
+#pragma unroll
+    for (int b = 0; b < 4; b++) row.pair(A + al * 4 + b, k, u0[b], u1[b]);
+#pragma unroll
+    for (int z = 0; z < 4; z++) row.pair(B + de * 4 + z, k, d0[z], d1[z]);
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+#pragma unroll
+      for (int z = 0; z < 4; z++) {
+        cmac_conj(M[b][z], u0[b], d0[z]);
+        cmac_conj(M[b][z], u1[b], d1[z]);
+      }
+  }
+  {
     Cx<R> u[4], d[4];
 #pragma unroll
-    for (int b = 0; b < 4; b++) u[b] = A[sblk(al, b) + ab];
+    for (int b = 0; b < 4; b++) u[b] = row.last(A + al * 4 + b);
 #pragma unroll
-    for (int z = 0; z < 4; z++) d[z] = B[sblk(de, z) + ab];
+    for (int z = 0; z < 4; z++) d[z] = row.last(B + de * 4 + z);
 #pragma unroll
     for (int b = 0; b < 4; b++)
 #pragma unroll
@@ -227,7 +309,10 @@ __device__ __forceinline__ void meson_site(const Cx<R>* __restrict__ A, const Cx
   for (int g2 = 0; g2 < 16; g2++) {
     Cx<R> c = czero<R>();
 #pragma unroll
-    for (int d = 0; d < 4; d++) c = c + cunit(shfl_idx16(N[g2], lt.gsrc[d], mask), lt.gre[d], lt.gim[d]);
+    for (int d = 0; d < 4; d++) {
+      const unsigned e = lt.gam >> (8 * d);
+      c = c + cunit(shfl_idx16(N[g2], (int)(e & 15u), mask), (int)((e >> 4) & 3u) - 1, (int)((e >> 6) & 3u) - 1);
+    }
     out[g2] = c;
   }
 }
@@ -240,31 +325,32 @@ __device__ __forceinline__ void meson_site(const Cx<R>* __restrict__ A, const Cx
 //   isospin 3/2, G^{AA}, Z = A: (-1, 1, 1, -1, 1, -1)
 // out = {iso-1/2 Delta+ (u,u,d), iso-1/2 Delta0 (d,d,u), iso-3/2 Delta++ (u,u,u),
 // iso-3/2 Delta- (d,d,d)} for table g (k = g + 1) and lane (mu, mu').
-template <typename R>
-__device__ __forceinline__ void delta_site(const Cx<R>* __restrict__ U, const Cx<R>* __restrict__ D, int g, int l,
-                                           unsigned mask, Cx<R> out[4]) {
-  const DiquarkLane dl = load_diquark_lane(c_delta_lane[g], l);
+template <typename Row>
+__device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt, int g, int l, unsigned mask,
+                                           Cx<typename Row::R> out[4]) {
+  typedef typename Row::R R;
+  const DiquarkLane dl = unpack_diquark_lane(g == 0 ? lt.delta[0] : g == 1 ? lt.delta[1] : lt.delta[2]);
   const R third = R(1) / R(3);
 #pragma unroll
   for (int i = 0; i < 4; i++) out[i] = czero<R>();
   // G^{uu}, G^{dd}: isospin 1/2 with the other flavour on the third line, isospin 3/2 with the same
 #pragma unroll 1
   for (int pair = 0; pair < 2; pair++) {
-    const Cx<R>* X = pair == 0 ? U : D;
-    const Cx<R>* O = pair == 0 ? D : U;
+    const int X = pair == 0 ? kU : kD;
+    const int O = pair == 0 ? kD : kU;
     Cx<R> q[9];
-    diquark_G<R>(X, X, c_delta_sink[g], l >> 2, l & 3, q);
-    const Cx<R> a = diquark_eval<R, true, true, true>(q, O, dl, l, mask, 0, 2, 0, -2, 1, -1);
-    const Cx<R> b = diquark_eval<R, true, true, true>(q, X, dl, l, mask, -1, 1, 1, -1, 1, -1);
+    diquark_G(row, X, X, c_delta_sink[g], l >> 2, l & 3, q);
+    const Cx<R> a = diquark_eval<true, true, true>(q, row, O, dl, l, mask, 0, 2, 0, -2, 1, -1);
+    const Cx<R> b = diquark_eval<true, true, true>(q, row, X, dl, l, mask, -1, 1, 1, -1, 1, -1);
     out[pair] = out[pair] + cscale(a, third);
     out[2 + pair] = out[2 + pair] + b;
   }
   // G^{ud} (A = u) and its lane transpose G^{du} (A = d; C g_k is symmetric)
   Cx<R> q[9];
-  diquark_G<R>(U, D, c_delta_sink[g], l >> 2, l & 3, q);
-  out[0] = out[0] + cscale(diquark_eval<R, true, true, true>(q, U, dl, l, mask, -4, 0, 2, -2, 4, 0), third);
+  diquark_G(row, kU, kD, c_delta_sink[g], l >> 2, l & 3, q);
+  out[0] = out[0] + cscale(diquark_eval<true, true, true>(q, row, kU, dl, l, mask, -4, 0, 2, -2, 4, 0), third);
   diquark_transpose<R>(q, l, mask, R(1));
-  out[1] = out[1] + cscale(diquark_eval<R, true, true, true>(q, D, dl, l, mask, -4, 0, 2, -2, 4, 0), third);
+  out[1] = out[1] + cscale(diquark_eval<true, true, true>(q, row, kD, dl, l, mask, -4, 0, 2, -2, 4, 0), third);
 }
 
 }  // namespace p2
