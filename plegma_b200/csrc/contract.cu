@@ -104,19 +104,6 @@ struct Writer {
   }
 };
 
-// Delta outputs of table g: group g of each isospin block, datasets (u-rich, d-rich).
-template <typename R>
-__device__ __forceinline__ void delta_out(const ContractArgs& a, const Writer<R>& w, int l, int g, const Cx<R> o[4]) {
-  if (a.what & 2u) {
-    w.put(a.k.diso12 + (g * 2 + 0) * 16 + l, o[0]);
-    w.put(a.k.diso12 + (g * 2 + 1) * 16 + l, o[1]);
-  }
-  if (a.what & 4u) {
-    w.put(a.k.diso32 + (g * 2 + 0) * 16 + l, o[2]);
-    w.put(a.k.diso32 + (g * 2 + 1) * 16 + l, o[3]);
-  }
-}
-
 // DELTA selects the instantiation: the Delta blocks only (true) or every other
 // block (false); a request with both runs the two instantiations over the same
 // tiles (the Delta part is ~5x the rest in arithmetic, so the second pass over
@@ -126,12 +113,18 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
                                               unsigned mask, const Writer<typename Row::R>& w) {
   typedef typename Row::R R;
   if (DELTA) {
-#pragma unroll 1
-    for (int g = 0; g < 3; g++) {
-      Cx<R> o[4];
-      delta_site(row, lt, g, l, mask, o);
-      delta_out(a, w, l, g, o);
-    }
+    // group g of each isospin block, datasets (u-rich, d-rich)
+    // the iso-1/2 partial sums are parked in the iso-1/2 output slots when
+    // those are requested, else in the iso-3/2 slots that are written later
+    const int park = (a.what & 2u) ? a.k.diso12 : a.k.diso32;
+    delta_site(
+        row, lt, l, mask,
+        [&](int g, int j, Cx<R> v) {
+          if (j < 2 && (a.what & 2u)) w.put(a.k.diso12 + (g * 2 + j) * 16 + l, v);
+          if (j >= 2 && (a.what & 4u)) w.put(a.k.diso32 + (g * 2 + j - 2) * 16 + l, v);
+        },
+        [&](int g, int j, Cx<R> v) { w.out[(long long)(park + (g * 2 + j) * 16 + l) * w.V3] = v; },
+        [&](int g, int j) { return w.out[(long long)(park + (g * 2 + j) * 16 + l) * w.V3]; });
     return;
   }
   if (a.what & 1u) {
@@ -239,13 +232,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
   issue_tile<Tin, true>(a, st, tile, ntiles, tiles_per_tau);
 
   int cur = -1;  // slice whose maxima the spare slots hold
-  float rmax[18];
+  // the Delta instantiation tracks its maxima in shared memory only
+  constexpr int kSlots = DELTA ? 1 : 18;
+  float rmax[kSlots];
 #pragma unroll
-  for (int i = 0; i < 18; i++) rmax[i] = 0.f;
+  for (int i = 0; i < kSlots; i++) rmax[i] = 0.f;
   // lane maxima -> shared (the two half-warps of a warp own the same components)
   auto flush_lane = [&]() {
+    if (DELTA) return;
 #pragma unroll
-    for (int i = 0; i < 18; i++) {
+    for (int i = 0; i < kSlots; i++) {
       const float m = fmaxf(rmax[i], __shfl_xor_sync(0xffffffffu, rmax[i], 16));
       rmax[i] = 0.f;
       if (!(tid & 16)) {
@@ -295,7 +291,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
     const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + hw;
     if (x < a.V3) {
       const RowF32 row{sf + hw * kRow32, hw & 7};
-      const Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, rmax, sf};
+      const Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, DELTA ? nullptr : rmax, sf};
       contract_site<DELTA>(a, row, lt, l, mask, w);
     }
   }

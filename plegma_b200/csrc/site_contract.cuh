@@ -140,8 +140,35 @@ __device__ __forceinline__ LaneTables load_lane_tables(int l) {
   return t;
 }
 
-// G^{XY} for lane (x', y') and a sink table sink[iA] = (nu, lam, sA); X and Y
-// are block offsets (kU, kD) of the two diquark lines in the site row.
+// q += sgn * P^{XY}_{(nu, lam)} for lane (x', y'):
+//   P[c][e] = sum eps_abc eps_{c1 c2 e} X[nu][x'][a][c1] Y[lam][y'][b][c2]
+// (36 complex products); X and Y are block offsets (kU, kD) of the two
+// diquark lines in the site row.
+template <typename Row>
+__device__ __forceinline__ void diquark_acc(const Row& row, int X, int Y, int nu, int lam, typename Row::R sgn,
+                                            int xp, int yp, Cx<typename Row::R> q[9]) {
+  typedef typename Row::R R;
+  Cx<R> a[9], b[9];
+  row.load9(X + nu * 4 + xp, a);
+  row.load9(Y + lam * 4 + yp, b);
+#pragma unroll
+  for (int i = 0; i < 9; i++) a[i] = cscale(a[i], sgn);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      const int e1 = (e + 1) % 3, e2 = (e + 2) % 3;
+      Cx<R>& r = q[c * 3 + e];
+      cmac(r, a[c1 * 3 + e1], b[c2 * 3 + e2]);
+      cmsub(r, a[c1 * 3 + e2], b[c2 * 3 + e1]);
+      cmsub(r, a[c2 * 3 + e1], b[c1 * 3 + e2]);
+      cmac(r, a[c2 * 3 + e2], b[c1 * 3 + e1]);
+    }
+  }
+}
+
+// G^{XY} = sum over a sink table sink[iA] = (nu, lam, sA) of sA P^{XY}_{(nu, lam)}.
 template <typename Row>
 __device__ __forceinline__ void diquark_G(const Row& row, int X, int Y, const int (*sink)[3], int xp, int yp,
                                           Cx<typename Row::R> q[9]) {
@@ -149,27 +176,7 @@ __device__ __forceinline__ void diquark_G(const Row& row, int X, int Y, const in
 #pragma unroll
   for (int i = 0; i < 9; i++) q[i] = czero<R>();
 #pragma unroll 1
-  for (int iA = 0; iA < 4; iA++) {
-    const R sgn = R(sink[iA][2]);
-    Cx<R> a[9], b[9];
-    row.load9(X + sink[iA][0] * 4 + xp, a);
-    row.load9(Y + sink[iA][1] * 4 + yp, b);
-#pragma unroll
-    for (int i = 0; i < 9; i++) a[i] = cscale(a[i], sgn);
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
-#pragma unroll
-      for (int e = 0; e < 3; e++) {
-        const int e1 = (e + 1) % 3, e2 = (e + 2) % 3;
-        Cx<R>& r = q[c * 3 + e];
-        cmac(r, a[c1 * 3 + e1], b[c2 * 3 + e2]);
-        cmsub(r, a[c1 * 3 + e2], b[c2 * 3 + e1]);
-        cmsub(r, a[c2 * 3 + e1], b[c1 * 3 + e2]);
-        cmac(r, a[c2 * 3 + e2], b[c1 * 3 + e1]);
-      }
-    }
-  }
+  for (int iA = 0; iA < 4; iA++) diquark_acc(row, X, Y, sink[iA][0], sink[iA][1], R(sink[iA][2]), xp, yp, q);
 }
 
 // G^{YX} from G^{XY}: move lane (y', x') to lane (x', y') with the table's sign.
@@ -180,13 +187,14 @@ __device__ __forceinline__ void diquark_transpose(Cx<R> q[9], int l, unsigned ma
   for (int i = 0; i < 9; i++) q[i] = cscale(shfl_idx16(q[i], src, mask), sign);
 }
 
-// One group of Wick terms sharing G and the third line Z (block offset in the
-// site row); returns the lane's share of T[mu = l >> 2][mu' = l & 3].  S1, S2,
-// TA select the term types present.
-template <bool S1, bool S2, bool TA, typename Row>
-__device__ __forceinline__ Cx<typename Row::R> diquark_eval(const Cx<typename Row::R> g[9], const Row& row, int Z,
-                                                            const DiquarkLane& dl, int l, unsigned mask, int c1A,
-                                                            int c1B, int c2A, int c2B, int cN, int cL) {
+// Slot terms of one group of Wick terms sharing G and the third line Z (block
+// offset in the site row); returns the lane's share of T[mu = l >> 2][mu' = l & 3].
+//   slot 2: T[mu][mu'] = sum_{x'} f2 sum_ce G(x', mu')[c][e] Z[mu][z2][c][e]
+//   slot 1: T[mu][mu'] = sum_{y'} f1 sum_ce G(mu', y')[c][e] Z[mu][z1][c][e]
+template <bool S1, bool S2, typename Row>
+__device__ __forceinline__ Cx<typename Row::R> diquark_slots(const Cx<typename Row::R> g[9], const Row& row, int Z,
+                                                             const DiquarkLane& dl, int l, unsigned mask, int c1A,
+                                                             int c1B, int c2A, int c2B) {
   typedef typename Row::R R;
   const int mu = l >> 2, mup = l & 3;
   Cx<R> r = czero<R>();
@@ -224,21 +232,46 @@ __device__ __forceinline__ Cx<typename Row::R> diquark_eval(const Cx<typename Ro
       if (m == mu) r = r + v;
     }
   }
-  if (TA) {
-    const R fa = R(cN * dl.sN - cL * dl.sL);
-    Cx<R> z[9];
-    row.load9(Z + mu * 4 + mup, z);
-#pragma unroll
-    for (int i = 0; i < 9; i++) {
-      Cx<R> d = cscale(g[i], fa);
-      d = d + shfl_xor16(d, 1, mask);
-      d = d + shfl_xor16(d, 2, mask);
-      d = d + shfl_xor16(d, 4, mask);
-      d = d + shfl_xor16(d, 8, mask);
-      cmac(r, d, z[i]);
-    }
-  }
   return r;
+}
+
+// Type-a terms: D = sum over the 16 lanes of fa G (all lanes get D), then the
+// lane's T[mu][mu'] = sum_ce D[c][e] Z[mu][mu'][c][e].
+template <typename R>
+__device__ __forceinline__ void diquark_D(const Cx<R> g[9], R fa, unsigned mask, Cx<R> D[9]) {
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    Cx<R> d = cscale(g[i], fa);
+    d = d + shfl_xor16(d, 1, mask);
+    d = d + shfl_xor16(d, 2, mask);
+    d = d + shfl_xor16(d, 4, mask);
+    d = d + shfl_xor16(d, 8, mask);
+    D[i] = d;
+  }
+}
+template <typename Row>
+__device__ __forceinline__ Cx<typename Row::R> diquark_typea(const Cx<typename Row::R> D[9], const Row& row, int Z,
+                                                             int l) {
+  typedef typename Row::R R;
+  Cx<R> z[9];
+  row.load9(Z + (l >> 2) * 4 + (l & 3), z);
+  Cx<R> r = czero<R>();
+#pragma unroll
+  for (int i = 0; i < 9; i++) cmac(r, D[i], z[i]);
+  return r;
+}
+
+// All Wick terms of one group: slot terms plus type-a terms with the Wick
+// coefficients (c1A, c1B, c2A, c2B, cN, cL).
+template <bool S1, bool S2, typename Row>
+__device__ __forceinline__ Cx<typename Row::R> diquark_eval(const Cx<typename Row::R> g[9], const Row& row, int Z,
+                                                            const DiquarkLane& dl, int l, unsigned mask, int c1A,
+                                                            int c1B, int c2A, int c2B, int cN, int cL) {
+  typedef typename Row::R R;
+  const Cx<R> r = diquark_slots<S1, S2>(g, row, Z, dl, l, mask, c1A, c1B, c2A, c2B);
+  Cx<R> D[9];
+  diquark_D(g, R(cN * dl.sN - cL * dl.sL), mask, D);
+  return r + diquark_typea(D, row, Z, l);
 }
 
 // Nucleon C g5, both datasets: out[0] = proton (u u d), out[1] = neutron (d d u),
@@ -250,9 +283,9 @@ __device__ __forceinline__ void nucleon_site(const Row& row, const LaneTables& l
   Cx<R> g[9];
   diquark_G(row, kU, kD, c_nuc_sink, l >> 2, l & 3, g);  // G^{ud}
   const DiquarkLane dl = unpack_diquark_lane(lt.nuc);
-  out[0] = diquark_eval<true, false, true>(g, row, kU, dl, l, mask, -1, 0, 0, 0, 1, 0);
+  out[0] = diquark_eval<true, false>(g, row, kU, dl, l, mask, -1, 0, 0, 0, 1, 0);
   diquark_transpose<R>(g, l, mask, R(-1));  // G^{du}
-  out[1] = diquark_eval<true, false, true>(g, row, kD, dl, l, mask, -1, 0, 0, 0, 1, 0);
+  out[1] = diquark_eval<true, false>(g, row, kD, dl, l, mask, -1, 0, 0, 0, 1, 0);
 }
 
 // Generic meson block of the lines A and B (block offsets): lane g1 gets
@@ -323,34 +356,86 @@ __device__ __forceinline__ void meson_site(const Row& row, int A, int B, const L
 //   isospin 1/2, G^{AA}, Z = B: (0, 2, 0, -2, 1, -1)        x 1/3
 //   isospin 1/2, G^{AB}, Z = A: (-4, 0, 2, -2, 4, 0)        x 1/3
 //   isospin 3/2, G^{AA}, Z = A: (-1, 1, 1, -1, 1, -1)
-// out = {iso-1/2 Delta+ (u,u,d), iso-1/2 Delta0 (d,d,u), iso-3/2 Delta++ (u,u,u),
-// iso-3/2 Delta- (d,d,d)} for table g (k = g + 1) and lane (mu, mu').
-template <typename Row>
-__device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt, int g, int l, unsigned mask,
-                                           Cx<typename Row::R> out[4]) {
+// Both G^{AA} groups have cN = 1, cL = -1, so they share the type-a sum D.
+//
+// The three sink tables share products: C g_1 and C g_2 use the diagonal
+// pairs (nu, nu) with signs (+ - - +) and (+ + - -), so with
+// A = P00 - P22 and B = P11 - P33, G_1 = A - B and G_2 = A + B; C g_3 uses
+// (0,1), (1,0), (2,3), (3,2) with signs (+ + - -), and for a single flavour
+// P^{XX}_{(lam, nu)}(x', y') = P^{XX}_{(nu, lam)}(y', x'), so
+// G_3^{XX} = Q + Q^T with Q = P01 - P23 (lane transpose).  For G^{uu} and
+// G^{dd} that is 6 products instead of 12 (G^{ud} keeps 12): 24 per site and
+// lane instead of 36.  The tables are pinned in the spin-table tests.
+//
+// For k = g + 1 and lane (mu, mu'), out(g, j, v) receives the final value of
+// j = 0: iso-1/2 Delta+ (u,u,d), 1: iso-1/2 Delta0 (d,d,u), 2: iso-3/2
+// Delta++ (u,u,u), 3: iso-3/2 Delta- (d,d,d); the G^{ud} part of the
+// iso-1/2 values is parked first with part(g, j, v) and read back with
+// part_get(g, j) (registers are the scarce resource here).
+template <typename Row, typename Out, typename Part, typename PartGet>
+__device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt, int l, unsigned mask, Out&& out,
+                                           Part&& part, PartGet&& part_get) {
   typedef typename Row::R R;
-  const DiquarkLane dl = unpack_diquark_lane(g == 0 ? lt.delta[0] : g == 1 ? lt.delta[1] : lt.delta[2]);
+  const int xp = l >> 2, yp = l & 3;
   const R third = R(1) / R(3);
-#pragma unroll
-  for (int i = 0; i < 4; i++) out[i] = czero<R>();
-  // G^{uu}, G^{dd}: isospin 1/2 with the other flavour on the third line, isospin 3/2 with the same
+  // iso-1/2 partial sums from G^{ud} / G^{du}, completed by the G^{uu} / G^{dd} terms
+  // G^{ud} (A = u) and its lane transpose G^{du} (A = d; C g_k is symmetric)
+#pragma unroll 1
+  for (int g = 0; g < 3; g++) {
+    Cx<R> q[9];
+    diquark_G(row, kU, kD, c_delta_sink[g], xp, yp, q);
+    const DiquarkLane dl = unpack_diquark_lane(g == 0 ? lt.delta[0] : g == 1 ? lt.delta[1] : lt.delta[2]);
+    part(g, 0, cscale(diquark_eval<true, true>(q, row, kU, dl, l, mask, -4, 0, 2, -2, 4, 0), third));
+    diquark_transpose<R>(q, l, mask, R(1));
+    part(g, 1, cscale(diquark_eval<true, true>(q, row, kD, dl, l, mask, -4, 0, 2, -2, 4, 0), third));
+  }
+  // G^{uu} (pair 0: Delta+ and Delta++) and G^{dd} (pair 1: Delta0 and Delta-)
 #pragma unroll 1
   for (int pair = 0; pair < 2; pair++) {
     const int X = pair == 0 ? kU : kD;
     const int O = pair == 0 ? kD : kU;
-    Cx<R> q[9];
-    diquark_G(row, X, X, c_delta_sink[g], l >> 2, l & 3, q);
-    const Cx<R> a = diquark_eval<true, true, true>(q, row, O, dl, l, mask, 0, 2, 0, -2, 1, -1);
-    const Cx<R> b = diquark_eval<true, true, true>(q, row, X, dl, l, mask, -1, 1, 1, -1, 1, -1);
-    out[pair] = out[pair] + cscale(a, third);
-    out[2 + pair] = out[2 + pair] + b;
+    Cx<R> ga[9], gb[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) ga[i] = gb[i] = czero<R>();
+    diquark_acc(row, X, X, 0, 0, R(1), xp, yp, ga);
+    diquark_acc(row, X, X, 2, 2, R(-1), xp, yp, ga);
+    diquark_acc(row, X, X, 1, 1, R(1), xp, yp, gb);
+    diquark_acc(row, X, X, 3, 3, R(-1), xp, yp, gb);
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+      const Cx<R> t = ga[i];
+      ga[i] = t - gb[i];
+      gb[i] = t + gb[i];
+    }
+#pragma unroll
+    for (int g = 0; g < 3; g++) {
+      Cx<R> q[9];
+      if (g < 2) {
+#pragma unroll
+        for (int i = 0; i < 9; i++) q[i] = g == 0 ? ga[i] : gb[i];
+      } else {
+#pragma unroll
+        for (int i = 0; i < 9; i++) q[i] = czero<R>();
+        diquark_acc(row, X, X, 0, 1, R(1), xp, yp, q);
+        diquark_acc(row, X, X, 2, 3, R(-1), xp, yp, q);
+        Cx<R> t[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) t[i] = q[i];
+        diquark_transpose<R>(t, l, mask, R(1));
+#pragma unroll
+        for (int i = 0; i < 9; i++) q[i] = q[i] + t[i];
+      }
+      const DiquarkLane dl = unpack_diquark_lane(g == 0 ? lt.delta[0] : g == 1 ? lt.delta[1] : lt.delta[2]);
+      Cx<R> iso12 = diquark_slots<true, true>(q, row, O, dl, l, mask, 0, 2, 0, -2);
+      Cx<R> iso32 = diquark_slots<true, true>(q, row, X, dl, l, mask, -1, 1, 1, -1);
+      Cx<R> D[9];
+      diquark_D(q, R(dl.sN + dl.sL), mask, D);  // cN = 1, cL = -1 for both groups
+      iso12 = iso12 + diquark_typea(D, row, O, l);
+      iso32 = iso32 + diquark_typea(D, row, X, l);
+      out(g, pair, part_get(g, pair) + cscale(iso12, third));
+      out(g, 2 + pair, iso32);
+    }
   }
-  // G^{ud} (A = u) and its lane transpose G^{du} (A = d; C g_k is symmetric)
-  Cx<R> q[9];
-  diquark_G(row, kU, kD, c_delta_sink[g], l >> 2, l & 3, q);
-  out[0] = out[0] + cscale(diquark_eval<true, true, true>(q, row, kU, dl, l, mask, -4, 0, 2, -2, 4, 0), third);
-  diquark_transpose<R>(q, l, mask, R(1));
-  out[1] = out[1] + cscale(diquark_eval<true, true, true>(q, row, kD, dl, l, mask, -4, 0, 2, -2, 4, 0), third);
 }
 
 }  // namespace p2

@@ -162,3 +162,18 @@ def test_delta_all_isospins_plain():
     err = per_t_error(out, what, 6, moms, ref, taus)
     assert err.max() < TOL, err
     ctx.close()
+
+
+@pytest.mark.parametrize("what", [p2.DELTA_ISO12, p2.DELTA_ISO32])
+@pytest.mark.parametrize("mode", [p2.P2_PLAIN_FP64, p2.P2_SPLIT_FP16])
+def test_delta_single_isospin(what, mode):
+    """One Delta isospin block alone (the other block's slots are not part of
+    the result), both forms."""
+    ctx = p2.Context((3, 4, 5, 6))
+    bufs = device_props(ctx, [(43, 0), (43, 1)], t0=1)
+    out, moms = run(ctx, bufs, (2, 1, 0, 1), 6, what, q2max=1, mode=mode)
+    taus = list(range(6))
+    ref = oracle_blocks(ctx.L, bufs, (2, 1, 0, 1), moms, what, taus)
+    err = per_t_error(out, what, 6, moms, ref, taus)
+    assert err.max() < (TOL if mode == p2.P2_PLAIN_FP64 else 1e-6), err
+    ctx.close()
