@@ -192,6 +192,34 @@ p2_status p2_ft_apply(p2_ctx* ctx, const double* field, int dof, int nt, const i
 p2_status p2_ft_apply_noalloc(p2_ctx* ctx, const double* field, int dof, int nt, const int* moms, int nmom,
                               int sign, double* out);
 
+/* ---- table-driven baryons (the reference's UDSC set) --------------------- */
+/* contractBaryonsUDSC(propUP, propDN, propST, propCH, only_st, only_ch)
+ * (lib/PLEGMA_Correlator.cu:137-189, lib/kernels/PLEGMA_baryons_udsc.cu:
+ * 85-309): the octet and decuplet baryons of u, d, s, c quarks with the
+ * projected interpolators of the reference's generated spin tables (e.g.
+ * proton/Pp_Cg5_Cg5, DeltaPl/Pp_Cgi_Cgi, DeltaPlPl/Ppgigj_Cgi_Cgj).  The
+ * flavour products run in the reference's order, skipping those that need a
+ * propagator that is not given (index -1); only_st / only_ch keep only the
+ * products containing s / c.  Result: [dataset][tau][mom] complex double,
+ * datasets in the order of p2_udsc_datasets.  Plain FP64 form; FP64
+ * device-resident propagators. */
+typedef struct {
+  int source[4];
+  int totalT;
+  const int* moms; /* explicit momenta [nmom][3], or NULL for q2max */
+  int nmom;
+  int q2max;
+  int prop_u, prop_d, prop_s, prop_c; /* indices into props, -1 = not given */
+  int only_st, only_ch;
+  double* out;
+  int out_location;
+} p2_udsc_request;
+
+/* Dataset names ("proton/Pp_Cg5_Cg5", ...) a request produces, one per line,
+ * into names (capacity cap, NUL-terminated; may be NULL); returns their count. */
+int p2_udsc_datasets(const p2_udsc_request* req, char* names, size_t cap);
+p2_status p2_contract_udsc(p2_ctx* ctx, const p2_prop* props, int nprops, const p2_udsc_request* req);
+
 /* ---- CUDA graphs -------------------------------------------------------- */
 /* The whole launch sequence of p2_contract_project(props, reqs) recorded once
  * and replayed with one cudaGraphLaunch: batched sources in one submission,

@@ -368,3 +368,76 @@ void orc_udsc_site(const double* p1, const double* p2, const double* p3, int n, 
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// Table-driven baryon two-point functions of one flavour product
+// (lib/kernels/PLEGMA_baryons_udsc.cu:85-134 per site, projected as
+// lib/kernels/PLEGMA_kernel_utils.cuh:820-860):
+//   p1, p2, p3   the product's three propagators (flavour-sorted roles)
+//   ndata        datasets; dataset d has entries ent_begin[d] .. ent_begin[d+1]-1
+//                of idx[][6] (spin indices) and w[][2] (single-precision weights)
+//   out          [ntau][ndata][nmom] complex; abs_sum [ntau][ndata] (may be NULL)
+int orc_udsc_twopt(const int* L, int nt, int t_first, const void* p1, const void* p2, const void* p3, int fp32,
+                   const int* src, const int* moms, int nmom, int ndata, const int* ent_begin,
+                   const signed char* idx, const float* w, const int* taus, int ntau, double* out,
+                   double* abs_sum) {
+  const long V3 = (long)L[0] * L[1] * L[2];
+  const int T = L[3];
+  View v1{p1, fp32, V3 * nt}, v2{p2, fp32, V3 * nt}, v3{p3, fp32, V3 * nt};
+  for (int it = 0; it < ntau; it++) {
+    const int t = (src[3] + taus[it]) % T;
+    const int j = ((t - t_first) % T + T) % T;
+    if (j >= nt) return 2;
+    cplx* o = (cplx*)out + (long)it * ndata * nmom;
+    for (long i = 0; i < (long)ndata * nmom; i++) o[i] = {0, 0};
+    std::vector<double> asum(ndata, 0.0);
+#pragma omp parallel
+    {
+      std::vector<cplx> loc((size_t)ndata * nmom, cplx{0, 0});
+      std::vector<double> locabs(ndata, 0.0);
+      Prop A, B, Cp;
+#pragma omp for schedule(static)
+      for (long x3 = 0; x3 < V3; x3++) {
+        const long sid = x3 + V3 * j;
+        gather(v1, sid, A);
+        gather(v2, sid, B);
+        gather(v3, sid, Cp);
+        const int id[3] = {(int)(x3 % L[0]), (int)((x3 / L[0]) % L[1]), (int)(x3 / ((long)L[0] * L[1]))};
+        for (int d = 0; d < ndata; d++) {
+          cplx acc = {0, 0};
+          for (int e = ent_begin[d]; e < ent_begin[d + 1]; e++) {
+            const signed char* m = idx + 6 * e;
+            const cplx we = {(double)w[2 * e], (double)w[2 * e + 1]};
+            for (int cc1 = 0; cc1 < 6; cc1++) {
+              const int a = p2::kEps[cc1][0], b = p2::kEps[cc1][1], c = p2::kEps[cc1][2];
+              for (int cc2 = 0; cc2 < 6; cc2++) {
+                const int a1 = p2::kEps[cc2][0], b1 = p2::kEps[cc2][1], c1 = p2::kEps[cc2][2];
+                const cplx f = (double)(p2::kEpsSign[cc1] * p2::kEpsSign[cc2]) * we;
+                acc = acc + f * A[m[0]][m[1]][a][a1] * B[m[2]][m[3]][b][b1] * Cp[m[4]][m[5]][c][c1];
+              }
+            }
+          }
+          locabs[d] += std::sqrt(acc.x * acc.x + acc.y * acc.y);
+          for (int p = 0; p < nmom; p++) {
+            double ph = 0;
+            for (int i = 0; i < 3; i++) ph += (double)moms[3 * p + i] * (double)(id[i] - src[i]) / (double)L[i];
+            ph *= 2.0 * M_PI;
+            const cplx e = {std::cos(ph), -std::sin(ph)};
+            loc[(size_t)d * nmom + p] = loc[(size_t)d * nmom + p] + acc * e;
+          }
+        }
+      }
+#pragma omp critical
+      {
+        for (long i = 0; i < (long)ndata * nmom; i++) o[i] = o[i] + loc[i];
+        for (int d = 0; d < ndata; d++) asum[d] += locabs[d];
+      }
+    }
+    if (abs_sum)
+      for (int d = 0; d < ndata; d++) abs_sum[(long)it * ndata + d] = asum[d];
+  }
+  return 0;
+}
+
+}  // extern "C"

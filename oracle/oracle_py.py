@@ -37,6 +37,10 @@ def oracle():
                                C.c_int, C.c_void_p]
         lib.orc_udsc_site.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                       C.c_void_p]
+        lib.orc_udsc_twopt.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.c_int,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.c_int,
+                                       C.c_void_p, C.c_void_p]
         _orc = lib
     return _orc
 
@@ -136,3 +140,37 @@ def ref_delta(u1, d1, iso32, g):
     d1 = np.ascontiguousarray(d1, dtype=np.complex128)
     lib.ref_delta(u1.ctypes.data, d1.ctypes.data, int(iso32), int(g), out.ctypes.data)
     return out
+
+
+def udsc_twopt(L, props, src, moms, datasets, taus, t_first=0, fp32=False):
+    """Table-driven baryon two-point functions of one flavour product.
+
+    props: the product's three propagators (complex arrays [144][V3*nt]);
+    datasets: [(name, [(s0..s5)], [complex weight])] as plegma_b200.udsc.products().
+    Returns (out[ntau][ndata][nmom], abs_sum[ntau][ndata])."""
+    lib = oracle()
+    L = _ip(L)
+    V3 = int(L[0] * L[1] * L[2])
+    nt = props[0].shape[-1] // V3
+    moms = _ip(moms).reshape(-1, 3)
+    taus = _ip(taus)
+    ent = [0]
+    idx, w = [], []
+    for _, tups, ws in datasets:
+        idx += [list(t) for t in tups]
+        w += [[np.real(x), np.imag(x)] for x in ws]
+        ent.append(len(idx))
+    idx = np.ascontiguousarray(idx, dtype=np.int8)
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    ent = _ip(ent)
+    props = [np.ascontiguousarray(p) for p in props]
+    out = np.zeros((len(taus), len(datasets), len(moms)), dtype=np.complex128)
+    asum = np.zeros((len(taus), len(datasets)), dtype=np.float64)
+    rc = lib.orc_udsc_twopt(L.ctypes.data_as(C.POINTER(C.c_int)), nt, t_first, props[0].ctypes.data,
+                            props[1].ctypes.data, props[2].ctypes.data, int(fp32),
+                            _ip(src).ctypes.data_as(C.POINTER(C.c_int)), moms.ctypes.data_as(C.POINTER(C.c_int)),
+                            len(moms), len(datasets), ent.ctypes.data, idx.ctypes.data, w.ctypes.data,
+                            taus.ctypes.data_as(C.POINTER(C.c_int)), len(taus), out.ctypes.data, asum.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"orc_udsc_twopt failed ({rc})")
+    return out, asum

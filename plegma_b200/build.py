@@ -17,8 +17,9 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libplegma2pt.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+GENDIR = os.path.join(LIBDIR, "gen")  # headers generated at build time (not committed)
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp", "--expt-relaxed-constexpr",
-                     "-I" + os.path.join(ROOT, "include")]
+                     "-I" + os.path.join(ROOT, "include"), "-I" + GENDIR]
 
 
 def _sources():
@@ -27,7 +28,7 @@ def _sources():
 
 def _deps():
     return _sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))) + \
-        [os.path.join(ROOT, "include", "plegma2pt.h")]
+        [os.path.join(ROOT, "include", "plegma2pt.h"), os.path.join(GENDIR, "udsc_tables.h")]
 
 
 def _stale(out, deps):
@@ -41,8 +42,10 @@ def build(force=False, verbose=False, jobs=None):
     os.makedirs(LIBDIR, exist_ok=True)
     objdir = os.path.join(LIBDIR, "obj")
     os.makedirs(objdir, exist_ok=True)
-    from . import spin
+    from . import spin, udsc
     spin.emit_header(os.path.join(CSRC, "spin_tables.h"))
+    os.makedirs(GENDIR, exist_ok=True)
+    udsc.emit_header(os.path.join(GENDIR, "udsc_tables.h"))
     headers = [d for d in _deps() if not d.endswith(".cu")]
     objs = []
     procs = []

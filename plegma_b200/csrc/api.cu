@@ -576,6 +576,7 @@ p2_status p2_ctx_destroy(p2_ctx* c) {
     for (cudaEvent_t e : p.pool) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->stream);
   p2::precision_release(c);
+  p2_udsc_release(c);
   delete c;
   return P2_OK;
 }

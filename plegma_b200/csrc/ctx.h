@@ -43,6 +43,8 @@ constexpr unsigned kAllBits = 0x7Fu;
 
 }  // namespace p2host
 
+struct p2_udsc_cache;  // table-driven baryons: per-product lane plans (udsc.cu)
+
 struct p2_ctx {
   p2_geom g{};
   int Ll[4]{};
@@ -74,6 +76,7 @@ struct p2_ctx {
   // plain form: phase tables and momentum list, rebuilt when the momentum list changes
   p2host::DevBuf ptab;
   std::vector<int> plain_moms_key;
+  p2_udsc_cache* udsc = nullptr;
   // launch-shape autotuner (shared with the context's graphs)
   std::shared_ptr<p2host::Tuner> tuner = std::make_shared<p2host::Tuner>();
 
@@ -183,6 +186,8 @@ p2_status make_plan(p2_ctx* c, const p2_request& r, Plan& pl);
 p2_status upload_async(p2_ctx* c, DevBuf& b, const void* src, size_t bytes, const char* what);
 
 }  // namespace p2host
+
+void p2_udsc_release(p2_ctx* c);
 
 namespace p2 {
 // split-FP16 path (precision.cu)

@@ -59,6 +59,13 @@ class P2Request(C.Structure):
                 ("prop_d", C.c_int), ("out", C.c_void_p), ("out_location", C.c_int)]
 
 
+class P2UdscRequest(C.Structure):
+    _fields_ = [("source", C.c_int * 4), ("totalT", C.c_int), ("moms", C.POINTER(C.c_int)), ("nmom", C.c_int),
+                ("q2max", C.c_int), ("prop_u", C.c_int), ("prop_d", C.c_int), ("prop_s", C.c_int),
+                ("prop_c", C.c_int), ("only_st", C.c_int), ("only_ch", C.c_int), ("out", C.c_void_p),
+                ("out_location", C.c_int)]
+
+
 class P2Block(C.Structure):
     _fields_ = [("bit", C.c_uint), ("groups", C.c_int), ("datasets", C.c_int), ("comps", C.c_int),
                 ("offset", C.c_size_t)]
@@ -73,7 +80,7 @@ EXPORTS = ["p2_ctx_create", "p2_ctx_destroy", "p2_last_error", "p2_sync", "p2_se
            "p2_mom_list", "p2_block_info", "p2_contract_project", "p2_contract_position", "p2_ft_apply",
            "p2_synth_propagator", "p2_profile_enable", "p2_profile_read", "p2_alloc", "p2_free", "p2_copy",
            "p2_ft_apply_noalloc", "p2_set_workspace", "p2_graph_create", "p2_graph_launch", "p2_graph_sync",
-           "p2_graph_destroy", "p2_tune_enable", "p2_tune_count"]
+           "p2_graph_destroy", "p2_tune_enable", "p2_tune_count", "p2_udsc_datasets", "p2_contract_udsc"]
 
 _lib = None
 
@@ -99,6 +106,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.p2_graph_destroy.argtypes = [C.c_void_p]
     lib.p2_tune_enable.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
     lib.p2_tune_count.argtypes = [C.c_void_p]
+    lib.p2_udsc_datasets.argtypes = [C.POINTER(P2UdscRequest), C.c_char_p, C.c_size_t]
+    lib.p2_contract_udsc.argtypes = [C.c_void_p, C.POINTER(P2Prop), C.c_int, C.POINTER(P2UdscRequest)]
     lib.p2_components.argtypes = [C.c_uint]
     lib.p2_mom_list.argtypes = [C.c_int, C.POINTER(C.c_int)]
     lib.p2_block_info.argtypes = [C.c_uint, C.c_int, C.c_int, C.POINTER(P2Block), C.c_int, C.POINTER(C.c_size_t)]
@@ -242,6 +251,32 @@ class Context:
         pa = (P2Prop * len(props))(*props)
         self.check(self.lib.p2_contract_position(self.h, pa, len(props), C.byref(req)))
 
+    @staticmethod
+    def udsc_request(source, totalT, out_ptr, out_location=P2_DEVICE, q2max=0, moms: Optional[np.ndarray] = None,
+                     prop_u=-1, prop_d=-1, prop_s=-1, prop_c=-1, only_st=False, only_ch=False) -> P2UdscRequest:
+        """A table-driven baryon request (contractBaryonsUDSC); prop_* index the props list, -1 = not given."""
+        r = P2UdscRequest()
+        r.source[:] = list(source)
+        r.totalT = totalT
+        if moms is not None:
+            m = np.ascontiguousarray(moms, dtype=np.int32)
+            r._moms_keep = m
+            r.moms = m.ctypes.data_as(C.POINTER(C.c_int))
+            r.nmom = len(m)
+        else:
+            r.moms = None
+            r.nmom = 0
+        r.q2max = q2max
+        r.prop_u, r.prop_d, r.prop_s, r.prop_c = prop_u, prop_d, prop_s, prop_c
+        r.only_st, r.only_ch = int(only_st), int(only_ch)
+        r.out = out_ptr
+        r.out_location = out_location
+        return r
+
+    def contract_udsc(self, props: Sequence[P2Prop], req: P2UdscRequest):
+        pa = (P2Prop * len(props))(*props)
+        self.check(self.lib.p2_contract_udsc(self.h, pa, len(props), C.byref(req)))
+
     def graph(self, props: Sequence[P2Prop], reqs: Sequence[P2Request]) -> "Graph":
         """p2_graph_create: record the launch sequence of contract_project(props, reqs)."""
         return Graph(self, props, reqs)
@@ -307,6 +342,16 @@ class Graph:
             self.close()
         except Exception:
             pass
+
+
+def udsc_datasets(req: P2UdscRequest):
+    """Dataset names of a table-driven baryon request, in result order."""
+    lib = load()
+    n = lib.p2_udsc_datasets(C.byref(req), None, 0)
+    buf = C.create_string_buffer(64 * max(n, 1) + 1)
+    lib.p2_udsc_datasets(C.byref(req), buf, len(buf))
+    names = buf.value.decode().split("\n")
+    return [x for x in names if x]
 
 
 def result_blocks(contractions: int, totalT: int, nmom: int, flat: np.ndarray):

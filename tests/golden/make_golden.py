@@ -38,7 +38,7 @@ def c_array_numbers(text: str, name: str):
         j += 1
     body = re.sub(r"//[^\n]*", "", text[i:j + 1])
     body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
-    return [float(x) for x in re.findall(r"-?\d+(?:\.\d+)?", body)]
+    return [float(x) for x in re.findall(r"-?\d+(?:\.\d+)?(?:[eE][-+]?\d+)?", body)]
 
 
 def reference_digests(ref_root: str):
@@ -63,6 +63,33 @@ def reference_digests(ref_root: str):
         "eps": spin.table_digest(c_array_numbers(ku, "eps")),
         "sgn_eps": spin.table_digest(c_array_numbers(ku, "sgn_eps")),
     }
+    out.update(reference_udsc_digests(kern))
+    return out
+
+
+def reference_udsc_digests(kern: str):
+    """Digests of the reference's table-driven baryon lists
+    (PLEGMA_baryons_udsc_arrays.cu/.cuh, written by its python/baryons.py):
+    the product list, the dataset names, and per dataset the ordered
+    (6 spin indices, single-precision weight) entries."""
+    from plegma_b200 import udsc
+    with open(os.path.join(kern, "PLEGMA_baryons_udsc_arrays.cuh")) as f:
+        hdr = f.read()
+    with open(os.path.join(kern, "PLEGMA_baryons_udsc_arrays.cu")) as f:
+        arr = f.read()
+    prods = re.findall(r'"(\w+)"', re.search(r"BP_prop_prods\s*=\s*\{(.*?)\};", hdr).group(1))
+    names_block = re.search(r"BP_prop_prods_names\s*=\s*\{(.*?)\};\n", hdr, flags=re.S).group(1)
+    names = re.findall(r'"([^"]+)"', names_block)
+    out = {"udsc_products": udsc.names_digest(prods), "udsc_names": udsc.names_digest(names)}
+    ds = {}
+    for n in names:
+        key = n.replace("/", "_")
+        idx = [int(x) for x in c_array_numbers(arr, key + "_idxs")]
+        vals = c_array_numbers(arr, key + "_vals")
+        tups = [tuple(idx[6 * i:6 * i + 6]) for i in range(len(idx) // 6)]
+        w = [complex(vals[2 * i], vals[2 * i + 1]) for i in range(len(vals) // 2)]
+        ds[n] = udsc.ordered_digest(tups, w)
+    out["udsc_datasets"] = ds
     return out
 
 

@@ -130,3 +130,17 @@ def test_graph_and_workspace_entry_points_validate_on_host_only_context():
         ctx.graph([prop, prop], [req])
     assert e.value.status == p2.P2_ERR_UNSUPPORTED
     ctx.close()
+
+
+def test_udsc_dataset_selection_follows_the_reference_filters():
+    """p2_udsc_datasets: products needing a missing flavour are skipped,
+    only_st / only_ch keep the products with s / c, order as the reference's."""
+    from plegma_b200 import udsc
+    prods = udsc.products()
+    R = p2.Context.udsc_request
+    assert len(p2.udsc_datasets(R((0, 0, 0, 0), 4, 0, prop_u=0, prop_d=1))) == 28
+    allds = p2.udsc_datasets(R((0, 0, 0, 0), 4, 0, prop_u=0, prop_d=1, prop_s=2, prop_c=3))
+    assert allds == [n for _, dss in prods for n, _, _ in dss]
+    only_ch = p2.udsc_datasets(R((0, 0, 0, 0), 4, 0, prop_u=0, prop_d=1, prop_s=2, prop_c=3, only_ch=True))
+    assert only_ch == [n for k, dss in prods if "c" in k for n, _, _ in dss]
+    assert p2.udsc_datasets(R((0, 0, 0, 0), 4, 0, prop_s=0, only_ch=True)) == []
