@@ -507,6 +507,69 @@ class PLEGMA_Correlator {
     run(p1, p2, what, false);
   }
 
+  // lib/PLEGMA_Correlator.cu:137-189: the table-driven baryon set over the u,
+  // d, s, c propagators; a propagator created with NONE is not available and
+  // the flavour products that need it are skipped.  One dataset per
+  // (baryon, interpolator) with an empty shape.  Momentum space; FP64.
+  void contractBaryonsUDSC(PLEGMA_Propagator<Float>& up, PLEGMA_Propagator<Float>& dn, PLEGMA_Propagator<Float>& st,
+                           PLEGMA_Propagator<Float>& ch, bool only_st = false, bool only_ch = false) {
+    if (corr_space != MOMENTUM_SPACE)
+      throw PLEGMA_exception("contractBaryonsUDSC: position-space output is not supported");
+    PLEGMA_Propagator<Float>* all[4] = {&up, &dn, &st, &ch};
+    std::vector<p2_prop> props;
+    int idx[4];
+    for (int k = 0; k < 4; k++) {
+      idx[k] = all[k]->getAllocation() == NONE ? -1 : (int)props.size();
+      if (idx[k] >= 0) props.push_back(all[k]->view());
+    }
+    std::vector<int> m = corr_mom_space->int_moms();
+    const int nmom = (int)m.size() / 3;
+    p2_udsc_request r{};
+    for (int d = 0; d < 4; d++) r.source[d] = source[d];
+    r.totalT = totalT;
+    r.moms = m.data();
+    r.nmom = nmom;
+    r.prop_u = idx[0];
+    r.prop_d = idx[1];
+    r.prop_s = idx[2];
+    r.prop_c = idx[3];
+    r.only_st = only_st;
+    r.only_ch = only_ch;
+    const int nd = p2_udsc_datasets(&r, nullptr, 0);
+    std::vector<char> text((size_t)64 * (nd + 1), 0);
+    p2_udsc_datasets(&r, text.data(), text.size());
+    shape = {};
+    groups = {};
+    description = "";
+    datasets.clear();
+    std::string cur;
+    for (char ch_ : std::string(text.data())) {
+      if (ch_ == '\n') {
+        datasets.push_back(cur);
+        cur.clear();
+      } else {
+        cur += ch_;
+      }
+    }
+    buf.assign(getTotalSize() * 2, Float(0));
+    if (nd == 0) return;
+    std::vector<double> res((size_t)2 * nd * totalT * nmom, 0.0);
+    r.out = res.data();
+    r.out_location = P2_HOST;
+    Runtime::check(p2_contract_udsc(Runtime::context(), props.data(), (int)props.size(), &r), "contract");
+    const int lt = localT();
+    for (int d = 0; d < nd; d++)
+      for (int i = 0; i < lt; i++) {
+        const int tau = (i + startT()) % totalT;
+        for (int p = 0; p < nmom; p++) {
+          const size_t src = ((size_t)d * totalT + tau) * nmom + p;
+          const size_t dst = ((size_t)d * lt + i) * nmom + p;
+          buf[2 * dst] = (Float)res[2 * src];
+          buf[2 * dst + 1] = (Float)res[2 * src + 1];
+        }
+      }
+  }
+
   // ASCII writer of lib/PLEGMA_Correlator.cu:721-807 (momentum space, one process).
   void writeASCII(const std::string& filename_out) const {
     if (corr_space != MOMENTUM_SPACE) throw PLEGMA_exception("WriteASCII do not support writing in position space.");

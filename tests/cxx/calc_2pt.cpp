@@ -1,7 +1,7 @@
 // A caller of the drop-in C++ surface, written the way the reference's
 // production driver (plegma/Calc_2pt.cpp:73-131) uses PLEGMA_Correlator:
 // two propagators, a momentum-space correlator per source, contractMesons*,
-// contractBaryons, writeFile.  The GPU tests compare what it writes with the
+// contractBaryons, contractBaryonsUDSC, writeFile.  The GPU tests compare what it writes with the
 // C ABI results and the oracle.
 //
 //   calc_2pt Lx Ly Lz Lt sx sy sz st totalT q2max mode out_prefix
@@ -44,6 +44,11 @@ int main(int argc, char** argv) {
     bar.setMode(mode);
     bar.contractBaryons(up, dn);
     bar.writeFile(out + "_baryons", DEFAULT_FORMAT);
+
+    PLEGMA_Correlator<double> udsc(MOMENTUM_SPACE, src, q2max, totalT);
+    PLEGMA_Propagator<double> st(NONE), ch(NONE);
+    udsc.contractBaryonsUDSC(up, dn, st, ch);
+    udsc.writeFile(out + "_udsc", DEFAULT_FORMAT);
 
     PLEGMA_Correlator<double> pos(POSITION_SPACE, src, 0, totalT);
     pos.contractBaryons(up, dn);

@@ -136,3 +136,20 @@ def test_ft_apply(outputs):
     u = bufs[0].cpu().numpy()
     ref = orc.ft(L, u.reshape(144, -1), 144, L[3], moms, -1)
     assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-13
+
+
+def test_udsc_through_the_drop_in(outputs):
+    """contractBaryonsUDSC with s and c not allocated: the 28 light datasets,
+    empty shape, values equal to the C ABI's on the same propagators."""
+    import torch
+    prefix, ctx, bufs, moms = outputs
+    meta, v = load(prefix + "_udsc")
+    req = ctx.udsc_request(SRC, TOTALT, 0, moms=moms, prop_u=0, prop_d=1)
+    names = p2.udsc_datasets(req)
+    assert meta["shape"] == [TOTALT, len(moms), 2]
+    assert meta["datasets"] == ["/" + n for n in names]
+    out = torch.zeros(len(names) * TOTALT * len(moms), dtype=torch.complex128, device="cuda")
+    req.out = out.data_ptr()
+    ctx.contract_udsc([ctx.prop(b.data_ptr()) for b in bufs], req)
+    ctx.sync()
+    assert np.array_equal(v, out.cpu().numpy())
