@@ -192,6 +192,14 @@ p2_status p2_ft_apply(p2_ctx* ctx, const double* field, int dof, int nt, const i
 p2_status p2_ft_apply_noalloc(p2_ctx* ctx, const double* field, int dof, int nt, const int* moms, int nmom,
                               int sign, double* out);
 
+/* Source-relative times tau of a request that this rank computes: the slices
+ * of the window inside its time slab (p2_geom coords[3]) that both
+ * propagator views hold.  Writes up to max of them into taus (may be NULL)
+ * and returns their count, or -1 for an invalid request; works on host-only
+ * contexts.  The reference's counterpart is the window bookkeeping of
+ * PLEGMA_Correlator (startT/endT/localT, include/PLEGMA_Correlator.h:53-79). */
+int p2_local_taus(p2_ctx* ctx, const p2_prop* props, int nprops, const p2_request* req, int* taus, int max);
+
 /* ---- table-driven baryons (the reference's UDSC set) --------------------- */
 /* contractBaryonsUDSC(propUP, propDN, propST, propCH, only_st, only_ch)
  * (lib/PLEGMA_Correlator.cu:137-189, lib/kernels/PLEGMA_baryons_udsc.cu:

@@ -726,6 +726,20 @@ p2_status p2_contract_project(p2_ctx* c, const p2_prop* props, int nprops, const
   return P2_OK;
 }
 
+int p2_local_taus(p2_ctx* c, const p2_prop* props, int nprops, const p2_request* r, int* taus, int max) {
+  if (!c || !props || !r || nprops < 1) return -1;
+  if (r->prop_u < 0 || r->prop_u >= nprops || r->prop_d < 0 || r->prop_d >= nprops) return -1;
+  for (int i = 0; i < nprops; i++)
+    if (check_prop(c, props[i], "prop") != P2_OK) return -1;
+  Plan pl;
+  if (make_plan(c, *r, pl) != P2_OK) return -1;
+  const int idx = 0;
+  const Work w = make_work(c, props, r, &idx, 1, c->T);
+  const int n = (int)w.sl.size();
+  for (int i = 0; taus && i < n && i < max; i++) taus[i] = w.sl[i].tau;
+  return n;
+}
+
 p2_status p2_contract_position(p2_ctx* c, const p2_prop* props, int nprops, const p2_request* r) {
   if (!c) return P2_ERR_INVALID_ARG;
   if (!props || !r || nprops < 1) return c->fail(P2_ERR_INVALID_ARG, "empty props or request");

@@ -80,7 +80,7 @@ EXPORTS = ["p2_ctx_create", "p2_ctx_destroy", "p2_last_error", "p2_sync", "p2_se
            "p2_mom_list", "p2_block_info", "p2_contract_project", "p2_contract_position", "p2_ft_apply",
            "p2_synth_propagator", "p2_profile_enable", "p2_profile_read", "p2_alloc", "p2_free", "p2_copy",
            "p2_ft_apply_noalloc", "p2_set_workspace", "p2_graph_create", "p2_graph_launch", "p2_graph_sync",
-           "p2_graph_destroy", "p2_tune_enable", "p2_tune_count", "p2_udsc_datasets", "p2_contract_udsc"]
+           "p2_graph_destroy", "p2_tune_enable", "p2_tune_count", "p2_udsc_datasets", "p2_contract_udsc", "p2_local_taus"]
 
 _lib = None
 
@@ -106,6 +106,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.p2_graph_destroy.argtypes = [C.c_void_p]
     lib.p2_tune_enable.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
     lib.p2_tune_count.argtypes = [C.c_void_p]
+    lib.p2_local_taus.argtypes = [C.c_void_p, C.POINTER(P2Prop), C.c_int, C.POINTER(P2Request),
+                                  C.POINTER(C.c_int), C.c_int]
     lib.p2_udsc_datasets.argtypes = [C.POINTER(P2UdscRequest), C.c_char_p, C.c_size_t]
     lib.p2_contract_udsc.argtypes = [C.c_void_p, C.POINTER(P2Prop), C.c_int, C.POINTER(P2UdscRequest)]
     lib.p2_components.argtypes = [C.c_uint]
@@ -246,6 +248,15 @@ class Context:
         pa = (P2Prop * len(props))(*props)
         ra = (P2Request * len(reqs))(*reqs)
         self.check(self.lib.p2_contract_project(self.h, pa, len(props), ra, len(reqs)))
+
+    def local_taus(self, props: Sequence[P2Prop], req: P2Request):
+        """p2_local_taus: source-relative times this rank computes."""
+        pa = (P2Prop * len(props))(*props)
+        buf = (C.c_int * max(self.L[3], 1))()
+        n = self.lib.p2_local_taus(self.h, pa, len(props), C.byref(req), buf, len(buf))
+        if n < 0:
+            raise P2Error(P2_ERR_INVALID_ARG, "p2_local_taus: invalid request")
+        return list(buf[:n])
 
     def contract_position(self, props: Sequence[P2Prop], req: P2Request):
         pa = (P2Prop * len(props))(*props)
