@@ -133,43 +133,44 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
     w.put_slot(a.k.nuc + l, pn[0], 0);
     w.put_slot(a.k.nuc + 16 + l, pn[1], 1);
   }
+  const int g1 = lt.meson_g1();  // the sink Gamma of this lane's meson outputs
   if (a.what & (8u | 16u | 32u)) {
     Cx<R> c[16];
     meson_site(row, kU, kD, lt, l, mask, c);
     if (a.what & 8u) {
 #pragma unroll
-      for (int g2 = 0; g2 < 16; g2++) w.put_slot(a.k.g16 + l * 16 + g2, c[g2], 2 + g2);
+      for (int g2 = 0; g2 < 16; g2++) w.put_slot(a.k.g16 + g1 * 16 + g2, c[g2], 2 + g2);
     }
     if (a.what & 16u) {
-      if (l == 0) w.put(a.k.all34 + 0, c[0]);
-      if (l == 5) w.put(a.k.all34 + 1, c[5]);
-      if (l >= 1 && l <= 4) {
+      if (g1 == 0) w.put(a.k.all34 + 0, c[0]);
+      if (g1 == 5) w.put(a.k.all34 + 1, c[5]);
+      if (g1 >= 1 && g1 <= 4) {
 #pragma unroll
-        for (int g2 = 1; g2 <= 4; g2++) w.put(a.k.all34 + 2 + (l - 1) * 4 + (g2 - 1), c[g2]);
+        for (int g2 = 1; g2 <= 4; g2++) w.put(a.k.all34 + 2 + (g1 - 1) * 4 + (g2 - 1), c[g2]);
       }
-      if (l >= 6 && l <= 9) {
+      if (g1 >= 6 && g1 <= 9) {
 #pragma unroll
-        for (int g2 = 6; g2 <= 9; g2++) w.put(a.k.all34 + 18 + (l - 6) * 4 + (g2 - 6), c[g2]);
+        for (int g2 = 6; g2 <= 9; g2++) w.put(a.k.all34 + 18 + (g1 - 6) * 4 + (g2 - 6), c[g2]);
       }
     }
     if (a.what & 32u) {
-      const int j = diag10_slot(l);
+      const int j = diag10_slot(g1);
 #pragma unroll
       for (int g2 = 0; g2 < 16; g2++)
-        if (g2 == l && j >= 0) w.put(a.k.new10 + j, c[g2]);
+        if (g2 == g1 && j >= 0) w.put(a.k.new10 + j, c[g2]);
     }
   }
   if (a.what & 64u) {
-    const int j = diag10_slot(l);
+    const int j = diag10_slot(g1);
     Cx<R> c[16];
     meson_site(row, kU, kU, lt, l, mask, c);
 #pragma unroll
     for (int g2 = 0; g2 < 16; g2++)
-      if (g2 == l && j >= 0) w.put(a.k.diag10 + j, c[g2]);
+      if (g2 == g1 && j >= 0) w.put(a.k.diag10 + j, c[g2]);
     meson_site(row, kD, kD, lt, l, mask, c);
 #pragma unroll
     for (int g2 = 0; g2 < 16; g2++)
-      if (g2 == l && j >= 0) w.put(a.k.diag10 + 10 + j, c[g2]);
+      if (g2 == g1 && j >= 0) w.put(a.k.diag10 + 10 + j, c[g2]);
   }
 }
 
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
       if (!(tid & 16)) {
         int k = -1;
         if (i < 2 && (a.what & 1u)) k = a.k.nuc + 16 * i + l;
-        if (i >= 2 && (a.what & 8u)) k = a.k.g16 + l * 16 + (i - 2);
+        if (i >= 2 && (a.what & 8u)) k = a.k.g16 + lt.meson_g1() * 16 + (i - 2);
         if (k >= 0) atomicMax(smax_slot(sf, k), __float_as_int(m));
       }
     }

@@ -70,6 +70,23 @@ __device__ __forceinline__ Cx<R> cunit(Cx<R> a, int re, int im) {
   return cx<R>(R(re) * a.x - R(im) * a.y, R(re) * a.y + R(im) * a.x);
 }
 
+// Packed float pairs for the paired FP32 FMA (fma.rn.f32x2): one instruction
+// updates both halves of a register pair.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2pack(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2unpack(f32x2 v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 f2fma(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
 // Index of spin block (mu, nu) in a site's 144 components; colour (a, b) adds a*3 + b.
 __host__ __device__ constexpr int sblk(int mu, int nu) { return (mu * 4 + nu) * 9; }
 

@@ -43,21 +43,21 @@ struct DiquarkLane {
 // Per-lane table entries packed into registers (the tables are indexed by
 // lane, so reading them from constant memory inside the site loop would
 // serialise the half-warp): a diquark lane descriptor as 8 fields of 4 bits
-// (value + 1), and the sink-Gamma stage of the mesons as 4 bytes (source
-// lane, Re + 1, Im + 1 of G_g1[d][pi1(d)] for d = 0..3).
+// (value + 1), and the sink-Gamma stage of the mesons (spin.meson_lane_table):
+// the lane's sink Gamma g1 (4 bits), then Re + 1, Im + 1 of the phases D and
+// r (2 bits each).
 struct LaneTables {
   unsigned nuc;       // nucleon C g5 descriptor
   unsigned delta[3];  // Delta C g_k descriptors, k = 1..3
-  unsigned gam;       // meson stage
+  unsigned mes;       // meson stage
+  __device__ __forceinline__ int meson_g1() const { return (int)(mes & 15u); }
 };
 
-__constant__ int c_gamma_perm[16][4] = P2_INIT_GammaPerm;
-__constant__ int c_gamma_re[16][4] = P2_INIT_GammaRe;
-__constant__ int c_gamma_im[16][4] = P2_INIT_GammaIm;
 __constant__ int c_nuc_sink[4][3] = P2_INIT_NucSink;
 __constant__ int c_nuc_lane[16][8] = P2_INIT_NucLane;
 __constant__ int c_delta_sink[3][4][3] = P2_INIT_DeltaSink;
 __constant__ int c_delta_lane[3][16][8] = P2_INIT_DeltaLane;
+__constant__ int c_meson_lane[16][5] = P2_INIT_MesonLane;
 
 // ---- shared-memory views of one site's two propagators --------------------
 // Spin block b = mu * 4 + nu of flavour f is block 16 f + b; colour (a, b) is
@@ -130,13 +130,9 @@ __device__ __forceinline__ LaneTables load_lane_tables(int l) {
   t.nuc = pack_diquark_lane(c_nuc_lane, l);
 #pragma unroll
   for (int g = 0; g < 3; g++) t.delta[g] = pack_diquark_lane(c_delta_lane[g], l);
-  t.gam = 0;
-#pragma unroll
-  for (int d = 0; d < 4; d++) {
-    const unsigned src = (unsigned)(c_gamma_perm[l][d] * 4 + d);
-    const unsigned re = (unsigned)(c_gamma_re[l][d] + 1), im = (unsigned)(c_gamma_im[l][d] + 1);
-    t.gam |= (src | (re << 4) | (im << 6)) << (8 * d);
-  }
+  t.mes = (unsigned)c_meson_lane[l][0] | ((unsigned)(c_meson_lane[l][1] + 1) << 4) |
+          ((unsigned)(c_meson_lane[l][2] + 1) << 6) | ((unsigned)(c_meson_lane[l][3] + 1) << 8) |
+          ((unsigned)(c_meson_lane[l][4] + 1) << 10);
   return t;
 }
 
@@ -288,14 +284,11 @@ __device__ __forceinline__ void nucleon_site(const Row& row, const LaneTables& l
   out[1] = diquark_eval<true, false>(g, row, kD, dl, l, mask, -1, 0, 0, 0, 1, 0);
 }
 
-// Generic meson block of the lines A and B (block offsets): lane g1 gets
-// C[g1][g2] for g2 = 0..15 in out[].
+// M_{al de}[b][z] = sum over colour of A[al][b] conj(B[de][z]).
 template <typename Row>
-__device__ __forceinline__ void meson_site(const Row& row, int A, int B, const LaneTables& lt, int l, unsigned mask,
-                                           Cx<typename Row::R> out[16]) {
+__device__ __forceinline__ void meson_M(const Row& row, int A, int B, int al, int de,
+                                        Cx<typename Row::R> M[4][4]) {
   typedef typename Row::R R;
-  const int al = l >> 2, de = l & 3;
-  Cx<R> M[4][4];
 #pragma unroll
   for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -316,37 +309,94 @@ __device__ __forceinline__ void meson_site(const Row& row, int A, int B, const L
         cmac_conj(M[b][z], u1[b], d1[z]);
       }
   }
-  {
-    Cx<R> u[4], d[4];
+  Cx<R> u[4], d[4];
 #pragma unroll
-    for (int b = 0; b < 4; b++) u[b] = row.last(A + al * 4 + b);
+  for (int b = 0; b < 4; b++) u[b] = row.last(A + al * 4 + b);
 #pragma unroll
-    for (int z = 0; z < 4; z++) d[z] = row.last(B + de * 4 + z);
+  for (int z = 0; z < 4; z++) d[z] = row.last(B + de * 4 + z);
 #pragma unroll
-    for (int b = 0; b < 4; b++)
+  for (int b = 0; b < 4; b++)
 #pragma unroll
-      for (int z = 0; z < 4; z++) cmac_conj(M[b][z], u[b], d[z]);
+    for (int z = 0; z < 4; z++) cmac_conj(M[b][z], u[b], d[z]);
+}
+
+// FP32 tile: the same sum with paired FMAs on (Re, Im) pairs,
+//   M += (u.x, u.y) * (d.x, d.x) + (u.y, -u.x) * (d.y, d.y),
+// two instructions per complex product instead of four.
+template <>
+__device__ __forceinline__ void meson_M<RowF32>(const RowF32& row, int A, int B, int al, int de, Cx<float> Mo[4][4]) {
+  f32x2 M[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) M[i][j] = f2pack(0.f, 0.f);
+  auto colour = [&](const Cx<float> u[4], const Cx<float> d[4]) {
+    f32x2 u1[4], u2[4];
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      u1[b] = f2pack(u[b].x, u[b].y);
+      u2[b] = f2pack(u[b].y, -u[b].x);
+    }
+#pragma unroll
+    for (int z = 0; z < 4; z++) {
+      const f32x2 dx = f2pack(d[z].x, d[z].x), dy = f2pack(d[z].y, d[z].y);
+#pragma unroll
+      for (int b = 0; b < 4; b++) M[b][z] = f2fma(u2[b], dy, f2fma(u1[b], dx, M[b][z]));
+    }
+  };
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    Cx<float> u0[4], u1[4], d0[4], d1[4];
+#pragma unroll
+    for (int b = 0; b < 4; b++) row.pair(A + al * 4 + b, k, u0[b], u1[b]);
+#pragma unroll
+    for (int z = 0; z < 4; z++) row.pair(B + de * 4 + z, k, d0[z], d1[z]);
+    colour(u0, d0);
+    colour(u1, d1);
   }
+  Cx<float> u[4], d[4];
+#pragma unroll
+  for (int b = 0; b < 4; b++) u[b] = row.last(A + al * 4 + b);
+#pragma unroll
+  for (int z = 0; z < 4; z++) d[z] = row.last(B + de * 4 + z);
+  colour(u, d);
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) f2unpack(M[i][j], Mo[i][j].x, Mo[i][j].y);
+}
+
+// Generic meson block of the lines A and B (block offsets): the lane gets
+// C[g1][g2] for g2 = 0..15 in out[], g1 = lt.meson_g1() (a permutation of the
+// lanes).  Lane (al, de) first forms N_{al de}[g2] = sum_b G2[b][pi2(b)]
+// M[b][pi2(b)]; the sink Gamma C[g1][g2] = sum_d G1[d][pi1(d)] N_{pi1(d) d}[g2]
+// then runs as a Walsh-Hadamard transform over the 4 lanes of the lane's
+// class (spin.meson_lane_table): phase D, two butterflies (xor 5, xor 10),
+// phase r.
+template <typename Row>
+__device__ __forceinline__ void meson_site(const Row& row, int A, int B, const LaneTables& lt, int l, unsigned mask,
+                                           Cx<typename Row::R> out[16]) {
+  typedef typename Row::R R;
+  const int al = l >> 2, de = l & 3;
+  Cx<R> M[4][4];
+  meson_M(row, A, B, al, de, M);
   constexpr int GP[16][4] = P2_INIT_GammaPerm;
   constexpr int GR[16][4] = P2_INIT_GammaRe;
   constexpr int GI[16][4] = P2_INIT_GammaIm;
-  Cx<R> N[16];
+  const int dre = (int)((lt.mes >> 4) & 3u) - 1, dim = (int)((lt.mes >> 6) & 3u) - 1;
+  const int rre = (int)((lt.mes >> 8) & 3u) - 1, rim = (int)((lt.mes >> 10) & 3u) - 1;
+  const R s0 = (de & 1) ? R(-1) : R(1), s1 = (de & 2) ? R(-1) : R(1);
 #pragma unroll
   for (int g2 = 0; g2 < 16; g2++) {
     Cx<R> n = czero<R>();
 #pragma unroll
     for (int b = 0; b < 4; b++) n = n + cunit(M[b][GP[g2][b]], GR[g2][b], GI[g2][b]);
-    N[g2] = n;
-  }
-#pragma unroll
-  for (int g2 = 0; g2 < 16; g2++) {
-    Cx<R> c = czero<R>();
-#pragma unroll
-    for (int d = 0; d < 4; d++) {
-      const unsigned e = lt.gam >> (8 * d);
-      c = c + cunit(shfl_idx16(N[g2], (int)(e & 15u), mask), (int)((e >> 4) & 3u) - 1, (int)((e >> 6) & 3u) - 1);
-    }
-    out[g2] = c;
+    Cx<R> x = cunit(n, dre, dim);
+    Cx<R> p = shfl_xor16(x, 5, mask);
+    x = cx<R>(fma(s0, x.x, p.x), fma(s0, x.y, p.y));
+    p = shfl_xor16(x, 10, mask);
+    x = cx<R>(fma(s1, x.x, p.x), fma(s1, x.y, p.y));
+    out[g2] = cunit(x, rre, rim);
   }
 }
 
