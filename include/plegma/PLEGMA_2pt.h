@@ -354,7 +354,8 @@ class PLEGMA_Correlator {
       size_t off = 0;
       for (int b = 0; b < nb; b++) {
         const p2_block& B = blocks[b];
-        const bool baryon = B.bit == P2_NUCLEON_CG5 || B.bit == P2_DELTA_ISO12 || B.bit == P2_DELTA_ISO32;
+        const bool baryon = B.bit == P2_NUCLEON_CG5 || B.bit == P2_NUCLEON_NTOR || B.bit == P2_NUCLEON_RTON ||
+                            B.bit == P2_NUCLEON_RTOR || B.bit == P2_DELTA_ISO12 || B.bit == P2_DELTA_ISO32;
         for (int gd = 0; gd < B.groups * B.datasets; gd++)
           for (int i = 0; i < lt; i++) {
             const int tau = (i + startT()) % totalT;
@@ -492,16 +493,19 @@ class PLEGMA_Correlator {
   }
   // lib/PLEGMA_Correlator.cu:117-135: nucleon C g5 (proton, neutron); with
   // deltas, the Delta C g_k groups of the light-baryon build after it.
-  void contractBaryons(PLEGMA_Propagator<Float>& p1, PLEGMA_Propagator<Float>& p2, bool deltas = false) {
+  // lib/PLEGMA_Correlator.cu:117-135; light_build = the reference built with
+  // PLEGMA_LIGHT_BARYONS: the second nucleon interpolator and the Deltas too.
+  void contractBaryons(PLEGMA_Propagator<Float>& p1, PLEGMA_Propagator<Float>& p2, bool light_build = false) {
     shape = {16};
     datasets = {"twop_baryon_1", "twop_baryon_2"};
     groups = {"baryons/nucl_nucl"};
     unsigned what = P2_NUCLEON_CG5;
-    if (deltas) {
-      for (const char* g : {"baryons/deltap_deltaz_11", "baryons/deltap_deltaz_22", "baryons/deltap_deltaz_33",
+    if (light_build) {
+      for (const char* g : {"baryons/nucl_nucl2", "baryons/nucl2_nucl", "baryons/nucl2_nucl2",
+                            "baryons/deltap_deltaz_11", "baryons/deltap_deltaz_22", "baryons/deltap_deltaz_33",
                             "baryons/deltapp_deltamm_11", "baryons/deltapp_deltamm_22", "baryons/deltapp_deltamm_33"})
         groups.push_back(g);
-      what |= P2_DELTA_ISO12 | P2_DELTA_ISO32;
+      what |= P2_NUCLEON_NTOR | P2_NUCLEON_RTON | P2_NUCLEON_RTOR | P2_DELTA_ISO12 | P2_DELTA_ISO32;
     }
     description = "1,g1,g2,g3,g4,g5,g5g1,g5g2,g5g3,g5g4,s12,s13,s23,s41,s42,s43";
     run(p1, p2, what, false);

@@ -57,10 +57,14 @@ typedef enum { P2_PLAIN_FP64 = 0, P2_SPLIT_FP16 = 1 } p2_mode;
 
 typedef enum { P2_DEVICE = 0, P2_HOST = 1 } p2_location;
 
-/* Contraction blocks (bit order = order in the result).
+/* Contraction blocks, in their order in the result.
  *   groups x datasets x components per site                     reference
  *   NUCLEON_CG5   1 x 2 x 16  nucl_nucl: proton (u,u,d), neutron   PLEGMA_baryons_NtoN.cu:6-46
  *                 16 = (mu, mu') open spin, mu*4 + mu'
+ *   NUCLEON_NTOR  1 x 2 x 16  nucl_nucl2: N = eps (u C g5 d) u at  PLEGMA_baryons_NtoR.cu:6-52
+ *                 the sink, R = eps (u C d) g5 u at the source
+ *   NUCLEON_RTON  1 x 2 x 16  nucl2_nucl                           PLEGMA_baryons_RtoN.cu:6-52
+ *   NUCLEON_RTOR  1 x 2 x 16  nucl2_nucl2                          PLEGMA_baryons_RtoR.cu:6-46
  *   DELTA_ISO12   3 x 2 x 16  deltap_deltaz_kk, k = 1..3          PLEGMA_baryons_deltas.cu:7-59
  *   DELTA_ISO32   3 x 2 x 16  deltapp_deltamm_kk, k = 1..3        PLEGMA_baryons_deltas.cu:62-110
  *   MESON_G16     1 x 1 x 256 all (G_sink, G_src) pairs of the 16 PLEGMA_mesonsAll.cuh:52-76
@@ -76,7 +80,10 @@ enum {
   P2_MESON_G16 = 1u << 3,
   P2_MESON_ALL34 = 1u << 4,
   P2_MESON_NEW10 = 1u << 5,
-  P2_MESON_DIAG10 = 1u << 6
+  P2_MESON_DIAG10 = 1u << 6,
+  P2_NUCLEON_NTOR = 1u << 7,
+  P2_NUCLEON_RTON = 1u << 8,
+  P2_NUCLEON_RTOR = 1u << 9
 };
 
 typedef struct p2_ctx p2_ctx;

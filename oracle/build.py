@@ -44,7 +44,8 @@ def build_ref(ref_root=DEFAULT_REF, force=False):
     (read in place, never copied) with the small type shim in ref_shim/.
     Returns the library path, or None when the sources are not present."""
     kern = os.path.join(ref_root, "lib", "kernels")
-    srcs = [os.path.join(kern, "PLEGMA_baryons_NtoN.cu"), os.path.join(kern, "PLEGMA_baryons_deltas.cu")]
+    srcs = [os.path.join(kern, f) for f in ("PLEGMA_baryons_NtoN.cu", "PLEGMA_baryons_NtoR.cu", "PLEGMA_baryons_RtoN.cu",
+                                           "PLEGMA_baryons_RtoR.cu", "PLEGMA_baryons_deltas.cu")]
     if not all(os.path.exists(s) for s in srcs):
         return None
     os.makedirs(REF_OUT, exist_ok=True)

@@ -7,7 +7,8 @@
 //
 // Every loop follows the reference literally (same index order, same
 // unfactorised sums), so this is a slow but faithful transcription:
-//   nucleon      lib/kernels/PLEGMA_baryons_NtoN.cu:6-46
+//   nucleon      lib/kernels/PLEGMA_baryons_NtoN.cu:6-46, second interpolator
+//                PLEGMA_baryons_NtoR.cu, _RtoN.cu, _RtoR.cu
 //   Delta        lib/kernels/PLEGMA_baryons_deltas.cu:7-110
 //   mesons       lib/kernels/PLEGMA_mesonsAll.cuh:34-82 (generic G1 S1 G2 S2^dag),
 //                PLEGMA_mesons.cuh:29-53, PLEGMA_mesonsNew.cuh:27-45
@@ -46,6 +47,9 @@ enum : unsigned {
   MESON_ALL34 = 1u << 4,
   MESON_NEW10 = 1u << 5,
   MESON_DIAG10 = 1u << 6,
+  NUCLEON_NTOR = 1u << 7,
+  NUCLEON_RTON = 1u << 8,
+  NUCLEON_RTOR = 1u << 9,
 };
 
 // Diagonal structures of contractMesons / contractMesonsNew, in output order.
@@ -54,6 +58,9 @@ constexpr int kMeson10[10] = {0, 5, 1, 2, 3, 4, 6, 7, 8, 9};
 int components(unsigned what) {
   int k = 0;
   if (what & NUCLEON_CG5) k += 32;
+  if (what & NUCLEON_NTOR) k += 32;
+  if (what & NUCLEON_RTON) k += 32;
+  if (what & NUCLEON_RTOR) k += 32;
   if (what & DELTA_ISO12) k += 96;
   if (what & DELTA_ISO32) k += 96;
   if (what & MESON_G16) k += 256;
@@ -171,11 +178,96 @@ void delta_iso32(const Prop& P1, const Prop& P2, int g, cplx* out) {
     }
 }
 
+// Second nucleon interpolator R = eps (u C d) g5 u against N and itself,
+// out[(ds*4+mu)*4+mup]:
+//   NtoR  lib/kernels/PLEGMA_baryons_NtoR.cu:6-52
+//   RtoN  lib/kernels/PLEGMA_baryons_RtoN.cu:6-52
+//   RtoR  lib/kernels/PLEGMA_baryons_RtoR.cu:6-46
+// The index tables are the reference's (generated by plegma_b200/spin.py).
+void nucleon_ntor(const Prop& p1, const Prop& p2, cplx* out) {
+  for (int mu = 0; mu < 4; mu++) {
+    cplx tmp[8] = {};
+    for (int idx = 0; idx < 64; idx++) {
+      const int* m = p2::kNtrIdx[idx];
+      const int nu = m[0], lu = m[1], lup = m[2], nup = m[3], mup = m[4], rho = m[5];
+      for (int cc1 = 0; cc1 < 6; cc1++) {
+        int a = p2::kEps[cc1][0], b = p2::kEps[cc1][1], c = p2::kEps[cc1][2];
+        for (int cc2 = 0; cc2 < 6; cc2++) {
+          int a1 = p2::kEps[cc2][0], b1 = p2::kEps[cc2][1], c1 = p2::kEps[cc2][2];
+          double f = (double)(p2::kEpsSign[cc1] * p2::kEpsSign[cc2] * p2::kNtrVal[idx]);
+          tmp[mup] = tmp[mup] - f * p2[lu][lup][b][b1] *
+                                    (p1[nu][nup][a][a1] * p1[mu][rho][c][c1] - p1[nu][rho][a][c1] * p1[mu][nup][c][a1]);
+          tmp[4 + mup] = tmp[4 + mup] - f * p1[lu][lup][b][b1] *
+                                            (p2[nu][nup][a][a1] * p2[mu][rho][c][c1] - p2[nu][rho][a][c1] * p2[mu][nup][c][a1]);
+        }
+      }
+    }
+    for (int i = 0; i < 2; i++)
+      for (int mup = 0; mup < 4; mup++) out[(i * 4 + mu) * 4 + mup] = tmp[i * 4 + mup];
+  }
+}
+
+void nucleon_rton(const Prop& p1, const Prop& p2, cplx* out) {
+  for (int mup = 0; mup < 4; mup++) {
+    cplx tmp[8] = {};
+    for (int idx = 0; idx < 64; idx++) {
+      const int* m = p2::kRtnIdx[idx];
+      const int nu = m[0], lu = m[1], lup = m[2], nup = m[3], mu = m[4], rho = m[5];
+      for (int cc1 = 0; cc1 < 6; cc1++) {
+        int a = p2::kEps[cc1][0], b = p2::kEps[cc1][1], c = p2::kEps[cc1][2];
+        for (int cc2 = 0; cc2 < 6; cc2++) {
+          int a1 = p2::kEps[cc2][0], b1 = p2::kEps[cc2][1], c1 = p2::kEps[cc2][2];
+          double f = (double)(p2::kEpsSign[cc1] * p2::kEpsSign[cc2] * p2::kRtnVal[idx]);
+          tmp[mu] = tmp[mu] + f * p2[lu][lup][b][b1] *
+                                  (p1[nu][nup][a][a1] * p1[rho][mup][c][c1] - p1[nu][mup][a][c1] * p1[rho][nup][c][a1]);
+          tmp[4 + mu] = tmp[4 + mu] + f * p1[lu][lup][b][b1] *
+                                          (p2[nu][nup][a][a1] * p2[rho][mup][c][c1] - p2[nu][mup][a][c1] * p2[rho][nup][c][a1]);
+        }
+      }
+    }
+    for (int i = 0; i < 2; i++)
+      for (int mu = 0; mu < 4; mu++) out[(i * 4 + mu) * 4 + mup] = tmp[i * 4 + mu];
+  }
+}
+
+void nucleon_rtor(const Prop& p1, const Prop& p2, cplx* out) {
+  for (int i = 0; i < 32; i++) out[i] = {0, 0};
+  for (int idx = 0; idx < 256; idx++) {
+    const int* m = p2::kRtrIdx[idx];
+    const int nu = m[0], lu = m[1], lup = m[2], nup = m[3], mu = m[4], rho = m[5], mup = m[6], rhop = m[7];
+    for (int cc1 = 0; cc1 < 6; cc1++) {
+      int a = p2::kEps[cc1][0], b = p2::kEps[cc1][1], c = p2::kEps[cc1][2];
+      for (int cc2 = 0; cc2 < 6; cc2++) {
+        int a1 = p2::kEps[cc2][0], b1 = p2::kEps[cc2][1], c1 = p2::kEps[cc2][2];
+        double f = (double)(p2::kEpsSign[cc1] * p2::kEpsSign[cc2] * p2::kRtrVal[idx]);
+        out[mu * 4 + mup] = out[mu * 4 + mup] - f * p2[lu][lup][b][b1] *
+                                                    (p1[nu][nup][a][a1] * p1[rho][rhop][c][c1] -
+                                                     p1[nu][rhop][a][c1] * p1[rho][nup][c][a1]);
+        out[(4 + mu) * 4 + mup] = out[(4 + mu) * 4 + mup] - f * p1[lu][lup][b][b1] *
+                                                                (p2[nu][nup][a][a1] * p2[rho][rhop][c][c1] -
+                                                                 p2[nu][rhop][a][c1] * p2[rho][nup][c][a1]);
+      }
+    }
+  }
+}
+
 // All requested components of one site, in block order.
 void site_components(const Prop& u, const Prop& d, unsigned what, cplx* c) {
   int k = 0;
   if (what & NUCLEON_CG5) {
     nucleon(u, d, c + k);
+    k += 32;
+  }
+  if (what & NUCLEON_NTOR) {
+    nucleon_ntor(u, d, c + k);
+    k += 32;
+  }
+  if (what & NUCLEON_RTON) {
+    nucleon_rton(u, d, c + k);
+    k += 32;
+  }
+  if (what & NUCLEON_RTOR) {
+    nucleon_rtor(u, d, c + k);
     k += 32;
   }
   if (what & DELTA_ISO12) {

@@ -52,6 +52,7 @@ def reference():
         lib = C.CDLL(REF_LIB)
         lib.ref_nucleon.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         lib.ref_delta.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        lib.ref_light.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         _ref = lib
     return _ref
 
@@ -130,6 +131,16 @@ def ref_nucleon(u1, d1):
     u1 = np.ascontiguousarray(u1, dtype=np.complex128)
     d1 = np.ascontiguousarray(d1, dtype=np.complex128)
     lib.ref_nucleon(u1.ctypes.data, d1.ctypes.data, out.ctypes.data)
+    return out
+
+
+def ref_light(u1, d1, which):
+    """The reference's NtoR (0), RtoN (1), RtoR (2) on one site: [2][4][4]."""
+    lib = reference()
+    out = np.zeros(32, dtype=np.complex128)
+    u1 = np.ascontiguousarray(u1, dtype=np.complex128)
+    d1 = np.ascontiguousarray(d1, dtype=np.complex128)
+    lib.ref_light(u1.ctypes.data, d1.ctypes.data, int(which), out.ctypes.data)
     return out
 
 

@@ -1,11 +1,18 @@
 // C entry points over the reference's own nucleon and Delta contraction
-// functions (lib/kernels/PLEGMA_baryons_NtoN.cu, PLEGMA_baryons_deltas.cu),
+// functions (lib/kernels/PLEGMA_baryons_NtoN.cu, _NtoR.cu, _RtoN.cu, _RtoR.cu,
+// PLEGMA_baryons_deltas.cu),
 // compiled from the reference sources as host code by oracle/build.py.
 // TEST INFRASTRUCTURE ONLY: used by tests/ to pin the oracle.
 #include "ref_shim/PLEGMA_kernel_utils.cuh"
 
 template <typename FloatA, typename FloatB, typename FloatC>
 void contract_NtoN_kernel(propTex<FloatA>&, propTex<FloatB>&, Float2<FloatC>*, int);
+template <typename FloatA, typename FloatB, typename FloatC>
+void contract_NtoR_kernel(propTex<FloatA>&, propTex<FloatB>&, Float2<FloatC>*, int);
+template <typename FloatA, typename FloatB, typename FloatC>
+void contract_RtoN_kernel(propTex<FloatA>&, propTex<FloatB>&, Float2<FloatC>*, int);
+template <typename FloatA, typename FloatB, typename FloatC>
+void contract_RtoR_kernel(propTex<FloatA>&, propTex<FloatB>&, Float2<FloatC>*, int);
 template <typename FloatA, typename FloatB, typename FloatC, int gamma>
 void contract_deltas_iso1o2_kernel(propTex<FloatA>&, propTex<FloatB>&, Float2<FloatC>*, int);
 template <typename FloatA, typename FloatB, typename FloatC, int gamma>
@@ -26,6 +33,17 @@ void ref_nucleon(const double* u, const double* d, double* out) {
   propTex<double> t1(u), t2(d);
   Float2<double> acc[32];
   contract_NtoN_kernel<double, double, double>(t1, t2, acc, 0);
+  copy_out(acc, 32, out);
+}
+
+// which: 0 NtoR, 1 RtoN, 2 RtoR; out: 32 complex ([2][4][4]).
+void ref_light(const double* u, const double* d, int which, double* out) {
+  propTex<double> t1(u), t2(d);
+  Float2<double> acc[32];
+  for (int i = 0; i < 32; i++) acc[i] = Float2<double>(0., 0.);
+  if (which == 0) contract_NtoR_kernel<double, double, double>(t1, t2, acc, 0);
+  if (which == 1) contract_RtoN_kernel<double, double, double>(t1, t2, acc, 0);
+  if (which == 2) contract_RtoR_kernel<double, double, double>(t1, t2, acc, 0);
   copy_out(acc, 32, out);
 }
 

@@ -25,10 +25,11 @@ int components_of(unsigned what) {
 }
 
 p2::CompOffsets offsets_of(unsigned what) {
-  p2::CompOffsets o{-1, -1, -1, -1, -1, -1, -1};
+  p2::CompOffsets o{-1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
   int k = 0;
-  int* slot[] = {&o.nuc, &o.diso12, &o.diso32, &o.g16, &o.all34, &o.new10, &o.diag10};
-  for (int i = 0; i < 7; i++)
+  int* slot[] = {&o.nuc, &o.ntor, &o.rton, &o.rtor, &o.diso12, &o.diso32, &o.g16, &o.all34, &o.new10, &o.diag10};
+  static_assert(sizeof(slot) / sizeof(slot[0]) == sizeof(kBlocks) / sizeof(kBlocks[0]), "one offset per block");
+  for (int i = 0; i < 10; i++)
     if (what & kBlocks[i].bit) {
       *slot[i] = k;
       k += kBlocks[i].groups * kBlocks[i].datasets * kBlocks[i].comps;

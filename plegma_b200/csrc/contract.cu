@@ -104,15 +104,21 @@ struct Writer {
   }
 };
 
-// DELTA selects the instantiation: the Delta blocks only (true) or every other
-// block (false); a request with both runs the two instantiations over the same
-// tiles (the Delta part is ~5x the rest in arithmetic, so the second pass over
-// the propagators is hidden under its compute).
+// DELTA selects the instantiation: the Delta blocks and the second nucleon
+// interpolator (true) or every other block (false); a request with both runs
+// the two instantiations over the same tiles (the Delta part is ~5x the rest
+// in arithmetic, so the second pass over the propagators is hidden under its
+// compute).
 template <bool DELTA, typename Row>
 __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& row, const LaneTables& lt, int l,
                                               unsigned mask, const Writer<typename Row::R>& w) {
   typedef typename Row::R R;
-  if (DELTA) {
+  if (DELTA && (a.what & (128u | 256u | 512u))) {
+    const int base[3] = {a.k.ntor, a.k.rton, a.k.rtor};
+    light_nucleon_site(row, lt, l, mask, (a.what & 128u) != 0, (a.what & 256u) != 0, (a.what & 512u) != 0,
+                       [&](int j, int ds, Cx<R> v) { w.put(base[j] + 16 * ds + l, v); });
+  }
+  if (DELTA && (a.what & (2u | 4u))) {
     // group g of each isospin block, datasets (u-rich, d-rich)
     // the iso-1/2 partial sums are parked in the iso-1/2 output slots when
     // those are requested, else in the iso-3/2 slots that are written later
@@ -125,8 +131,8 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
         },
         [&](int g, int j, Cx<R> v) { w.out[(long long)(park + (g * 2 + j) * 16 + l) * w.V3] = v; },
         [&](int g, int j) { return w.out[(long long)(park + (g * 2 + j) * 16 + l) * w.V3]; });
-    return;
   }
+  if (DELTA) return;
   if (a.what & 1u) {
     Cx<R> pn[2];
     nucleon_site(row, lt, l, mask, pn);
@@ -371,7 +377,8 @@ cudaError_t launch_f32_t(const ContractArgs& a, int grid, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-constexpr unsigned kDeltaBits = 2u | 4u;
+// the second instantiation: Delta and the second nucleon interpolator
+constexpr unsigned kDeltaBits = 2u | 4u | 128u | 256u | 512u;
 
 cudaError_t launch_contract_plain(const ContractArgs& a, int grid, cudaStream_t s) {
   cudaError_t e = cudaSuccess;

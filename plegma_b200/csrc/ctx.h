@@ -35,11 +35,12 @@ struct BlockDef {
   int groups, datasets, comps;
 };
 constexpr BlockDef kBlocks[] = {
-    {P2_NUCLEON_CG5, 1, 2, 16},  {P2_DELTA_ISO12, 3, 2, 16}, {P2_DELTA_ISO32, 3, 2, 16},
+    {P2_NUCLEON_CG5, 1, 2, 16},  {P2_NUCLEON_NTOR, 1, 2, 16}, {P2_NUCLEON_RTON, 1, 2, 16},
+    {P2_NUCLEON_RTOR, 1, 2, 16}, {P2_DELTA_ISO12, 3, 2, 16},  {P2_DELTA_ISO32, 3, 2, 16},
     {P2_MESON_G16, 1, 1, 256},   {P2_MESON_ALL34, 1, 1, 34}, {P2_MESON_NEW10, 1, 1, 10},
     {P2_MESON_DIAG10, 1, 2, 10},
 };
-constexpr unsigned kAllBits = 0x7Fu;
+constexpr unsigned kAllBits = 0x3FFu;
 
 }  // namespace p2host
 

@@ -10,7 +10,7 @@ constexpr int kMaxBlocks = 8;
 
 // Where each contraction block's components sit inside the K components of a site.
 struct CompOffsets {
-  int nuc, diso12, diso32, g16, all34, new10, diag10;
+  int nuc, ntor, rton, rtor, diso12, diso32, g16, all34, new10, diag10;
 };
 
 // One time slice of one request, as the kernels see it.  A launch covers an

@@ -30,10 +30,12 @@ std::vector<int> component_exponents(unsigned what) {
       e.push_back(nd);
     }
   };
-  if (what & P2_NUCLEON_CG5) {
-    push(16, 2, 1);  // proton: u u d
-    push(16, 1, 2);  // neutron: d d u
-  }
+  for (unsigned bit : {(unsigned)P2_NUCLEON_CG5, (unsigned)P2_NUCLEON_NTOR, (unsigned)P2_NUCLEON_RTON,
+                       (unsigned)P2_NUCLEON_RTOR})
+    if (what & bit) {
+      push(16, 2, 1);  // proton: u u d
+      push(16, 1, 2);  // neutron: d d u
+    }
   if (what & P2_DELTA_ISO12)
     for (int g = 0; g < 3; g++) {
       push(16, 2, 1);

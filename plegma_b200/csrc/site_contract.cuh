@@ -49,6 +49,8 @@ struct DiquarkLane {
 struct LaneTables {
   unsigned nuc;       // nucleon C g5 descriptor
   unsigned delta[3];  // Delta C g_k descriptors, k = 1..3
+  unsigned light[3];  // NtoR, RtoN, RtoR descriptors (spin.light_lane_tables)
+  unsigned lg5;       // their g5 signs, 2 bits each (value + 1)
   unsigned mes;       // meson stage
   __device__ __forceinline__ int meson_g1() const { return (int)(mes & 15u); }
 };
@@ -58,6 +60,9 @@ __constant__ int c_nuc_lane[16][8] = P2_INIT_NucLane;
 __constant__ int c_delta_sink[3][4][3] = P2_INIT_DeltaSink;
 __constant__ int c_delta_lane[3][16][8] = P2_INIT_DeltaLane;
 __constant__ int c_meson_lane[16][5] = P2_INIT_MesonLane;
+__constant__ int c_c_sink[4][3] = P2_INIT_CSink;
+__constant__ int c_light_lane[3][16][8] = P2_INIT_LightLane;
+__constant__ int c_light_g5[16][3] = P2_INIT_LightG5;
 
 // ---- shared-memory views of one site's two propagators --------------------
 // Spin block b = mu * 4 + nu of flavour f is block 16 f + b; colour (a, b) is
@@ -130,6 +135,10 @@ __device__ __forceinline__ LaneTables load_lane_tables(int l) {
   t.nuc = pack_diquark_lane(c_nuc_lane, l);
 #pragma unroll
   for (int g = 0; g < 3; g++) t.delta[g] = pack_diquark_lane(c_delta_lane[g], l);
+#pragma unroll
+  for (int j = 0; j < 3; j++) t.light[j] = pack_diquark_lane(c_light_lane[j], l);
+  t.lg5 = (unsigned)(c_light_g5[l][0] + 1) | ((unsigned)(c_light_g5[l][1] + 1) << 2) |
+          ((unsigned)(c_light_g5[l][2] + 1) << 4);
   t.mes = (unsigned)c_meson_lane[l][0] | ((unsigned)(c_meson_lane[l][1] + 1) << 4) |
           ((unsigned)(c_meson_lane[l][2] + 1) << 6) | ((unsigned)(c_meson_lane[l][3] + 1) << 8) |
           ((unsigned)(c_meson_lane[l][4] + 1) << 10);
@@ -484,6 +493,53 @@ __device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt,
       iso32 = iso32 + diquark_typea(D, row, X, l);
       out(g, pair, part_get(g, pair) + cscale(iso12, third));
       out(g, 2 + pair, iso32);
+    }
+  }
+}
+
+// ---- second nucleon interpolator (PLEGMA_baryons_NtoR.cu, _RtoN.cu, _RtoR.cu) ----
+// N = eps (u^T C g5 d) u, R = eps (u^T C d) g5 u.  Each variant is the nucleon's
+// Wick structure with the sink diquark of its sink interpolator (G^{ud} for
+// C g5 or C), the source descriptors of its (sink, source) table, and a g5
+// on the open spin of the third quark, which moves values between lanes:
+// lane (mu, mu') takes T_NR from lane (mu, mu' ^ 2) (xor 2), T_RN from
+// (mu ^ 2, mu') (xor 8), T_RR from (mu ^ 2, mu' ^ 2) (xor 10), with the signs
+// of spin.light_lane_tables.  out(j, ds, v): j = 0 NtoR, 1 RtoN, 2 RtoR;
+// ds 0 = proton (u u d), 1 = neutron (d d u).
+template <typename Row, typename Out>
+__device__ __forceinline__ void light_nucleon_site(const Row& row, const LaneTables& lt, int l, unsigned mask,
+                                                   bool ntor, bool rton, bool rtor, Out&& out) {
+  typedef typename Row::R R;
+  constexpr int kCT[1] = P2_INIT_CTransposeSign;
+  const R s_nr = R((int)(lt.lg5 & 3u) - 1), s_rn = R((int)((lt.lg5 >> 2) & 3u) - 1);
+  const R s_rr = R((int)((lt.lg5 >> 4) & 3u) - 1);
+  if (ntor) {
+    Cx<R> g[9];
+    diquark_G(row, kU, kD, c_nuc_sink, l >> 2, l & 3, g);  // sink C g5
+    const DiquarkLane dl = unpack_diquark_lane(lt.light[0]);
+    const Cx<R> p = diquark_eval<true, false>(g, row, kU, dl, l, mask, -1, 0, 0, 0, 1, 0);
+    diquark_transpose<R>(g, l, mask, R(-1));
+    const Cx<R> n = diquark_eval<true, false>(g, row, kD, dl, l, mask, -1, 0, 0, 0, 1, 0);
+    out(0, 0, cscale(shfl_xor16(p, 2, mask), s_nr));
+    out(0, 1, cscale(shfl_xor16(n, 2, mask), s_nr));
+  }
+  if (rton || rtor) {
+    Cx<R> g[9];
+    diquark_G(row, kU, kD, c_c_sink, l >> 2, l & 3, g);  // sink C
+    const DiquarkLane drn = unpack_diquark_lane(lt.light[1]), drr = unpack_diquark_lane(lt.light[2]);
+    Cx<R> prn = czero<R>(), prr = czero<R>();
+    if (rton) prn = diquark_eval<true, false>(g, row, kU, drn, l, mask, -1, 0, 0, 0, 1, 0);
+    if (rtor) prr = diquark_eval<true, false>(g, row, kU, drr, l, mask, -1, 0, 0, 0, 1, 0);
+    diquark_transpose<R>(g, l, mask, R(kCT[0]));
+    if (rton) {
+      const Cx<R> n = diquark_eval<true, false>(g, row, kD, drn, l, mask, -1, 0, 0, 0, 1, 0);
+      out(1, 0, cscale(shfl_xor16(prn, 8, mask), s_rn));
+      out(1, 1, cscale(shfl_xor16(n, 8, mask), s_rn));
+    }
+    if (rtor) {
+      const Cx<R> n = diquark_eval<true, false>(g, row, kD, drr, l, mask, -1, 0, 0, 0, 1, 0);
+      out(2, 0, cscale(shfl_xor16(prr, 10, mask), s_rr));
+      out(2, 1, cscale(shfl_xor16(n, 10, mask), s_rr));
     }
   }
 }

@@ -28,11 +28,17 @@ MESON_G16 = 1 << 3
 MESON_ALL34 = 1 << 4
 MESON_NEW10 = 1 << 5
 MESON_DIAG10 = 1 << 6
+NUCLEON_NTOR = 1 << 7
+NUCLEON_RTON = 1 << 8
+NUCLEON_RTOR = 1 << 9
 
 #: (bit, groups, datasets, comps, group names, dataset names), the reference's names
 #: (lib/PLEGMA_Correlator.cu:43-135).
 BLOCKS = [
     (NUCLEON_CG5, 1, 2, 16, ["baryons/nucl_nucl"], ["twop_baryon_1", "twop_baryon_2"]),
+    (NUCLEON_NTOR, 1, 2, 16, ["baryons/nucl_nucl2"], ["twop_baryon_1", "twop_baryon_2"]),
+    (NUCLEON_RTON, 1, 2, 16, ["baryons/nucl2_nucl"], ["twop_baryon_1", "twop_baryon_2"]),
+    (NUCLEON_RTOR, 1, 2, 16, ["baryons/nucl2_nucl2"], ["twop_baryon_1", "twop_baryon_2"]),
     (DELTA_ISO12, 3, 2, 16, ["baryons/deltap_deltaz_11", "baryons/deltap_deltaz_22", "baryons/deltap_deltaz_33"],
      ["twop_baryon_1", "twop_baryon_2"]),
     (DELTA_ISO32, 3, 2, 16, ["baryons/deltapp_deltamm_11", "baryons/deltapp_deltamm_22",

@@ -131,6 +131,83 @@ def nucleon_table():
     return diquark_table(CG5)
 
 
+def mixed_diquark_table(ga: np.ndarray, gb: np.ndarray):
+    """As diquark_table with G_A at the sink and G_B at the source:
+    entries (nu, lambda, lambda', nu', G_A[nu][lambda] G_B-bar[lambda'][nu'])."""
+    gbb = bar(gb)
+    rows = []
+    for nu, lu in itertools.product(range(NS), range(NS)):
+        if abs(ga[nu, lu]) < 1e-12:
+            continue
+        for lup, nup in itertools.product(range(NS), range(NS)):
+            if abs(gbb[lup, nup]) < 1e-12:
+                continue
+            v = ga[nu, lu] * gbb[lup, nup]
+            if abs(v.imag) > 1e-12:
+                raise ValueError("complex diquark weight")
+            rows.append((nu, lu, lup, nup, int(round(v.real))))
+    return rows
+
+
+# Second nucleon interpolator of the reference's light-baryon build:
+#   N = eps_abc (u_a^T C g5 d_b) u_c,   R = eps_abc (u_a^T C d_b) g5 u_c.
+# NtoR, RtoN, RtoR (lib/kernels/PLEGMA_baryons_NtoR.cu, _RtoN.cu, _RtoR.cu)
+# are nucleon-type contractions with G_A / G_B = C g5 or C and a g5 on the open
+# spin of the third quark at the sink (R at the sink) and/or the source (R at
+# the source).  Their tables, in the reference's column order:
+#   NtoR (nu, lambda, lambda', nu', mu', rho): w_AB * g5[rho][mu']
+#   RtoN (nu, lambda, lambda', nu', mu, rho):  w_AB * g5[mu][rho]
+#   RtoR (nu, lambda, lambda', nu', mu, rho, mu', rho'): w_AB g5[mu][rho] g5[rho'][mu']
+def _g5_pairs(transposed: bool):
+    out = []
+    for a in range(NS):
+        for b in range(NS):
+            v = G5[b, a] if transposed else G5[a, b]
+            if abs(v) > 1e-12:
+                out.append((a, b, int(round(v.real))))
+    return out
+
+
+def light_nucleon_tables():
+    """{'NtoR': rows, 'RtoN': rows, 'RtoR': rows}, each row the index columns + value."""
+    out = {}
+    for name, ga, gb in (("NtoR", CG5, CMAT), ("RtoN", CMAT, CG5), ("RtoR", CMAT, CMAT)):
+        rows = []
+        for nu, lu, lup, nup, w in mixed_diquark_table(ga, gb):
+            if name == "NtoR":
+                for mup, rho, g in _g5_pairs(True):
+                    rows.append((nu, lu, lup, nup, mup, rho, w * g))
+            elif name == "RtoN":
+                for mu, rho, g in _g5_pairs(False):
+                    rows.append((nu, lu, lup, nup, mu, rho, w * g))
+            else:
+                for mu, rho, g1 in _g5_pairs(False):
+                    for mup, rhop, g2 in _g5_pairs(True):
+                        rows.append((nu, lu, lup, nup, mu, rho, mup, rhop, w * g1 * g2))
+        out[name] = rows
+    return out
+
+
+def light_lane_tables():
+    """Lane-parallel form of NtoR, RtoN, RtoR: (sink table of C, lane descriptors
+    of the (C g5, C), (C, C g5), (C, C) diquark tables, and per lane the g5
+    shuffles): lane (mu, mu') takes T_NR from lane (mu, mu' ^ 2), T_RN from
+    (mu ^ 2, mu'), T_RR from (mu ^ 2, mu' ^ 2), with the signs
+    -g5[mu'^2][mu'], +g5[mu][mu^2], -g5[mu][mu^2] g5[mu'^2][mu'] (the explicit
+    signs of the reference's loops)."""
+    sink_c = diquark_lane_tables(diquark_table(CMAT))[0]
+    lanes = [diquark_lane_tables(mixed_diquark_table(a, b))[1] for a, b in ((CG5, CMAT), (CMAT, CG5), (CMAT, CMAT))]
+    signs = []
+    for l in range(16):
+        mu, mup = l >> 2, l & 3
+        assert abs(G5[mup ^ 2, mup]) > 0 and abs(G5[mu, mu ^ 2]) > 0
+        s_nr = -int(round(G5[mup ^ 2, mup].real))
+        s_rn = int(round(G5[mu, mu ^ 2].real))
+        s_rr = -int(round((G5[mu, mu ^ 2] * G5[mup ^ 2, mup]).real))
+        signs.append((s_nr, s_rn, s_rr))
+    return sink_c, lanes, signs
+
+
 def transpose_sign(gamma: np.ndarray) -> int:
     """G^{YX} on lane (y', x') equals sign * G^{XY} on lane (x', y'): -1 for an
     antisymmetric diquark matrix (C g5), +1 for a symmetric one (C g_k)."""
@@ -296,6 +373,16 @@ def header_text() -> str:
            _c_array("kDeltaSink", "int", [diquark_lane_tables(t)[0] for t in dl]),
            _c_array("kDeltaLane", "int", [diquark_lane_tables(t)[1] for t in dl]),
            _c_array("kMesonLane", "int", meson_lane_table()),
+           _c_array("kNtrIdx", "int", [r[:6] for r in light_nucleon_tables()["NtoR"]]),
+           _c_array("kNtrVal", "int", [r[6] for r in light_nucleon_tables()["NtoR"]]),
+           _c_array("kRtnIdx", "int", [r[:6] for r in light_nucleon_tables()["RtoN"]]),
+           _c_array("kRtnVal", "int", [r[6] for r in light_nucleon_tables()["RtoN"]]),
+           _c_array("kRtrIdx", "int", [r[:8] for r in light_nucleon_tables()["RtoR"]]),
+           _c_array("kRtrVal", "int", [r[8] for r in light_nucleon_tables()["RtoR"]]),
+           _c_array("kCSink", "int", light_lane_tables()[0]),
+           _c_array("kLightLane", "int", light_lane_tables()[1]),
+           _c_array("kLightG5", "int", light_lane_tables()[2]),
+           _c_array("kCTransposeSign", "int", [transpose_sign(CMAT)]),
            _c_array("kEps", "int", eps),
            _c_array("kEpsSign", "int", sgn),
            "}  // namespace p2\n"]

@@ -63,6 +63,12 @@ def reference_digests(ref_root: str):
         "eps": spin.table_digest(c_array_numbers(ku, "eps")),
         "sgn_eps": spin.table_digest(c_array_numbers(ku, "sgn_eps")),
     }
+    for key, fname, tname in (("ntor", "PLEGMA_baryons_NtoR.cu", "NTR"), ("rton", "PLEGMA_baryons_RtoN.cu", "RtoN"),
+                              ("rtor", "PLEGMA_baryons_RtoR.cu", "RTR")):
+        with open(os.path.join(kern, fname)) as f:
+            src = f.read()
+        out[key + "_indices"] = spin.table_digest(c_array_numbers(src, tname + "_indices"))
+        out[key + "_values"] = spin.table_digest(c_array_numbers(src, tname + "_values"))
     out.update(reference_udsc_digests(kern))
     return out
 

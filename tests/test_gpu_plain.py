@@ -177,3 +177,21 @@ def test_delta_single_isospin(what, mode):
     err = per_t_error(out, what, 6, moms, ref, taus)
     assert err.max() < (TOL if mode == p2.P2_PLAIN_FP64 else 1e-6), err
     ctx.close()
+
+
+LIGHT = p2.NUCLEON_NTOR | p2.NUCLEON_RTON | p2.NUCLEON_RTOR
+
+
+@pytest.mark.parametrize("what", [LIGHT, NUC | LIGHT | p2.DELTA_ISO12 | p2.MESON_G16, p2.NUCLEON_RTOR])
+@pytest.mark.parametrize("mode", [p2.P2_PLAIN_FP64, p2.P2_SPLIT_FP16])
+def test_second_nucleon_interpolator(what, mode):
+    """NtoR, RtoN, RtoR (the reference's light-baryon build), alone and mixed
+    with the other blocks, both forms."""
+    ctx = p2.Context((4, 3, 2, 6))
+    bufs = device_props(ctx, [(45, 0), (45, 1)], t0=3)
+    out, moms = run(ctx, bufs, (1, 2, 1, 3), 6, what, q2max=2, mode=mode)
+    taus = list(range(6))
+    ref = oracle_blocks(ctx.L, bufs, (1, 2, 1, 3), moms, what, taus)
+    err = per_t_error(out, what, 6, moms, ref, taus)
+    assert err.max() < (TOL if mode == p2.P2_PLAIN_FP64 else 1e-6), err
+    ctx.close()

@@ -172,3 +172,13 @@ def test_twopt_zero_momentum_is_site_sum(rng):
     # tau -> global slice (t0 + tau) mod T: tau = 1 is slice 0
     s = np.array([orc.site(u[:, x], d[:, x], NUC | G16) for x in range(V3)])
     assert np.allclose(pos[1].T, s)
+
+
+@pytest.mark.parametrize("which,bit", [(0, 1 << 7), (1, 1 << 8), (2, 1 << 9)])
+def test_oracle_second_nucleon_interpolator_matches_reference_build(rng, which, bit):
+    """NtoR, RtoN, RtoR of the oracle against the reference's own functions."""
+    if orc.reference() is None:
+        pytest.skip("reference contraction library not built here")
+    for _ in range(3):
+        u, d = rand_site(rng), rand_site(rng)
+        assert rel(orc.site(u, d, bit), orc.ref_light(u, d, which)) < 1e-13

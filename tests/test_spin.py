@@ -76,3 +76,11 @@ def test_generated_header_is_current():
     path = os.path.join(os.path.dirname(spin.__file__), "csrc", "spin_tables.h")
     with open(path) as f:
         assert f.read() == spin.header_text()
+
+
+@pytest.mark.parametrize("key,name", [("ntor", "NtoR"), ("rton", "RtoN"), ("rtor", "RtoR")])
+def test_second_nucleon_interpolator_tables_match_reference(digests, key, name):
+    """NtoR, RtoN, RtoR tables (R = eps (u C d) g5 u) in the reference's column order."""
+    rows = spin.light_nucleon_tables()[name]
+    assert spin.table_digest([r[:-1] for r in rows]) == digests[key + "_indices"]
+    assert spin.table_digest([r[-1] for r in rows]) == digests[key + "_values"]
