@@ -172,8 +172,35 @@ class PLEGMA_Propagator : public PLEGMA_Field<Float> {
             "fillSynthetic");
     }
   }
+  // In-place pre-processing on the device copy, as the reference's methods
+  // (lib/PLEGMA_Propagator.cu:98-107,190-192): the physical-basis rotation
+  // with sign +-1, g5 P, and the antiperiodic sign on global t < t0.
+  void rotateToPhysicalBase_device(int sign) {
+    if (sign != 1 && sign != -1) throw PLEGMA_exception("The sign can be only +-1");
+    transform_(sign > 0 ? P2_PROP_ROTATE_PLUS : P2_PROP_ROTATE_MINUS, 0, "rotateToPhysicalBase_device");
+  }
+  void applyBoundaries_device(int t0) { transform_(P2_PROP_BOUNDARY, t0, "applyBoundaries_device"); }
+  void apply_gamma5() { transform_(P2_PROP_GAMMA5, 0, "apply_gamma5"); }
+  // The host copy: through the device copy (lib/PLEGMA_Propagator.cu:111-188
+  // rotates on the host; the result is the same).
+  void rotateToPhysicalBase_host(int sign) {
+    if (sign != 1 && sign != -1) throw PLEGMA_exception("The sign can be only +-1");
+    if (!this->h_elem || !this->d_elem)
+      throw PLEGMA_exception("rotateToPhysicalBase_host: field needs host and device storage");
+    this->copyToDevice();
+    rotateToPhysicalBase_device(sign);
+    this->copyToHost();
+  }
+  // The same transforms applied while contracting instead, leaving the stored
+  // field as it is (no extra pass over the field): flags P2_PROP_*.
+  void transformOnLoad(unsigned flags, int boundary_t0 = 0) {
+    load_xf = flags;
+    load_t0 = boundary_t0;
+  }
   p2_prop view() const {
     p2_prop p{};
+    p.transform = load_xf;
+    p.boundary_t0 = load_t0;
     p.data = this->d_elem ? (const void*)this->d_elem : (const void*)this->h_elem;
     if (!p.data) throw PLEGMA_exception("propagator has no storage");
     p.precision = precision_of<Float>();
@@ -181,6 +208,17 @@ class PLEGMA_Propagator : public PLEGMA_Field<Float> {
     p.t_first = Runtime::get().procPosition[DIM_T] * Runtime::get().localL[DIM_T];
     p.nt = Runtime::get().localL[DIM_T];
     return p;
+  }
+
+ private:
+  unsigned load_xf = 0;
+  int load_t0 = 0;
+  void transform_(unsigned flags, int t0, const char* what) {
+    if (!this->d_elem) throw PLEGMA_exception(std::string(what) + ": propagator has no device storage");
+    Runtime::check(p2_prop_transform(Runtime::context(), this->d_elem, precision_of<Float>(),
+                                     Runtime::get().procPosition[DIM_T] * Runtime::get().localL[DIM_T],
+                                     Runtime::get().localL[DIM_T], flags, t0),
+                   what);
   }
 };
 

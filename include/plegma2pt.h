@@ -101,6 +101,22 @@ typedef struct {
   int device;
 } p2_geom;
 
+/* Pre-processing a contraction applies to a propagator while loading it, in
+ * this order (the production driver applies the first and the last in place
+ * before contracting, plegma/Calc_2pt.cpp:112-113):
+ *   ROTATE_PLUS / ROTATE_MINUS  twisted-mass rotation to the physical basis,
+ *     P'[mu][nu] = (P[mu][nu] - P[mu+2][nu+2] + s i (P[mu][nu+2] + P[mu+2][nu])) / 2
+ *     with s = +1 / -1, indices mod 4 (PLEGMA_propagator_utils.cuh:97-126);
+ *   GAMMA5    g5 P, P'[mu][nu] = P[mu+2][nu] (PLEGMA_propagator_utils.cuh:31-53);
+ *   BOUNDARY  antiperiodic sign: P' = -P on global times t < boundary_t0
+ *     (PLEGMA_propagator_utils.cuh:64-80). */
+enum {
+  P2_PROP_ROTATE_PLUS = 1u << 0,
+  P2_PROP_ROTATE_MINUS = 1u << 1,
+  P2_PROP_GAMMA5 = 1u << 2,
+  P2_PROP_BOUNDARY = 1u << 3
+};
+
 /* Non-owning view of one propagator (PLEGMA_Propagator<Float>::D_elem()/H_elem()). */
 typedef struct {
   const void* data;
@@ -108,6 +124,8 @@ typedef struct {
   int location;  /* p2_location; host views are streamed through the device */
   int t_first;   /* global time of stored slice 0 */
   int nt;        /* stored slices (the local time extent for a full field) */
+  unsigned transform; /* P2_PROP_* applied on load (0 = none) */
+  int boundary_t0;    /* for P2_PROP_BOUNDARY */
 } p2_prop;
 
 /* One two-point request: one source, one time window, one contraction set. */
@@ -198,6 +216,15 @@ p2_status p2_ft_apply(p2_ctx* ctx, const double* field, int dof, int nt, const i
  * race. */
 p2_status p2_ft_apply_noalloc(p2_ctx* ctx, const double* field, int dof, int nt, const int* moms, int nmom,
                               int sign, double* out);
+
+/* Apply P2_PROP_* transforms in place to a device propagator field (layout as
+ * p2_prop, nt slices from global time t_first), asynchronously on the
+ * context's stream: rotateToPhysicalBase_device / apply_gamma5 /
+ * applyBoundaries_device of PLEGMA_Propagator (lib/PLEGMA_Propagator.cu,
+ * lib/kernels/PLEGMA_propagator_utils.cuh:31-134).  Setting p2_prop::transform
+ * instead applies them while contracting, without touching the field. */
+p2_status p2_prop_transform(p2_ctx* ctx, void* data, int precision, int t_first, int nt, unsigned transform,
+                            int boundary_t0);
 
 /* Source-relative times tau of a request that this rank computes: the slices
  * of the window inside its time slab (p2_geom coords[3]) that both

@@ -185,3 +185,24 @@ def udsc_twopt(L, props, src, moms, datasets, taus, t_first=0, fp32=False):
     if rc != 0:
         raise RuntimeError(f"orc_udsc_twopt failed ({rc})")
     return out, asum
+
+
+def prop_transform(p, V3, t_first, nt, T, transform, boundary_t0=0):
+    """The reference's propagator pre-processing on a host copy [144][V3*nt]:
+    rotateToPhysicalBase (lib/kernels/PLEGMA_propagator_utils.cuh:97-126),
+    g5 P (:31-53) and the antiperiodic sign (:64-80), in that order."""
+    P = np.array(p, dtype=np.complex128).reshape(4, 4, 9, nt, V3)
+    if transform & 3:
+        s = 1.0 if transform & 1 else -1.0
+        Q = np.empty_like(P)
+        for mu in range(4):
+            for nu in range(4):
+                Q[mu, nu] = 0.5 * (P[mu, nu] - P[(mu + 2) % 4, (nu + 2) % 4] +
+                                   s * 1j * (P[mu, (nu + 2) % 4] + P[(mu + 2) % 4, nu]))
+        P = Q
+    if transform & 4:
+        P = P[[2, 3, 0, 1]]
+    if transform & 8:
+        t = (t_first + np.arange(nt)) % T
+        P = np.where((t < boundary_t0)[None, None, None, :, None], -P, P)
+    return P.reshape(144, nt * V3)

@@ -91,6 +91,9 @@ p2_status check_prop(p2_ctx* c, const p2_prop& p, const char* name) {
     return c->fail(P2_ERR_INVALID_ARG, std::string(name) + ": bad precision");
   if (p.location != P2_DEVICE && p.location != P2_HOST)
     return c->fail(P2_ERR_INVALID_ARG, std::string(name) + ": bad location");
+  if (p.transform & ~0xFu) return c->fail(P2_ERR_INVALID_ARG, std::string(name) + ": unknown transform bits");
+  if ((p.transform & P2_PROP_ROTATE_PLUS) && (p.transform & P2_PROP_ROTATE_MINUS))
+    return c->fail(P2_ERR_INVALID_ARG, std::string(name) + ": both rotation signs");
   return P2_OK;
 }
 
@@ -138,6 +141,19 @@ Stager::Stager(p2_ctx* ctx, const p2_prop* pp, const p2_request* rr, const Work&
 
 namespace {
 size_t esz_of(const p2_prop& p) { return p.precision == P2_FP64 ? 16 : 8; }
+}  // namespace
+
+// PropXf code of a view's load-time transform on global time t.
+int prop_xf_code(const p2_prop& p, int t) {
+  int code = 0;
+  if (p.transform & P2_PROP_ROTATE_PLUS) code |= p2::PropXf::kRotPlus;
+  if (p.transform & P2_PROP_ROTATE_MINUS) code |= p2::PropXf::kRotMinus;
+  if (p.transform & P2_PROP_GAMMA5) code |= p2::PropXf::kGamma5;
+  if ((p.transform & P2_PROP_BOUNDARY) && t < p.boundary_t0) code |= p2::PropXf::kNegate;
+  return code;
+}
+
+namespace {
 }  // namespace
 
 p2_status Stager::prepare(double* const* outs) {
@@ -205,6 +221,9 @@ p2_status Stager::prepare(double* const* outs) {
       sd.tau = s.tau;
       sd.totalT = r.totalT;
       for (int d = 0; d < 3; d++) sd.x0[d] = r.source[d];
+      const int t = (r.source[3] + s.tau) % c->T;
+      sd.xf[0] = prop_xf_code(props[r.prop_u], t);
+      sd.xf[1] = prop_xf_code(props[r.prop_d], t);
     }
   }
   P2_TRY(c, c->sdesc.ensure(bytes), "descriptor alloc");

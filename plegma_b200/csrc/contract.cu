@@ -202,6 +202,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
     cp_async_wait<1>();
     __syncthreads();
     const int tl = (int)(tile / tiles_per_tau);
+    {
+      // load-time transform of the staged tile, in place (uniform per tile)
+      const int xfu = a.sl[tl].xf[0], xfd = a.sl[tl].xf[1];
+      if (xfu | xfd) {
+        const int s = tid & (kSitesPerTile - 1);
+        for (int q = tid >> 4; q < 72; q += kThreads / kSitesPerTile) {
+          const int f = q >= 36;
+          int comp[4];
+          prop_group_comps(q - 36 * f, comp);
+          Cx<double>* r = st + s * kRow + 144 * f;
+          prop_group_transform(r[comp[0]], r[comp[1]], r[comp[2]], r[comp[3]], f ? xfd : xfu);
+        }
+        __syncthreads();
+      }
+    }
     const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + hw;
     if (x < a.V3) {
       const RowF64 row{st + hw * kRow};
@@ -277,19 +292,35 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
     // (site s, components c0 + 16 j) reads the component-major staging and
     // writes the site's padded row (exact power-of-two scales; products are
     // formed in double so that no intermediate leaves the representable range)
+    // Thread (site s, transform groups q = c0 + 16 j of 72: 36 per flavour)
+    // applies the slice's load-time transform to the group's four blocks.
     {
       const double su = ldexp(1.0, -a.exps[2 * tl]), sd = ldexp(1.0, -a.exps[2 * tl + 1]);
+      const int xfu = a.sl[tl].xf[0], xfd = a.sl[tl].xf[1];
       const int s = tid & (kSitesPerTile - 1), c0 = tid >> 4, sw = s & 7;
       Cx<float>* row = sf + s * kRow32;
 #pragma unroll
-      for (int j = 0; j < 18; j++) {
-        const int f = j >= 9;
-        const int cc = c0 + 16 * (j - 9 * f);  // component within the flavour
-        const int blk = cc / 9, col = cc - 9 * blk;
-        const Cx<Tin> v = st[(144 * f + cc) * kSitesPerTile + s];
-        const double sc = f ? sd : su;
-        row[2 * row32_unit(16 * f + blk, col >> 1, sw) + (col & 1)] =
-            cx<float>((float)((double)v.x * sc), (float)((double)v.y * sc));
+      for (int j = 0; j < 5; j++) {
+        const int q = c0 + 16 * j;
+        if (q < 72) {
+          const int f = q >= 36;
+          int comp[4];
+          prop_group_comps(q - 36 * f, comp);
+          Cx<double> v[4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const Cx<Tin> x = st[(144 * f + comp[i]) * kSitesPerTile + s];
+            v[i] = cx<double>((double)x.x, (double)x.y);
+          }
+          prop_group_transform(v[0], v[1], v[2], v[3], f ? xfd : xfu);
+          const double sc = f ? sd : su;
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const int blk = comp[i] / 9, col = comp[i] - 9 * blk;
+            row[2 * row32_unit(16 * f + blk, col >> 1, sw) + (col & 1)] =
+                cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
+          }
+        }
       }
     }
     __syncthreads();
@@ -351,7 +382,8 @@ __global__ void k_sample_exponents(const SampleArgs a) {
     if (threadIdx.x < s) red[threadIdx.x] = max(red[threadIdx.x], red[threadIdx.x + s]);
     __syncthreads();
   }
-  if (threadIdx.x == 0) a.exp_out[2 * tl + f] = red[0] == -100000 ? 0 : red[0];
+  // a rotation can double an entry: one more power of two of headroom
+  if (threadIdx.x == 0) a.exp_out[2 * tl + f] = (red[0] == -100000 ? 0 : red[0]) + ((sd.xf[f] & 3) ? 1 : 0);
 }
 
 }  // namespace

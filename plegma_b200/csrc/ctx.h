@@ -180,6 +180,7 @@ struct Stager {
 };
 
 int components_of(unsigned what);
+int prop_xf_code(const p2_prop& p, int t);
 p2::CompOffsets offsets_of(unsigned what);
 // [3][nmom][Lmax] complex exp(sign i 2 pi n_d x_d / L_d), x_d the global coordinate of local xl
 std::vector<double> phase_tables(const p2_ctx* c, const int* moms, int nmom, int sign, int Lmax);

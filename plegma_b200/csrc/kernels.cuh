@@ -24,7 +24,13 @@ struct SliceDesc {
   int tau;                 // source-relative time of the slice
   int totalT;              // window of the request (result layout)
   int x0[3];               // spatial source position of the request
-  int pad;
+  int xf[2];               // load-time transform of the u and d slice (prop_xf_code)
+};
+
+// Load-time propagator transform of one slice, see P2_PROP_* in plegma2pt.h:
+// bits 0-1 rotation (1: s = +1, 2: s = -1), bit 2 g5 from the left, bit 3 sign flip.
+struct PropXf {
+  static constexpr int kRotPlus = 1, kRotMinus = 2, kGamma5 = 4, kNegate = 8;
 };
 
 struct ContractArgs {

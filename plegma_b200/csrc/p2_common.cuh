@@ -87,6 +87,51 @@ __device__ __forceinline__ f32x2 f2fma(f32x2 a, f32x2 b, f32x2 c) {
   return d;
 }
 
+// Load-time propagator transform (PropXf codes) of the four spin blocks
+// v0 = P[m][n], v1 = P[m][n+2], v2 = P[m+2][n], v3 = P[m+2][n+2] of one colour
+// pair (m, n in {0, 1}): rotation P'[mu][nu] = (P[mu][nu] - P[mu+2][nu+2] +
+// s i (P[mu][nu+2] + P[mu+2][nu])) / 2 (indices mod 4), then g5 P (P'[mu][nu] =
+// P[mu+2][nu]), then the sign.
+template <typename R>
+__device__ __forceinline__ void prop_group_transform(Cx<R>& v0, Cx<R>& v1, Cx<R>& v2, Cx<R>& v3, int code) {
+  const int rot = code & 3;
+  if (rot) {
+    const R s = rot == 1 ? R(1) : R(-1);
+    auto is = [&](Cx<R> x) { return cx<R>(-s * x.y, s * x.x); };
+    const Cx<R> a = cscale(v0 - v3 + is(v1 + v2), R(0.5));
+    const Cx<R> b = cscale(v1 - v2 + is(v0 + v3), R(0.5));
+    const Cx<R> c = cscale(v2 - v1 + is(v3 + v0), R(0.5));
+    const Cx<R> d = cscale(v3 - v0 + is(v2 + v1), R(0.5));
+    v0 = a;
+    v1 = b;
+    v2 = c;
+    v3 = d;
+  }
+  if (code & 4) {
+    const Cx<R> t0 = v0, t1 = v1;
+    v0 = v2;
+    v1 = v3;
+    v2 = t0;
+    v3 = t1;
+  }
+  if (code & 8) {
+    v0 = cscale(v0, R(-1));
+    v1 = cscale(v1, R(-1));
+    v2 = cscale(v2, R(-1));
+    v3 = cscale(v3, R(-1));
+  }
+}
+
+// Components of transform group q (0..35) of one propagator: colour pair
+// cc = q / 4, base (m, n) = ((q % 4) >> 1, q & 1); blocks b, b+2, b+8, b+10.
+__device__ __forceinline__ void prop_group_comps(int q, int comp[4]) {
+  const int cc = q >> 2, b = ((q & 3) >> 1) * 4 + (q & 1);
+  comp[0] = b * 9 + cc;
+  comp[1] = (b + 2) * 9 + cc;
+  comp[2] = (b + 8) * 9 + cc;
+  comp[3] = (b + 10) * 9 + cc;
+}
+
 // Index of spin block (mu, nu) in a site's 144 components; colour (a, b) adds a*3 + b.
 __host__ __device__ constexpr int sblk(int mu, int nu) { return (mu * 4 + nu) * 9; }
 

@@ -49,6 +49,8 @@ constexpr int kMaxDs = 16;          // datasets per product (the reference's lar
 
 struct UdscSlice {
   long long off[3];  // element offset of the slice inside each of the three views
+  int xf[3];         // load-time transform of each view on this slice (PropXf)
+  int pad;
 };
 
 struct UdscArgs {
@@ -105,6 +107,21 @@ __global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc(const UdscArgs a
     cp_async_wait<1>();
     __syncthreads();
     const int tl = (int)(tile / tiles_per_tau);
+    {
+      // load-time transforms of the staged tile, in place (uniform per tile)
+      const UdscSlice& sd = a.sl[tl];
+      if (sd.xf[0] | sd.xf[1] | sd.xf[2]) {
+        const int s = tid & (kSitesU - 1);
+        for (int q = tid >> 4; q < 108; q += kThreadsU / kSitesU) {
+          const int f = q / 36;
+          int comp[4];
+          prop_group_comps(q - 36 * f, comp);
+          Cx<double>* r = st + s * kRowU + 144 * f;
+          prop_group_transform(r[comp[0]], r[comp[1]], r[comp[2]], r[comp[3]], sd.xf[f]);
+        }
+        __syncthreads();
+      }
+    }
     const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesU + hw;
     if (x < a.V3) {
       const RowF64 row{st + hw * kRowU};
@@ -312,6 +329,8 @@ p2_status p2_contract_udsc(p2_ctx* c, const p2_prop* props, int nprops, const p2
       const p2_prop& pr = props[prop_of(*r, kUdscProduct[p][k])];
       if (!pr.data || pr.nt < 1 || pr.nt > c->T || pr.t_first < 0 || pr.t_first >= c->T)
         return c->fail(P2_ERR_INVALID_ARG, "p2_contract_udsc: bad propagator view");
+      if ((pr.transform & ~0xFu) || ((pr.transform & 1u) && (pr.transform & 2u)))
+        return c->fail(P2_ERR_INVALID_ARG, "p2_contract_udsc: bad transform bits");
       if (pr.precision != P2_FP64) return c->fail(P2_ERR_UNSUPPORTED, "p2_contract_udsc needs FP64 propagators");
       if (pr.location != P2_DEVICE)
         return c->fail(P2_ERR_UNSUPPORTED, "p2_contract_udsc needs device-resident propagators");
@@ -357,12 +376,13 @@ p2_status p2_contract_udsc(p2_ctx* c, const p2_prop* props, int nprops, const p2
     for (int tau = 0; tau < r->totalT; tau++) {
       const int t = (r->source[3] + tau) % T;
       if (t < tl0 || t >= tl0 + c->Ll[3]) continue;
-      UdscSlice s;
+      UdscSlice s{};
       bool ok = true;
       for (int k = 0; k < 3; k++) {
         const int j = ((t - v[k]->t_first) % T + T) % T;
         ok &= j < v[k]->nt;
         s.off[k] = (long long)j * c->V3;
+        s.xf[k] = prop_xf_code(*v[k], t);
       }
       if (!ok) continue;
       taus.push_back(tau);

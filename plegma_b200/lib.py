@@ -56,7 +56,13 @@ class P2Geom(C.Structure):
 
 class P2Prop(C.Structure):
     _fields_ = [("data", C.c_void_p), ("precision", C.c_int), ("location", C.c_int), ("t_first", C.c_int),
-                ("nt", C.c_int)]
+                ("nt", C.c_int), ("transform", C.c_uint), ("boundary_t0", C.c_int)]
+
+
+PROP_ROTATE_PLUS = 1 << 0
+PROP_ROTATE_MINUS = 1 << 1
+PROP_GAMMA5 = 1 << 2
+PROP_BOUNDARY = 1 << 3
 
 
 class P2Request(C.Structure):
@@ -86,7 +92,7 @@ EXPORTS = ["p2_ctx_create", "p2_ctx_destroy", "p2_last_error", "p2_sync", "p2_se
            "p2_mom_list", "p2_block_info", "p2_contract_project", "p2_contract_position", "p2_ft_apply",
            "p2_synth_propagator", "p2_profile_enable", "p2_profile_read", "p2_alloc", "p2_free", "p2_copy",
            "p2_ft_apply_noalloc", "p2_set_workspace", "p2_graph_create", "p2_graph_launch", "p2_graph_sync",
-           "p2_graph_destroy", "p2_tune_enable", "p2_tune_count", "p2_udsc_datasets", "p2_contract_udsc", "p2_local_taus"]
+           "p2_graph_destroy", "p2_tune_enable", "p2_tune_count", "p2_udsc_datasets", "p2_contract_udsc", "p2_local_taus", "p2_prop_transform"]
 
 _lib = None
 
@@ -112,6 +118,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.p2_graph_destroy.argtypes = [C.c_void_p]
     lib.p2_tune_enable.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
     lib.p2_tune_count.argtypes = [C.c_void_p]
+    lib.p2_prop_transform.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint, C.c_int]
     lib.p2_local_taus.argtypes = [C.c_void_p, C.POINTER(P2Prop), C.c_int, C.POINTER(P2Request),
                                   C.POINTER(C.c_int), C.c_int]
     lib.p2_udsc_datasets.argtypes = [C.POINTER(P2UdscRequest), C.c_char_p, C.c_size_t]
@@ -217,10 +224,13 @@ class Context:
         self.check(self.lib.p2_synth_propagator(self.h, C.c_void_p(ptr), int(on_device), precision, seed, flavour,
                                                 t0, decay, t_first, nt))
 
-    def prop(self, ptr: int, precision=P2_FP64, location=P2_DEVICE, t_first=0, nt=None) -> P2Prop:
-        """A propagator view; nt defaults to the local time extent."""
+    def prop(self, ptr: int, precision=P2_FP64, location=P2_DEVICE, t_first=0, nt=None, transform=0,
+             boundary_t0=0) -> P2Prop:
+        """A propagator view; nt defaults to the local time extent; transform = PROP_* bits applied on load."""
         nt = self.Ll[3] if nt is None else nt
         p = P2Prop()
+        p.transform = transform
+        p.boundary_t0 = boundary_t0
         p.data = ptr
         p.precision = precision
         p.location = location
@@ -254,6 +264,12 @@ class Context:
         pa = (P2Prop * len(props))(*props)
         ra = (P2Request * len(reqs))(*reqs)
         self.check(self.lib.p2_contract_project(self.h, pa, len(props), ra, len(reqs)))
+
+    def prop_transform(self, ptr: int, transform: int, boundary_t0=0, precision=P2_FP64, t_first=0, nt=None):
+        """p2_prop_transform: apply PROP_* transforms in place to a device field."""
+        nt = self.Ll[3] if nt is None else nt
+        self.check(self.lib.p2_prop_transform(self.h, C.c_void_p(ptr), precision, t_first, nt, transform,
+                                              boundary_t0))
 
     def local_taus(self, props: Sequence[P2Prop], req: P2Request):
         """p2_local_taus: source-relative times this rank computes."""

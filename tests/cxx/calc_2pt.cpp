@@ -1,8 +1,10 @@
 // A caller of the drop-in C++ surface, written the way the reference's
 // production driver (plegma/Calc_2pt.cpp:73-131) uses PLEGMA_Correlator:
 // two propagators, a momentum-space correlator per source, contractMesons*,
-// contractBaryons, contractBaryonsUDSC, writeFile.  The GPU tests compare what it writes with the
-// C ABI results and the oracle.
+// contractBaryons, contractBaryonsUDSC, writeFile, and the propagator
+// pre-processing (rotateToPhysicalBase_device, applyBoundaries_device,
+// apply_gamma5).  The GPU tests compare what it writes with the C ABI
+// results and the oracle.
 //
 //   calc_2pt Lx Ly Lz Lt sx sy sz st totalT q2max mode out_prefix
 #include <cstdio>
@@ -64,6 +66,27 @@ int main(int argc, char** argv) {
     up.copyToHost();
     f = std::fopen((out + "_up.bin").c_str(), "wb");
     std::fwrite(up.H_elem(), sizeof(double), (size_t)2 * 144 * up.Total_length(), f);
+    std::fclose(f);
+
+    // pre-processing: in place (rotation +1, boundary at the source, g5) and
+    // applied on load; the nucleon from both must agree
+    PLEGMA_Propagator<double> rot(BOTH), lazy(DEVICE);
+    rot.fillSynthetic(2024, 0, src[3], 0.5);
+    lazy.fillSynthetic(2024, 0, src[3], 0.5);
+    rot.rotateToPhysicalBase_device(+1);
+    rot.applyBoundaries_device(src[3]);
+    lazy.transformOnLoad(P2_PROP_ROTATE_PLUS | P2_PROP_BOUNDARY, src[3]);
+    PLEGMA_Correlator<double> br(MOMENTUM_SPACE, src, q2max, totalT), bl(MOMENTUM_SPACE, src, q2max, totalT);
+    br.setMode(mode);
+    bl.setMode(mode);
+    br.contractBaryons(rot, dn);
+    bl.contractBaryons(lazy, dn);
+    br.writeFile(out + "_baryons_rot", DEFAULT_FORMAT);
+    bl.writeFile(out + "_baryons_lazy", DEFAULT_FORMAT);
+    rot.apply_gamma5();
+    rot.copyToHost();
+    f = std::fopen((out + "_rot.bin").c_str(), "wb");
+    std::fwrite(rot.H_elem(), sizeof(double), (size_t)2 * 144 * rot.Total_length(), f);
     std::fclose(f);
     PLEGMA_finalize();
   } catch (const PLEGMA_exception& e) {

@@ -153,3 +153,19 @@ def test_udsc_through_the_drop_in(outputs):
     ctx.contract_udsc([ctx.prop(b.data_ptr()) for b in bufs], req)
     ctx.sync()
     assert np.array_equal(v, out.cpu().numpy())
+
+
+def test_propagator_preprocessing(outputs):
+    """rotateToPhysicalBase_device(+1), applyBoundaries_device(t0) and
+    apply_gamma5 against the oracle's restatement; the baryons of the field
+    transformed in place equal those of the same transforms applied on load."""
+    import oracle_py as orc
+    prefix, ctx, bufs, _ = outputs
+    rot = np.fromfile(prefix + "_rot.bin", dtype=np.float64)
+    rot = (rot[0::2] + 1j * rot[1::2]).reshape(144, -1)
+    xf = p2.PROP_ROTATE_PLUS | p2.PROP_BOUNDARY | p2.PROP_GAMMA5
+    ref = orc.prop_transform(bufs[0].cpu().numpy(), ctx.V3, 0, L[3], L[3], xf, SRC[3])
+    assert np.abs(rot - ref).max() <= 1e-15 * np.abs(ref).max()
+    _, a = load(prefix + "_baryons_rot")
+    _, b = load(prefix + "_baryons_lazy")
+    assert np.array_equal(a, b)
