@@ -150,6 +150,21 @@ class PLEGMA_Field {
   }
 };
 
+// Spinor fields (12 components, [mu 3 + c1][site]): the solver's output that
+// a propagator absorbs column by column (include/PLEGMA_Vector.h).
+template <typename Float>
+class PLEGMA_Vector : public PLEGMA_Field<Float> {
+ public:
+  explicit PLEGMA_Vector(ALLOCATION_FLAG a = BOTH, GHOST_FLAG = FIRST_SIDE)
+      : PLEGMA_Field<Float>(a, 12, Runtime::get().localVolume) {}
+};
+template <typename Float>
+class PLEGMA_Vector3D : public PLEGMA_Field<Float> {
+ public:
+  explicit PLEGMA_Vector3D(ALLOCATION_FLAG a = BOTH)
+      : PLEGMA_Field<Float>(a, 12, Runtime::get().localVolume / Runtime::get().localL[DIM_T]) {}
+};
+
 template <typename Float>
 class PLEGMA_Propagator : public PLEGMA_Field<Float> {
  public:
@@ -171,6 +186,16 @@ class PLEGMA_Propagator : public PLEGMA_Field<Float> {
             p2_synth_propagator(c, this->h_elem, 0, precision_of<Float>(), seed, flavour, t0, decay, t_first, nt),
             "fillSynthetic");
     }
+  }
+  // Column (nu, c2) from a spinor field, device to device
+  // (lib/PLEGMA_Propagator.cu:33-95): the whole 4-D vector; or only global
+  // slice global_it (from a 4-D or a 3-D vector), the rest of the column zero.
+  void absorb(PLEGMA_Vector<Float>& vec, int nu, int c2) { absorb_(vec.D_elem(), 0, -1, nu, c2); }
+  void absorb(PLEGMA_Vector<Float>& vec, int global_it, int nu, int c2) {
+    absorb_(vec.D_elem(), 0, global_it, nu, c2);
+  }
+  void absorb(PLEGMA_Vector3D<Float>& vec, int global_it, int nu, int c2) {
+    absorb_(vec.D_elem(), 1, global_it, nu, c2);
   }
   // In-place pre-processing on the device copy, as the reference's methods
   // (lib/PLEGMA_Propagator.cu:98-107,190-192): the physical-basis rotation
@@ -213,6 +238,15 @@ class PLEGMA_Propagator : public PLEGMA_Field<Float> {
  private:
   unsigned load_xf = 0;
   int load_t0 = 0;
+  void absorb_(const Float* v, int vec_3d, int global_it, int nu, int c2) {
+    if (!this->d_elem || !v) throw PLEGMA_exception("absorb: propagator and vector need device storage");
+    if (global_it >= Runtime::get().totalL[DIM_T])
+      throw PLEGMA_exception("The global time slice you provided exceed the temporal extent");
+    Runtime::check(p2_prop_absorb(Runtime::context(), this->d_elem, v, precision_of<Float>(),
+                                  Runtime::get().procPosition[DIM_T] * Runtime::get().localL[DIM_T],
+                                  Runtime::get().localL[DIM_T], nu, c2, vec_3d, global_it),
+                   "absorb");
+  }
   void transform_(unsigned flags, int t0, const char* what) {
     if (!this->d_elem) throw PLEGMA_exception(std::string(what) + ": propagator has no device storage");
     Runtime::check(p2_prop_transform(Runtime::context(), this->d_elem, precision_of<Float>(),

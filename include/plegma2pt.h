@@ -217,6 +217,19 @@ p2_status p2_ft_apply(p2_ctx* ctx, const double* field, int dof, int nt, const i
 p2_status p2_ft_apply_noalloc(p2_ctx* ctx, const double* field, int dof, int nt, const int* moms, int nmom,
                               int sign, double* out);
 
+/* Copy a spinor field (12 complex components per site, SoA [mu][c1][site]
+ * with mu 3 + c1 major, as the reference's PLEGMA_Vector / PLEGMA_Vector3D)
+ * into column (nu, c2) of a device propagator field (layout as p2_prop, nt
+ * slices from global time t_first), asynchronously on the context's stream:
+ * PLEGMA_Propagator::absorb (lib/PLEGMA_Propagator.cu:33-95).
+ * global_t < 0: the 4-D vector (same nt slices) is copied whole.
+ * global_t >= 0: the column is zeroed and only global slice global_t, when it
+ * lies in the view, is filled: from the same slice of a 4-D vector
+ * (vec_3d = 0) or from a 3-D vector of V3 sites (vec_3d = 1).
+ * global_t >= T is P2_ERR_INVALID_ARG (the reference aborts). */
+p2_status p2_prop_absorb(p2_ctx* ctx, void* prop, const void* vec, int precision, int t_first, int nt, int nu, int c2,
+                         int vec_3d, int global_t);
+
 /* Apply P2_PROP_* transforms in place to a device propagator field (layout as
  * p2_prop, nt slices from global time t_first), asynchronously on the
  * context's stream: rotateToPhysicalBase_device / apply_gamma5 /

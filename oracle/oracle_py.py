@@ -206,3 +206,18 @@ def prop_transform(p, V3, t_first, nt, T, transform, boundary_t0=0):
         t = (t_first + np.arange(nt)) % T
         P = np.where((t < boundary_t0)[None, None, None, :, None], -P, P)
     return P.reshape(144, nt * V3)
+
+
+def prop_absorb(p, vec, V3, t_first, nt, T, nu, c2, vec_3d=False, global_t=-1):
+    """PLEGMA_Propagator::absorb (lib/PLEGMA_Propagator.cu:33-95) on host
+    copies: prop [144][nt V3], vec [12][nt V3] (or [12][V3] for a 3-D vector)."""
+    P = np.array(p, dtype=np.complex128).reshape(4, 4, 3, 3, nt, V3)
+    if global_t < 0:
+        v = np.asarray(vec).reshape(4, 3, nt, V3)
+    else:
+        v = np.zeros((4, 3, nt, V3), dtype=np.complex128)
+        j = (global_t - t_first) % T
+        if j < nt:
+            v[:, :, j] = np.asarray(vec).reshape(4, 3, -1, V3)[:, :, 0 if vec_3d else j]
+    P[:, nu, :, c2] = v
+    return P.reshape(144, nt * V3)

@@ -92,7 +92,8 @@ EXPORTS = ["p2_ctx_create", "p2_ctx_destroy", "p2_last_error", "p2_sync", "p2_se
            "p2_mom_list", "p2_block_info", "p2_contract_project", "p2_contract_position", "p2_ft_apply",
            "p2_synth_propagator", "p2_profile_enable", "p2_profile_read", "p2_alloc", "p2_free", "p2_copy",
            "p2_ft_apply_noalloc", "p2_set_workspace", "p2_graph_create", "p2_graph_launch", "p2_graph_sync",
-           "p2_graph_destroy", "p2_tune_enable", "p2_tune_count", "p2_udsc_datasets", "p2_contract_udsc", "p2_local_taus", "p2_prop_transform"]
+           "p2_graph_destroy", "p2_tune_enable", "p2_tune_count", "p2_udsc_datasets", "p2_contract_udsc", "p2_local_taus", "p2_prop_transform",
+           "p2_prop_absorb"]
 
 _lib = None
 
@@ -119,6 +120,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.p2_tune_enable.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
     lib.p2_tune_count.argtypes = [C.c_void_p]
     lib.p2_prop_transform.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint, C.c_int]
+    lib.p2_prop_absorb.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                   C.c_int, C.c_int]
     lib.p2_local_taus.argtypes = [C.c_void_p, C.POINTER(P2Prop), C.c_int, C.POINTER(P2Request),
                                   C.POINTER(C.c_int), C.c_int]
     lib.p2_udsc_datasets.argtypes = [C.POINTER(P2UdscRequest), C.c_char_p, C.c_size_t]
@@ -270,6 +273,13 @@ class Context:
         nt = self.Ll[3] if nt is None else nt
         self.check(self.lib.p2_prop_transform(self.h, C.c_void_p(ptr), precision, t_first, nt, transform,
                                               boundary_t0))
+
+    def prop_absorb(self, prop: int, vec: int, nu: int, c2: int, precision=P2_FP64, t_first=0, nt=None,
+                    vec_3d=False, global_t=-1):
+        """p2_prop_absorb: column (nu, c2) of a device propagator from a spinor field."""
+        nt = self.Ll[3] if nt is None else nt
+        self.check(self.lib.p2_prop_absorb(self.h, C.c_void_p(prop), C.c_void_p(vec), precision, t_first, nt, nu, c2,
+                                           int(vec_3d), global_t))
 
     def local_taus(self, props: Sequence[P2Prop], req: P2Request):
         """p2_local_taus: source-relative times this rank computes."""

@@ -2,7 +2,7 @@
 // production driver (plegma/Calc_2pt.cpp:73-131) uses PLEGMA_Correlator:
 // two propagators, a momentum-space correlator per source, contractMesons*,
 // contractBaryons, contractBaryonsUDSC, writeFile, and the propagator
-// pre-processing (rotateToPhysicalBase_device, applyBoundaries_device,
+// pre-processing (absorb, rotateToPhysicalBase_device, applyBoundaries_device,
 // apply_gamma5).  The GPU tests compare what it writes with the C ABI
 // results and the oracle.
 //
@@ -87,6 +87,33 @@ int main(int argc, char** argv) {
     rot.copyToHost();
     f = std::fopen((out + "_rot.bin").c_str(), "wb");
     std::fwrite(rot.H_elem(), sizeof(double), (size_t)2 * 144 * rot.Total_length(), f);
+    std::fclose(f);
+
+    // a propagator built from twelve spinor fields (absorb), and one slice of
+    // another from a 3-D field; deterministic, exactly representable entries
+    PLEGMA_Propagator<double> built(BOTH), sliced(BOTH);
+    PLEGMA_Vector<double> vec(BOTH);
+    PLEGMA_Vector3D<double> vec3(BOTH);
+    for (int k = 0; k < 12; k++) {
+      for (size_t i = 0; i < 12 * vec.Total_length(); i++) {
+        vec.H_elem()[2 * i] = (double)((i * 7 + k * 13) % 101) / 16.0 - 3.0;
+        vec.H_elem()[2 * i + 1] = (double)((i * 5 + k * 3) % 67) / 8.0;
+      }
+      vec.copyToDevice();
+      built.absorb(vec, k / 3, k % 3);
+    }
+    for (size_t i = 0; i < 12 * vec3.Total_length(); i++) {
+      vec3.H_elem()[2 * i] = (double)(i % 29) - 14.0;
+      vec3.H_elem()[2 * i + 1] = (double)(i % 13) / 4.0;
+    }
+    vec3.copyToDevice();
+    sliced.fillSynthetic(5, 0, 0, 0.5);
+    sliced.absorb(vec3, src[3], 1, 2);
+    built.copyToHost();
+    sliced.copyToHost();
+    f = std::fopen((out + "_absorb.bin").c_str(), "wb");
+    std::fwrite(built.H_elem(), sizeof(double), (size_t)2 * 144 * built.Total_length(), f);
+    std::fwrite(sliced.H_elem(), sizeof(double), (size_t)2 * 144 * sliced.Total_length(), f);
     std::fclose(f);
     PLEGMA_finalize();
   } catch (const PLEGMA_exception& e) {

@@ -169,3 +169,26 @@ def test_propagator_preprocessing(outputs):
     _, a = load(prefix + "_baryons_rot")
     _, b = load(prefix + "_baryons_lazy")
     assert np.array_equal(a, b)
+
+
+def test_absorb(outputs):
+    """PLEGMA_Propagator::absorb of twelve PLEGMA_Vector fields, and of a
+    PLEGMA_Vector3D into the source slice of a filled propagator."""
+    import oracle_py as orc
+    prefix, ctx, bufs, _ = outputs
+    V = int(np.prod(L))
+    V3 = V // L[3]
+    raw = np.fromfile(prefix + "_absorb.bin", dtype=np.float64)
+    raw = raw[0::2] + 1j * raw[1::2]
+    built, sliced = raw[:144 * V].reshape(144, V), raw[144 * V:].reshape(144, V)
+    i = np.arange(12 * V)
+    expect = np.zeros((144, V), dtype=np.complex128)
+    for k in range(12):
+        vec = ((i * 7 + k * 13) % 101) / 16.0 - 3.0 + 1j * (((i * 5 + k * 3) % 67) / 8.0)
+        expect = orc.prop_absorb(expect, vec, V3, 0, L[3], L[3], k // 3, k % 3)
+    assert np.array_equal(built, expect)
+    j = np.arange(12 * V3)
+    vec3 = (j % 29) - 14.0 + 1j * ((j % 13) / 4.0)
+    (base,) = device_props(ctx, [(5, 0)], t0=0)
+    expect = orc.prop_absorb(base.cpu().numpy(), vec3, V3, 0, L[3], L[3], 1, 2, True, SRC[3])
+    assert np.array_equal(sliced, expect)

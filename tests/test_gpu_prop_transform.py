@@ -91,3 +91,48 @@ def test_fused_transform_in_table_driven_baryons():
         off += len(dss)
     assert off == len(names)
     ctx.close()
+
+
+def _vec(rng, n, dtype):
+    return torch.from_numpy(rng.standard_normal(n) + 1j * rng.standard_normal(n)).to(dtype).cuda()
+
+
+@pytest.mark.parametrize("dtype,prec", [(torch.complex128, p2.P2_FP64), (torch.complex64, p2.P2_FP32)])
+def test_absorb_matches_host(dtype, prec):
+    """The three forms of absorb (whole 4-D vector; one slice of a 4-D vector;
+    a 3-D vector into one slice), on a view of 5 slices from t = 3 of T = 6
+    (so it wraps) and with the slice outside the view (column zeroed)."""
+    ctx = p2.Context((3, 2, 2, 6))
+    V3, nt, t_first = ctx.V3, 5, 3
+    rng = np.random.default_rng(7)
+    prop = _vec(rng, 144 * nt * V3, dtype)
+    v4 = _vec(rng, 12 * nt * V3, dtype)
+    v3 = _vec(rng, 12 * V3, dtype)
+    cases = [(False, -1, 1, 2), (False, 0, 3, 0), (True, 4, 2, 1), (True, 2, 0, 2)]  # t = 2 is not in the view
+    for vec_3d, gt, nu, c2 in cases:
+        before = prop.cpu().numpy()
+        v = v3 if vec_3d else v4
+        ctx.prop_absorb(prop.data_ptr(), v.data_ptr(), nu, c2, prec, t_first, nt, vec_3d, gt)
+        ctx.sync()
+        ref = orc.prop_absorb(before, v.cpu().numpy(), V3, t_first, nt, 6, nu, c2, vec_3d, gt)
+        assert np.array_equal(prop.cpu().numpy().astype(np.complex128).reshape(144, -1), ref)
+    with pytest.raises(p2.P2Error) as e:
+        ctx.prop_absorb(prop.data_ptr(), v3.data_ptr(), 0, 0, prec, t_first, nt, True, 6)
+    assert e.value.status == p2.P2_ERR_INVALID_ARG
+    ctx.close()
+
+
+def test_propagator_from_twelve_columns_contracts_the_same():
+    """Twelve solver vectors (the columns of a propagator) absorbed one by one
+    give the propagator back bit for bit."""
+    ctx = p2.Context((2, 2, 4, 4))
+    (u,) = device_props(ctx, [(17, 0)], t0=1)
+    V = ctx.V3 * 4
+    cols = u.view(4, 4, 3, 3, V).permute(1, 3, 0, 2, 4).contiguous()  # [nu][c2][mu][c1][site]
+    rebuilt = torch.empty_like(u)
+    for nu in range(4):
+        for c2 in range(3):
+            ctx.prop_absorb(rebuilt.data_ptr(), cols[nu, c2].data_ptr(), nu, c2)
+    ctx.sync()
+    assert torch.equal(rebuilt, u)
+    ctx.close()
