@@ -41,7 +41,7 @@ constexpr int kStage = kSitesPerTile * kRow;
 // without bank conflicts and transposed by the split kernel's conversion.
 template <typename Tin, bool CM = false>
 __device__ __forceinline__ void issue_tile(const ContractArgs& a, Cx<Tin>* st, long long tile, long long ntiles,
-                                           int tiles_per_tau) {
+                                           int tiles_per_tau, int f0 = 0, int f1 = 2) {
   if (tile < ntiles) {
     const int tl = (int)(tile / tiles_per_tau);
     const int s = threadIdx.x & (kSitesPerTile - 1);
@@ -51,7 +51,7 @@ __device__ __forceinline__ void issue_tile(const ContractArgs& a, Cx<Tin>* st, l
     // thread i copies component i/16 + 16 r of site i%16; with 256 threads
     // rows r < 9 are the u view's 144 components and r >= 9 the d view's
 #pragma unroll
-    for (int f = 0; f < 2; f++) {
+    for (int f = f0; f < f1; f++) {
       const Cx<Tin>* src = (const Cx<Tin>*)(f ? sd->d : sd->u) + (f ? sd->off_d : sd->off_u) + (ok ? x : 0);
       const long long vol = f ? sd->vol_d : sd->vol_u;
 #pragma unroll 3
@@ -80,15 +80,26 @@ __device__ __forceinline__ int diag10_slot(int g) {
 // and 2 (32 s + j) + 1), which no load of the contraction reads.
 __device__ __forceinline__ int* smax_slot(Cx<float>* sf, int k) {
   const int p = k >> 1, s = p >> 5, j = p & 31;
-  return reinterpret_cast<int*>(sf + s * kRow32 + 2 * row32_unit(j, 4, s & 7) + 1) + (k & 1);
+  return reinterpret_cast<int*>(sf + s * kRow32 + 2 * row32_unit(j, 4) + 1) + (k & 1);
 }
+
+// Split form, 16 x 16 mesons: the outputs of a tile are staged in shared
+// memory as [g2][g1][site] (rows of 16 sites padded to 17, so the 16 lanes of
+// a half-warp, which hold 16 different g1, write 16 different bank pairs) and
+// written to HBM row by row, 128 contiguous bytes per component, by
+// flush_g16 below; direct stores from the lanes would touch 16 component rows
+// per instruction.
+constexpr int kG16Row = 17;
+constexpr int kG16Bytes = 256 * kG16Row * (int)sizeof(Cx<float>);
 
 template <typename R>
 struct Writer {
   Cx<R>* out;
   long long V3;
-  float* rmax;          // split form: this lane's running maxima of its nucleon (2) and G16 (16) outputs
+  float* rmax;          // split form: this lane's running maxima of its nucleon outputs (slots 0, 1)
   Cx<float>* smax_base;  // split form: tile whose spare slots hold the per-component maxima, or null
+  Cx<R>* g16;           // split form: the tile's 16 x 16 meson staging, or null (direct stores)
+  int site;             // site of the tile
   __device__ __forceinline__ void put(int k, Cx<R> v) const {
     out[(long long)k * V3] = v;
     if (smax_base) {
@@ -144,8 +155,13 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
     Cx<R> c[16];
     meson_site(row, kU, kD, lt, l, mask, c);
     if (a.what & 8u) {
+      if (w.g16) {
 #pragma unroll
-      for (int g2 = 0; g2 < 16; g2++) w.put_slot(a.k.g16 + g1 * 16 + g2, c[g2], 2 + g2);
+        for (int g2 = 0; g2 < 16; g2++) w.g16[(g2 * 16 + g1) * kG16Row + w.site] = c[g2];
+      } else {
+#pragma unroll
+        for (int g2 = 0; g2 < 16; g2++) w.out[(long long)(a.k.g16 + g1 * 16 + g2) * w.V3] = c[g2];
+      }
     }
     if (a.what & 16u) {
       if (g1 == 0) w.put(a.k.all34 + 0, c[0]);
@@ -220,7 +236,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
     const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + hw;
     if (x < a.V3) {
       const RowF64 row{st + hw * kRow};
-      const Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr, nullptr};
+      const Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr, nullptr, nullptr, hw};
       contract_site<DELTA>(a, row, lt, l, mask, w);
     }
     __syncthreads();
@@ -231,9 +247,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
 
 // Split form: FP32 arithmetic on power-of-two scaled inputs.  One staging
 // buffer in the input precision (component-major) plus an FP32 copy of the
-// tile in the padded, swizzled row layout of RowF32: the staging buffer is
-// refilled with the next tile's cp.async as soon as the current one is
-// converted, so two CTAs (16 warps) fit on an SM.
+// tile in the padded row layout of RowF32: the staging buffer is refilled
+// with the next tile's cp.async as soon as the current one is converted (the
+// part of it that holds the staged meson outputs after the flush), so two
+// CTAs (16 warps) fit on an SM.
 constexpr int kStage32 = kSitesPerTile * kRow32;
 
 template <typename Tin, bool DELTA>
@@ -241,6 +258,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<Tin>* st = (Cx<Tin>*)smem_raw;
   Cx<float>* sf = (Cx<float>*)(smem_raw + kSitesPerTile * 288 * sizeof(Cx<Tin>));
+  // 16 x 16 meson staging: with FP64 inputs the d half of the staging buffer,
+  // which is idle while a tile is contracted (only the u half of the next
+  // tile is in flight then; the d half follows the flush); with FP32 inputs
+  // a buffer of its own after the FP32 tile
+  constexpr bool kAlias = sizeof(Tin) == 8;
+  Cx<float>* og = kAlias ? (Cx<float>*)(st + 144 * kSitesPerTile) : sf + kStage32;
+  const bool stage = !DELTA && (a.what & 8u);
   const int tid = threadIdx.x;
   const int hw = tid >> 4, l = tid & 15;
   const unsigned mask = halfwarp_mask();
@@ -254,23 +278,33 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
   issue_tile<Tin, true>(a, st, tile, ntiles, tiles_per_tau);
 
   int cur = -1;  // slice whose maxima the spare slots hold
-  // the Delta instantiation tracks its maxima in shared memory only
+  // running maxima in registers: nucleon outputs of lane l (slots 0, 1) and
+  // the staged meson outputs this thread writes out (slots 2 + g2); the
+  // Delta instantiation tracks its maxima in shared memory only
   constexpr int kSlots = DELTA ? 1 : 18;
   float rmax[kSlots];
 #pragma unroll
   for (int i = 0; i < kSlots; i++) rmax[i] = 0.f;
-  // lane maxima -> shared (the two half-warps of a warp own the same components)
+  // register maxima -> shared, once per time slice
   auto flush_lane = [&]() {
-    if (DELTA) return;
+    if constexpr (!DELTA) {
+      // nucleon: lane l of both half-warps holds components nuc + 16 i + l
 #pragma unroll
-    for (int i = 0; i < kSlots; i++) {
-      const float m = fmaxf(rmax[i], __shfl_xor_sync(0xffffffffu, rmax[i], 16));
-      rmax[i] = 0.f;
-      if (!(tid & 16)) {
-        int k = -1;
-        if (i < 2 && (a.what & 1u)) k = a.k.nuc + 16 * i + l;
-        if (i >= 2 && (a.what & 8u)) k = a.k.g16 + lt.meson_g1() * 16 + (i - 2);
-        if (k >= 0) atomicMax(smax_slot(sf, k), __float_as_int(m));
+      for (int i = 0; i < 2; i++) {
+        const float m = fmaxf(rmax[i], __shfl_xor_sync(0xffffffffu, rmax[i], 16));
+        rmax[i] = 0.f;
+        if (!(tid & 16) && (a.what & 1u)) atomicMax(smax_slot(sf, a.k.nuc + 16 * i + l), __float_as_int(m));
+      }
+      // mesons: the 16 threads of half-warp g1 hold components g16 + 16 g1 + g2
+#pragma unroll
+      for (int i = 2; i < kSlots; i++) {
+        float m = rmax[i];
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 4));
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 8));
+        rmax[i] = 0.f;
+        if (l == 0 && stage) atomicMax(smax_slot(sf, a.k.g16 + 16 * hw + (i - 2)), __float_as_int(m));
       }
     }
   };
@@ -289,15 +323,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
       cur = tl;
     }
     // scale by 2^-E per flavour and convert to FP32 once per tile: thread
-    // (site s, components c0 + 16 j) reads the component-major staging and
-    // writes the site's padded row (exact power-of-two scales; products are
-    // formed in double so that no intermediate leaves the representable range)
-    // Thread (site s, transform groups q = c0 + 16 j of 72: 36 per flavour)
-    // applies the slice's load-time transform to the group's four blocks.
+    // (site s, transform groups q = c0 + 16 j of 72: 36 per flavour) reads the
+    // component-major staging, applies the slice's load-time transform to the
+    // group's four blocks and writes the site's padded row (exact
+    // power-of-two scales; products are formed in double so that no
+    // intermediate leaves the representable range)
     {
       const double su = ldexp(1.0, -a.exps[2 * tl]), sd = ldexp(1.0, -a.exps[2 * tl + 1]);
       const int xfu = a.sl[tl].xf[0], xfd = a.sl[tl].xf[1];
-      const int s = tid & (kSitesPerTile - 1), c0 = tid >> 4, sw = s & 7;
+      const int s = tid & (kSitesPerTile - 1), c0 = tid >> 4;
       Cx<float>* row = sf + s * kRow32;
 #pragma unroll
       for (int j = 0; j < 5; j++) {
@@ -317,7 +351,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
 #pragma unroll
           for (int i = 0; i < 4; i++) {
             const int blk = comp[i] / 9, col = comp[i] - 9 * blk;
-            row[2 * row32_unit(16 * f + blk, col >> 1, sw) + (col & 1)] =
+            row[2 * row32_unit(16 * f + blk, col >> 1) + (col & 1)] =
                 cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
           }
         }
@@ -325,12 +359,34 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
     }
     __syncthreads();
     // the staged tile has been converted: refill the staging buffer while contracting
-    issue_tile<Tin, true>(a, st, tile + gridDim.x, ntiles, tiles_per_tau);
-    const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + hw;
-    if (x < a.V3) {
-      const RowF32 row{sf + hw * kRow32, hw & 7};
-      const Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, DELTA ? nullptr : rmax, sf};
+    issue_tile<Tin, true>(a, st, tile + gridDim.x, ntiles, tiles_per_tau, 0, (kAlias && stage) ? 1 : 2);
+    const int x0 = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile;
+    if (x0 + hw < a.V3) {
+      const RowF32 row{sf + hw * kRow32};
+      const Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x0 + hw, a.V3, DELTA ? nullptr : rmax, sf,
+                            stage ? og : nullptr, hw};
       contract_site<DELTA>(a, row, lt, l, mask, w);
+    }
+    if constexpr (!DELTA) {
+      if (stage) {
+        __syncthreads();
+        // thread (site s = tid & 15, g1 = tid >> 4): components g16 + 16 g1 + g2,
+        // each a 128-byte row segment over the tile's 16 sites
+        const int s = tid & 15;
+        if (x0 + s < a.V3) {
+          Cx<float>* o = (Cx<float>*)a.out + ((long long)tl * a.K + a.k.g16 + 16 * hw) * a.V3 + x0 + s;
+#pragma unroll
+          for (int g2 = 0; g2 < 16; g2++) {
+            const Cx<float> v = og[(g2 * 16 + hw) * kG16Row + s];
+            o[(long long)g2 * a.V3] = v;
+            rmax[2 + g2] = fmaxf(rmax[2 + g2], fmaxf(fabsf(v.x), fabsf(v.y)));
+          }
+        }
+        if (kAlias) {
+          __syncthreads();
+          issue_tile<Tin, true>(a, st, tile + gridDim.x, ntiles, tiles_per_tau, 1, 2);
+        }
+      }
     }
   }
   cp_async_wait<0>();
@@ -401,7 +457,8 @@ cudaError_t launch_plain_t(const ContractArgs& a, int grid, cudaStream_t s) {
 
 template <typename Tin, bool DELTA>
 cudaError_t launch_f32_t(const ContractArgs& a, int grid, cudaStream_t s) {
-  const int smem = kSitesPerTile * 288 * (int)sizeof(Cx<Tin>) + kStage32 * (int)sizeof(Cx<float>);
+  const int smem = kSitesPerTile * 288 * (int)sizeof(Cx<Tin>) + kStage32 * (int)sizeof(Cx<float>) +
+                   ((!DELTA && sizeof(Tin) == 4) ? kG16Bytes : 0);
   if (a.K > 2 * 32 * kSitesPerTile) return cudaErrorInvalidValue;  // more components than spare slots
   cudaError_t e = ensure_smem((const void*)k_contract_f32<Tin, DELTA>, smem);
   if (e != cudaSuccess) return e;

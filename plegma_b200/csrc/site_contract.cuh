@@ -85,22 +85,22 @@ struct RowF64 {
 
 // Split-form FP32 tile: every block padded to 10 complex = five 16-byte units
 // (colours 2k, 2k+1 in unit k, colour 8 and a spare slot in unit 4), so a
-// block is four 16-byte loads and one 8-byte load.  Units are XOR-swizzled
-// by sw = site & 7 so that the transposing writes of 16 sites spread over
-// the banks.
-constexpr int kRow32 = 320;  // complex per site row (32 blocks x 10)
-__device__ __forceinline__ int row32_unit(int blk, int k, int sw) { return (blk * 5 + k) ^ sw; }
+// block is four 16-byte loads and one 8-byte load at fixed offsets from a
+// per-lane base.  Rows are 161 units apart (one unit of padding): the
+// transposing writes of 16 sites then start in 8 different bank groups,
+// and the two sites of a warp read disjoint bank groups.
+constexpr int kRow32 = 322;  // complex per site row (32 blocks x 10 + 2)
+__device__ __forceinline__ int row32_unit(int blk, int k) { return blk * 5 + k; }
 
 struct RowF32 {
   typedef float R;
   const Cx<float>* p;
-  int sw;
   __device__ __forceinline__ void pair(int blk, int k, Cx<float>& v0, Cx<float>& v1) const {
-    const float4 q = *reinterpret_cast<const float4*>(p + 2 * row32_unit(blk, k, sw));
+    const float4 q = *reinterpret_cast<const float4*>(p + 2 * row32_unit(blk, k));
     v0 = cx<float>(q.x, q.y);
     v1 = cx<float>(q.z, q.w);
   }
-  __device__ __forceinline__ Cx<float> last(int blk) const { return p[2 * row32_unit(blk, 4, sw)]; }
+  __device__ __forceinline__ Cx<float> last(int blk) const { return p[2 * row32_unit(blk, 4)]; }
   __device__ __forceinline__ void load9(int blk, Cx<float> v[9]) const {
 #pragma unroll
     for (int k = 0; k < 4; k++) pair(blk, k, v[2 * k], v[2 * k + 1]);
