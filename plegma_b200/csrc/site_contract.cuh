@@ -55,12 +55,10 @@ struct LaneTables {
   __device__ __forceinline__ int meson_g1() const { return (int)(mes & 15u); }
 };
 
-__constant__ int c_nuc_sink[4][3] = P2_INIT_NucSink;
 __constant__ int c_nuc_lane[16][8] = P2_INIT_NucLane;
 __constant__ int c_delta_sink[3][4][3] = P2_INIT_DeltaSink;
 __constant__ int c_delta_lane[3][16][8] = P2_INIT_DeltaLane;
 __constant__ int c_meson_lane[16][5] = P2_INIT_MesonLane;
-__constant__ int c_c_sink[4][3] = P2_INIT_CSink;
 __constant__ int c_light_lane[3][16][8] = P2_INIT_LightLane;
 __constant__ int c_light_g5[16][3] = P2_INIT_LightG5;
 
@@ -184,6 +182,72 @@ __device__ __forceinline__ void diquark_G(const Row& row, int X, int Y, const in
   for (int iA = 0; iA < 4; iA++) diquark_acc(row, X, Y, sink[iA][0], sink[iA][1], R(sink[iA][2]), xp, yp, q);
 }
 
+// The same with a sink table known at compile time (S = 0: nucleon C g5,
+// 1..3: Delta C g_k, 4: C): signs fold into the products, block offsets into
+// the load addresses.
+__host__ __device__ constexpr int sink_entry(int S, int i, int f) {
+  return S == 0 ? kNucSink[i][f] : S <= 3 ? kDeltaSink[S - 1][i][f] : kCSink[i][f];
+}
+template <int S, int iA, typename Row>
+__device__ __forceinline__ void diquark_acc_ct(const Row& row, int X, int Y, int xp, int yp,
+                                               Cx<typename Row::R> q[9]) {
+  constexpr int nu = sink_entry(S, iA, 0), lam = sink_entry(S, iA, 1), sg = sink_entry(S, iA, 2);
+  diquark_acc(row, X, Y, nu, lam, typename Row::R(sg), xp, yp, q);
+}
+template <int S, typename Row>
+__device__ __forceinline__ void diquark_G_ct(const Row& row, int X, int Y, int xp, int yp, Cx<typename Row::R> q[9]) {
+  typedef typename Row::R R;
+#pragma unroll
+  for (int i = 0; i < 9; i++) q[i] = czero<R>();
+  diquark_acc_ct<S, 0>(row, X, Y, xp, yp, q);
+  diquark_acc_ct<S, 1>(row, X, Y, xp, yp, q);
+  diquark_acc_ct<S, 2>(row, X, Y, xp, yp, q);
+  diquark_acc_ct<S, 3>(row, X, Y, xp, yp, q);
+}
+
+// Type-a weights fa = cN sN - cL sL of every source table vanish outside one
+// class {l0, l0 ^ 5, l0 ^ 10, l0 ^ 15} of lanes, so their sum over the
+// half-warp takes two butterfly steps (xor 5, xor 10) and a broadcast from
+// l0.  Under the lane transpose (x', y') -> (y', x') the weights are
+// symmetric or antisymmetric (tau = +1 / -1), so for G^{YX} = s G^{XY}
+// transposed the type-a sum is s tau times that of G^{XY}.  Both facts are
+// checked on the generated tables at compile time.
+__host__ __device__ constexpr int typea_lane(const int (&t)[16][8]) {
+  for (int l = 0; l < 16; l++)
+    if (t[l][6] || t[l][7]) return l;
+  return 0;
+}
+__host__ __device__ constexpr bool typea_one_class(const int (&t)[16][8]) {
+  const int l0 = typea_lane(t);
+  for (int l = 0; l < 16; l++) {
+    const int d = l ^ l0;
+    if ((t[l][6] || t[l][7]) && d != 0 && d != 5 && d != 10 && d != 15) return false;
+  }
+  return true;
+}
+__host__ __device__ constexpr int typea_tau(const int (&t)[16][8]) {
+  bool sym = true, anti = true;
+  for (int l = 0; l < 16; l++) {
+    const int lt = ((l & 3) << 2) | (l >> 2);
+    for (int f = 6; f < 8; f++) {
+      sym = sym && t[lt][f] == t[l][f];
+      anti = anti && t[lt][f] == -t[l][f];
+    }
+  }
+  return sym ? 1 : anti ? -1 : 0;
+}
+static_assert(typea_one_class(kNucLane) && typea_one_class(kDeltaLane[0]) && typea_one_class(kDeltaLane[1]) &&
+                  typea_one_class(kDeltaLane[2]) && typea_one_class(kLightLane[0]) &&
+                  typea_one_class(kLightLane[1]) && typea_one_class(kLightLane[2]),
+              "type-a weights outside one lane class");
+static_assert(typea_tau(kNucLane) == -1 && typea_tau(kLightLane[0]) == -1 && typea_tau(kLightLane[1]) == -1 &&
+                  typea_tau(kLightLane[2]) == -1,
+              "nucleon-type type-a weights not antisymmetric under the lane transpose");
+static_assert(typea_tau(kDeltaLane[0]) == 1 && typea_tau(kDeltaLane[1]) == 1 && typea_tau(kDeltaLane[2]) == 1,
+              "Delta type-a weights not symmetric under the lane transpose");
+static_assert(typea_lane(kDeltaLane[0]) == 0 && typea_lane(kDeltaLane[1]) == 0 && typea_lane(kDeltaLane[2]) == 1,
+              "Delta type-a lanes");
+
 // G^{YX} from G^{XY}: move lane (y', x') to lane (x', y') with the table's sign.
 template <typename R>
 __device__ __forceinline__ void diquark_transpose(Cx<R> q[9], int l, unsigned mask, R sign) {
@@ -240,18 +304,17 @@ __device__ __forceinline__ Cx<typename Row::R> diquark_slots(const Cx<typename R
   return r;
 }
 
-// Type-a terms: D = sum over the 16 lanes of fa G (all lanes get D), then the
-// lane's T[mu][mu'] = sum_ce D[c][e] Z[mu][mu'][c][e].
+// Type-a terms: D = sum over the 16 lanes of fa G (all lanes get D; fa is
+// zero outside the lane class of l0), then the lane's
+// T[mu][mu'] = sum_ce D[c][e] Z[mu][mu'][c][e].
 template <typename R>
-__device__ __forceinline__ void diquark_D(const Cx<R> g[9], R fa, unsigned mask, Cx<R> D[9]) {
+__device__ __forceinline__ void diquark_D(const Cx<R> g[9], R fa, unsigned mask, int l0, Cx<R> D[9]) {
 #pragma unroll
   for (int i = 0; i < 9; i++) {
     Cx<R> d = cscale(g[i], fa);
-    d = d + shfl_xor16(d, 1, mask);
-    d = d + shfl_xor16(d, 2, mask);
-    d = d + shfl_xor16(d, 4, mask);
-    d = d + shfl_xor16(d, 8, mask);
-    D[i] = d;
+    d = d + shfl_xor16(d, 5, mask);
+    d = d + shfl_xor16(d, 10, mask);
+    D[i] = shfl_idx16(d, l0, mask);
   }
 }
 template <typename Row>
@@ -266,17 +329,13 @@ __device__ __forceinline__ Cx<typename Row::R> diquark_typea(const Cx<typename R
   return r;
 }
 
-// All Wick terms of one group: slot terms plus type-a terms with the Wick
-// coefficients (c1A, c1B, c2A, c2B, cN, cL).
+// All Wick terms of one group: slot terms with the Wick coefficients
+// (c1A, c1B, c2A, c2B) plus the type-a terms of the sum D.
 template <bool S1, bool S2, typename Row>
 __device__ __forceinline__ Cx<typename Row::R> diquark_eval(const Cx<typename Row::R> g[9], const Row& row, int Z,
                                                             const DiquarkLane& dl, int l, unsigned mask, int c1A,
-                                                            int c1B, int c2A, int c2B, int cN, int cL) {
-  typedef typename Row::R R;
-  const Cx<R> r = diquark_slots<S1, S2>(g, row, Z, dl, l, mask, c1A, c1B, c2A, c2B);
-  Cx<R> D[9];
-  diquark_D(g, R(cN * dl.sN - cL * dl.sL), mask, D);
-  return r + diquark_typea(D, row, Z, l);
+                                                            int c1B, int c2A, int c2B, const Cx<typename Row::R> D[9]) {
+  return diquark_slots<S1, S2>(g, row, Z, dl, l, mask, c1A, c1B, c2A, c2B) + diquark_typea(D, row, Z, l);
 }
 
 // Nucleon C g5, both datasets: out[0] = proton (u u d), out[1] = neutron (d d u),
@@ -285,12 +344,14 @@ template <typename Row>
 __device__ __forceinline__ void nucleon_site(const Row& row, const LaneTables& lt, int l, unsigned mask,
                                              Cx<typename Row::R> out[2]) {
   typedef typename Row::R R;
-  Cx<R> g[9];
-  diquark_G(row, kU, kD, c_nuc_sink, l >> 2, l & 3, g);  // G^{ud}
+  Cx<R> g[9], D[9];
+  diquark_G_ct<0>(row, kU, kD, l >> 2, l & 3, g);  // G^{ud}
   const DiquarkLane dl = unpack_diquark_lane(lt.nuc);
-  out[0] = diquark_eval<true, false>(g, row, kU, dl, l, mask, -1, 0, 0, 0, 1, 0);
-  diquark_transpose<R>(g, l, mask, R(-1));  // G^{du}
-  out[1] = diquark_eval<true, false>(g, row, kD, dl, l, mask, -1, 0, 0, 0, 1, 0);
+  constexpr int l0 = typea_lane(kNucLane);
+  diquark_D(g, R(dl.sN), mask, l0, D);  // cN = 1, cL = 0
+  out[0] = diquark_eval<true, false>(g, row, kU, dl, l, mask, -1, 0, 0, 0, D);
+  diquark_transpose<R>(g, l, mask, R(-1));  // G^{du}; its type-a sum is (-1)(tau = -1) D
+  out[1] = diquark_eval<true, false>(g, row, kD, dl, l, mask, -1, 0, 0, 0, D);
 }
 
 // M_{al de}[b][z] = sum over colour of A[al][b] conj(B[de][z]).
@@ -441,12 +502,13 @@ __device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt,
   // G^{ud} (A = u) and its lane transpose G^{du} (A = d; C g_k is symmetric)
 #pragma unroll 1
   for (int g = 0; g < 3; g++) {
-    Cx<R> q[9];
+    Cx<R> q[9], D[9];
     diquark_G(row, kU, kD, c_delta_sink[g], xp, yp, q);
     const DiquarkLane dl = unpack_diquark_lane(g == 0 ? lt.delta[0] : g == 1 ? lt.delta[1] : lt.delta[2]);
-    part(g, 0, cscale(diquark_eval<true, true>(q, row, kU, dl, l, mask, -4, 0, 2, -2, 4, 0), third));
-    diquark_transpose<R>(q, l, mask, R(1));
-    part(g, 1, cscale(diquark_eval<true, true>(q, row, kD, dl, l, mask, -4, 0, 2, -2, 4, 0), third));
+    diquark_D(q, R(4 * dl.sN), mask, g == 2 ? 1 : 0, D);  // cN = 4, cL = 0
+    part(g, 0, cscale(diquark_eval<true, true>(q, row, kU, dl, l, mask, -4, 0, 2, -2, D), third));
+    diquark_transpose<R>(q, l, mask, R(1));  // G^{du}; its type-a sum is (+1)(tau = +1) D
+    part(g, 1, cscale(diquark_eval<true, true>(q, row, kD, dl, l, mask, -4, 0, 2, -2, D), third));
   }
   // G^{uu} (pair 0: Delta+ and Delta++) and G^{dd} (pair 1: Delta0 and Delta-)
 #pragma unroll 1
@@ -488,7 +550,7 @@ __device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt,
       Cx<R> iso12 = diquark_slots<true, true>(q, row, O, dl, l, mask, 0, 2, 0, -2);
       Cx<R> iso32 = diquark_slots<true, true>(q, row, X, dl, l, mask, -1, 1, 1, -1);
       Cx<R> D[9];
-      diquark_D(q, R(dl.sN + dl.sL), mask, D);  // cN = 1, cL = -1 for both groups
+      diquark_D(q, R(dl.sN + dl.sL), mask, g == 2 ? 1 : 0, D);  // cN = 1, cL = -1 for both groups
       iso12 = iso12 + diquark_typea(D, row, O, l);
       iso32 = iso32 + diquark_typea(D, row, X, l);
       out(g, pair, part_get(g, pair) + cscale(iso12, third));
@@ -514,30 +576,46 @@ __device__ __forceinline__ void light_nucleon_site(const Row& row, const LaneTab
   const R s_nr = R((int)(lt.lg5 & 3u) - 1), s_rn = R((int)((lt.lg5 >> 2) & 3u) - 1);
   const R s_rr = R((int)((lt.lg5 >> 4) & 3u) - 1);
   if (ntor) {
-    Cx<R> g[9];
-    diquark_G(row, kU, kD, c_nuc_sink, l >> 2, l & 3, g);  // sink C g5
+    Cx<R> g[9], D[9];
+    diquark_G_ct<0>(row, kU, kD, l >> 2, l & 3, g);  // sink C g5
     const DiquarkLane dl = unpack_diquark_lane(lt.light[0]);
-    const Cx<R> p = diquark_eval<true, false>(g, row, kU, dl, l, mask, -1, 0, 0, 0, 1, 0);
+    constexpr int l0 = typea_lane(kLightLane[0]);
+    diquark_D(g, R(dl.sN), mask, l0, D);
+    const Cx<R> p = diquark_eval<true, false>(g, row, kU, dl, l, mask, -1, 0, 0, 0, D);
     diquark_transpose<R>(g, l, mask, R(-1));
-    const Cx<R> n = diquark_eval<true, false>(g, row, kD, dl, l, mask, -1, 0, 0, 0, 1, 0);
+    const Cx<R> n = diquark_eval<true, false>(g, row, kD, dl, l, mask, -1, 0, 0, 0, D);
     out(0, 0, cscale(shfl_xor16(p, 2, mask), s_nr));
     out(0, 1, cscale(shfl_xor16(n, 2, mask), s_nr));
   }
   if (rton || rtor) {
     Cx<R> g[9];
-    diquark_G(row, kU, kD, c_c_sink, l >> 2, l & 3, g);  // sink C
+    diquark_G_ct<4>(row, kU, kD, l >> 2, l & 3, g);  // sink C
     const DiquarkLane drn = unpack_diquark_lane(lt.light[1]), drr = unpack_diquark_lane(lt.light[2]);
+    constexpr int l0rn = typea_lane(kLightLane[1]), l0rr = typea_lane(kLightLane[2]);
     Cx<R> prn = czero<R>(), prr = czero<R>();
-    if (rton) prn = diquark_eval<true, false>(g, row, kU, drn, l, mask, -1, 0, 0, 0, 1, 0);
-    if (rtor) prr = diquark_eval<true, false>(g, row, kU, drr, l, mask, -1, 0, 0, 0, 1, 0);
+    {
+      Cx<R> D[9];
+      if (rton) {
+        diquark_D(g, R(drn.sN), mask, l0rn, D);
+        prn = diquark_eval<true, false>(g, row, kU, drn, l, mask, -1, 0, 0, 0, D);
+      }
+      if (rtor) {
+        diquark_D(g, R(drr.sN), mask, l0rr, D);
+        prr = diquark_eval<true, false>(g, row, kU, drr, l, mask, -1, 0, 0, 0, D);
+      }
+    }
     diquark_transpose<R>(g, l, mask, R(kCT[0]));
     if (rton) {
-      const Cx<R> n = diquark_eval<true, false>(g, row, kD, drn, l, mask, -1, 0, 0, 0, 1, 0);
+      Cx<R> D[9];
+      diquark_D(g, R(drn.sN), mask, l0rn, D);
+      const Cx<R> n = diquark_eval<true, false>(g, row, kD, drn, l, mask, -1, 0, 0, 0, D);
       out(1, 0, cscale(shfl_xor16(prn, 8, mask), s_rn));
       out(1, 1, cscale(shfl_xor16(n, 8, mask), s_rn));
     }
     if (rtor) {
-      const Cx<R> n = diquark_eval<true, false>(g, row, kD, drr, l, mask, -1, 0, 0, 0, 1, 0);
+      Cx<R> D[9];
+      diquark_D(g, R(drr.sN), mask, l0rr, D);
+      const Cx<R> n = diquark_eval<true, false>(g, row, kD, drr, l, mask, -1, 0, 0, 0, D);
       out(2, 0, cscale(shfl_xor16(prr, 10, mask), s_rr));
       out(2, 1, cscale(shfl_xor16(n, 10, mask), s_rr));
     }
