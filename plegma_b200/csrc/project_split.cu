@@ -19,12 +19,16 @@
 // over site splits and the un-scaling are FP64 (k_split_reduce), in a fixed
 // order.
 //
-// CTA: 256 threads, one N-tile of NT components (2NT TMEM columns), a range
-// of 64-site k-steps.  Per k-step: thread 0 bulk-copies the two 16 KB phase
-// tiles (prebuilt in the swizzled layout) into the stage; all threads load
-// c (coalesced along x), split it and store it swizzled; one thread issues
-// 3 x 4 (x 2 N-halves) tcgen05.mma and commits to the stage's mbarrier,
-// which frees the stage two k-steps later.
+// CTA: 15 converter warps and one copy/MMA warp, one N-tile of NT
+// components (2NT TMEM columns), a range of 64-site k-steps.  Per k-step the
+// converters load c (coalesced along x, 16 bytes per thread and component),
+// split it and store it swizzled into one of two B stages, then each warp
+// arrives on the stage's "full" mbarrier; the MMA thread bulk-copies the two
+// 16 KB phase tiles (prebuilt in the swizzled layout) one k-step ahead into
+// one of three A stages, waits for A and B, issues 3 x 4 (x 2 N-halves)
+// tcgen05.mma and commits to the stage's "done" mbarrier, which the
+// converters wait for before refilling that stage two k-steps later.  No
+// block-wide barrier inside the k-loop.
 #include <cuda_fp16.h>
 
 #include "kernels.cuh"
@@ -36,12 +40,21 @@ namespace p2 {
 
 namespace {
 
-constexpr int kThreads = 512;  // 16 warps: producers of B (all), TMA/MMA issue (thread 0), epilogue
+constexpr int kConvWarps = 15;         // converter warps
+constexpr int kThreads = 512;          // + the copy / MMA warp (16 warps; all 16 run the epilogue)
 constexpr int kKS = 64;                   // sites per k-step
 constexpr int kATile = 128 * kKS * 2;     // bytes of one 128 x 64 FP16 tile
 
 __host__ __device__ constexpr int b_tile_bytes(int NT) { return 2 * NT * kKS * 2; }
-__host__ __device__ constexpr int stage_bytes(int NT) { return 2 * kATile + 2 * b_tile_bytes(NT); }
+// phase (A) stages: three when they fit beside the two B stages, so that each
+// k-step's phase copy is issued one k-step ahead of its MMAs
+constexpr int kSmemMax = 232448;
+__host__ __device__ constexpr int a_stages(int NT) {
+  return 2 * 2 * b_tile_bytes(NT) + 3 * 2 * kATile + 64 + 1024 <= kSmemMax ? 3 : 2;
+}
+__host__ __device__ constexpr int smem_bytes(int NT) {
+  return 2 * 2 * b_tile_bytes(NT) + a_stages(NT) * 2 * kATile + 64 + 1024;
+}
 __host__ __device__ constexpr int tmem_cols(int NT) {
   return 2 * NT <= 32 ? 32 : 2 * NT <= 64 ? 64 : 2 * NT <= 128 ? 128 : 2 * NT <= 256 ? 256 : 512;
 }
@@ -79,18 +92,20 @@ template <int NT>
 __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmArgs a) {
   constexpr int NR = 2 * NT;                 // B rows (Re, Im per component)
   constexpr int BT = b_tile_bytes(NT);
-  constexpr int ST = stage_bytes(NT);
+  constexpr int NA = a_stages(NT);
   constexpr int NH = NR > 256 ? 2 : 1;       // MMAs per product (N <= 256 each)
   constexpr int NM = NR / NH;
   constexpr uint32_t IDESC = tc::idesc_f16_f32(128, NM);
   constexpr int TCOLS = tmem_cols(NT);
-  constexpr int JN = NT / 16;                // components per producer thread
+  constexpr int JN = (NT + kConvWarps - 1) / kConvWarps;  // components per converter thread
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // the dynamic window is only guaranteed 16-byte aligned: round up to 1024
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* fullA = (uint64_t*)(smem + 2 * ST);
-  uint64_t* done = fullA + 2;
-  uint32_t* tslot = (uint32_t*)(done + 2);
+  unsigned char* sA = smem + 2 * 2 * BT;  // NA phase stages of 2 kATile (hi, lo) after the two B stages
+  uint64_t* fullA = (uint64_t*)(sA + NA * 2 * kATile);
+  uint64_t* done = fullA + 3;
+  uint64_t* fullB = done + 2;
+  uint32_t* tslot = (uint32_t*)(fullB + 2);
   int* flag = (int*)(tslot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -105,10 +120,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
     tc::tmem_relinquish();
   }
   if (tid == 0) {
-    tc::mbar_init(&fullA[0], 1);
-    tc::mbar_init(&fullA[1], 1);
-    tc::mbar_init(&done[0], 1);
-    tc::mbar_init(&done[1], 1);
+    for (int j = 0; j < NA; j++) tc::mbar_init(&fullA[j], 1);
+    for (int j = 0; j < 2; j++) {
+      tc::mbar_init(&done[j], 1);
+      tc::mbar_init(&fullB[j], kConvWarps);
+    }
     tc::fence_mbar_init();
     *flag = 0;
   }
@@ -116,95 +132,40 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = *tslot;
-
-  // producer role: site pair sp (sites 2sp, 2sp+1 of the k-step), components kg + 16j
-  const int sp = tid & 31, kg = tid >> 5;
-  float sc[JN];
-#pragma unroll
-  for (int j = 0; j < JN; j++) {
-    const int k = k0 + kg + 16 * j;
-    sc[j] = 0.f;
-    if (k < a.K) {
-      const float mx = __int_as_float(a.cmax[(long long)tau * a.K + k]);
-      int e = 0;
-      if (mx > 0.f) frexpf(mx, &e);
-      sc[j] = ldexpf(1.f, 14 - e);
-    }
-  }
-  const Cx<float>* cb = (const Cx<float>*)a.c + (long long)tau * a.K * a.V3;
   const unsigned char* Ab = (const unsigned char*)a.A + (long long)mt * a.nkstep * 2 * kATile;
-
-  int issued = -1;  // last k-step whose phase copy thread 0 issued
   bool failed = false;
-  // B values of the current k-step and the next one (register double buffer:
-  // the global loads of step i+1 are in flight while step i is split and fed
-  // to the tensor cores)
-  Cx<float> cur[JN][2], nxt[JN][2];
-  auto load_b = [&](int ks, Cx<float> (&r)[JN][2]) {
-    const long long x = (long long)ks * kKS + 2 * sp;
-#pragma unroll
-    for (int j = 0; j < JN; j++) {
-      const int k = k0 + kg + 16 * j;
-      r[j][0] = czero<float>();
-      r[j][1] = czero<float>();
-      if (k < a.K) {
-        const Cx<float>* src = cb + (long long)k * a.V3 + x;
-        if (x < a.V3) r[j][0] = src[0];
-        if (x + 1 < a.V3) r[j][1] = src[1];
-      }
-    }
-  };
-  if (nk > 0) load_b(ks0, cur);
-  for (int i = 0; i < nk; i++) {
-    const int s = i & 1;
-    unsigned char* st = smem + s * ST;
-    if (i + 1 < nk) load_b(ks0 + i + 1, nxt);
-    bool bad = false;
-    if (i >= 2) bad = !tc::mbar_wait(&done[s], ((i >> 1) - 1) & 1);
-    if (__syncthreads_or(bad || *flag)) {
-      failed = true;
-      break;
-    }
-    const int ks = ks0 + i;
-    if (tid == 0) {
-      tc::mbar_expect_tx(&fullA[s], 2 * kATile);
-      tc::bulk_g2s(st, Ab + (long long)ks * 2 * kATile, 2 * kATile, &fullA[s]);
-      issued = i;
-    }
-    // B: split c into hi/lo FP16, Re and Im rows per component
-    unsigned char* Bh = st + 2 * kATile;
-    unsigned char* Bl = Bh + BT;
-#pragma unroll
-    for (int j = 0; j < JN; j++) {
-      const int kk = kg + 16 * j;
-      const Cx<float> v0 = cur[j][0], v1 = cur[j][1];
-      const float r0 = v0.x * sc[j], i0 = v0.y * sc[j], r1 = v1.x * sc[j], i1 = v1.y * sc[j];
-      const __half2 hr = __floats2half2_rn(r0, r1);
-      const __half2 hi_ = __floats2half2_rn(i0, i1);
-      const float2 fr = __half22float2(hr), fi = __half22float2(hi_);
-      const __half2 lr = __floats2half2_rn(r0 - fr.x, r1 - fr.y);
-      const __half2 li = __floats2half2_rn(i0 - fi.x, i1 - fi.y);
-      const uint32_t ore = tc::sw128_offset(2 * kk, 2 * sp);
-      const uint32_t oim = tc::sw128_offset(2 * kk + 1, 2 * sp);
-      *(__half2*)(Bh + ore) = hr;
-      *(__half2*)(Bh + oim) = hi_;
-      *(__half2*)(Bl + ore) = lr;
-      *(__half2*)(Bl + oim) = li;
-    }
-#pragma unroll
-    for (int j = 0; j < JN; j++) {
-      cur[j][0] = nxt[j][0];
-      cur[j][1] = nxt[j][1];
-    }
-    tc::fence_proxy_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      if (!tc::mbar_wait(&fullA[s], (i >> 1) & 1)) {
-        *flag = 1;
-      } else {
+
+  if (warp == kConvWarps) {
+    // ---- copy / MMA warp: lane 0 ----
+    if (lane == 0 && nk > 0) {
+      int issued = -1, committed = -1;
+      auto issue_a = [&](int i) {  // phase tiles of k-step i into A stage i % NA
+        const int sa = i % NA;
+        tc::mbar_expect_tx(&fullA[sa], 2 * kATile);
+        tc::bulk_g2s(sA + sa * 2 * kATile, Ab + (long long)(ks0 + i) * 2 * kATile, 2 * kATile, &fullA[sa]);
+        issued = i;
+      };
+      issue_a(0);
+      for (int i = 0; i < nk && !failed; i++) {
+        // the phase copy of k-step `next` (one k-step ahead with three A
+        // stages, this k-step with two) reuses the stage of k-step next - NA,
+        // whose MMAs must be complete
+        const int next = i + NA - 2;
+        if (next < nk && next > issued) {
+          if (next >= NA && !tc::mbar_wait(&done[(next - NA) & 1], ((next - NA) >> 1) & 1)) {
+            failed = true;
+            break;
+          }
+          issue_a(next);
+        }
+        const int s = i & 1;
+        if (!tc::mbar_wait(&fullA[i % NA], (i / NA) & 1) || !tc::mbar_wait(&fullB[s], (i >> 1) & 1)) {
+          failed = true;
+          break;
+        }
         tc::tc_fence_after();
-        const uint32_t a_hi = tc::smem_u32(st), a_lo = a_hi + kATile;
-        const uint32_t b_hi = tc::smem_u32(Bh), b_lo = tc::smem_u32(Bl);
+        const uint32_t a_hi = tc::smem_u32(sA + (i % NA) * 2 * kATile), a_lo = a_hi + kATile;
+        const uint32_t b_hi = tc::smem_u32(smem + s * 2 * BT), b_lo = b_hi + BT;
 #pragma unroll
         for (int kk = 0; kk < kKS / 16; kk++) {
 #pragma unroll
@@ -219,19 +180,100 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
           }
         }
         tc::mma_commit(&done[s]);
+        committed = i;
+      }
+      // the accumulators are complete (or, after a failure, no MMA or phase
+      // copy is still in flight) before the block moves on
+      if (committed >= 0 && !tc::mbar_wait(&done[committed & 1], (committed >> 1) & 1)) failed = true;
+      if (failed) {
+        *flag = 1;
+        for (int j = max(0, issued - NA + 1); j <= issued; j++)
+          tc::mbar_wait(&fullA[j % NA], (j / NA) & 1, 1LL << 22);
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---- converters: site pair sp (sites 2sp, 2sp+1 of the k-step), components kg + 15 j ----
+    const int sp = tid & 31, kg = tid >> 5;
+    float sc[JN];
+#pragma unroll
+    for (int j = 0; j < JN; j++) {
+      const int k = k0 + kg + kConvWarps * j;
+      sc[j] = 0.f;
+      if (kg + kConvWarps * j < NT && k < a.K) {
+        const float mx = __int_as_float(a.cmax[(long long)tau * a.K + k]);
+        int e = 0;
+        if (mx > 0.f) frexpf(mx, &e);
+        sc[j] = ldexpf(1.f, 14 - e);
+      }
+    }
+    const Cx<float>* cb = (const Cx<float>*)a.c + (long long)tau * a.K * a.V3;
+    const bool even = (a.V3 & 1) == 0;  // site pairs 16-byte aligned
+    // B values of two consecutive k-steps (register double buffer, the two
+    // halves swapping roles every k-step: the loads of step i + 1 stay in
+    // flight while step i is split)
+    float4 b0[JN], b1[JN];
+    auto load_b = [&](int ks, float4 (&r)[JN]) {
+      const long long x = (long long)ks * kKS + 2 * sp;
+#pragma unroll
+      for (int j = 0; j < JN; j++) {
+        const int k = k0 + kg + kConvWarps * j;
+        r[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (kg + kConvWarps * j < NT && k < a.K && x < a.V3) {
+          const Cx<float>* src = cb + (long long)k * a.V3 + x;
+          if (even) {
+            r[j] = *reinterpret_cast<const float4*>(src);
+          } else {
+            r[j].x = src[0].x;
+            r[j].y = src[0].y;
+            if (x + 1 < a.V3) {
+              r[j].z = src[1].x;
+              r[j].w = src[1].y;
+            }
+          }
+        }
+      }
+    };
+    // one k-step; returns true when a wait timed out
+    auto step = [&](int i, const float4 (&cur)[JN], float4 (&nxt)[JN]) -> bool {
+      const int s = i & 1;
+      if (i + 1 < nk) load_b(ks0 + i + 1, nxt);
+      if (i >= 2 && !tc::mbar_wait(&done[s], ((i >> 1) - 1) & 1)) return true;
+      unsigned char* Bh = smem + s * 2 * BT;
+      unsigned char* Bl = Bh + BT;
+#pragma unroll
+      for (int j = 0; j < JN; j++) {
+        const int kk = kg + kConvWarps * j;
+        if (kk >= NT) break;
+        const float4 v = cur[j];
+        const float r0 = v.x * sc[j], i0 = v.y * sc[j], r1 = v.z * sc[j], i1 = v.w * sc[j];
+        const __half2 hr = __floats2half2_rn(r0, r1);
+        const __half2 hi_ = __floats2half2_rn(i0, i1);
+        const float2 fr = __half22float2(hr), fi = __half22float2(hi_);
+        const __half2 lr = __floats2half2_rn(r0 - fr.x, r1 - fr.y);
+        const __half2 li = __floats2half2_rn(i0 - fi.x, i1 - fi.y);
+        const uint32_t ore = tc::sw128_offset(2 * kk, 2 * sp);
+        const uint32_t oim = tc::sw128_offset(2 * kk + 1, 2 * sp);
+        *(__half2*)(Bh + ore) = hr;
+        *(__half2*)(Bh + oim) = hi_;
+        *(__half2*)(Bl + ore) = lr;
+        *(__half2*)(Bl + oim) = li;
+      }
+      tc::fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&fullB[s]);
+      return false;
+    };
+    if (nk > 0) load_b(ks0, b0);
+    for (int i = 0; i < nk; i += 2) {
+      if (*(volatile int*)flag || step(i, b0, b1) || (i + 1 < nk && step(i + 1, b1, b0))) {
+        failed = true;
+        break;
       }
     }
   }
-  if (!failed && nk > 0) {
-    const int last = nk - 1;
-    bool bad = !tc::mbar_wait(&done[last & 1], (last >> 1) & 1);
-    failed = __syncthreads_or(bad || *flag);
-  } else {
-    failed = __syncthreads_or(failed || *flag);
-  }
+  failed = __syncthreads_or(failed || *(volatile int*)flag);
   if (failed) {
-    // let any phase copy still in flight land before the CTA exits
-    if (tid == 0 && issued >= 0) tc::mbar_wait(&fullA[issued & 1], (issued >> 1) & 1, 1LL << 22);
     if (tid == 0) atomicExch(a.err, 1);
   } else {
     tc::tc_fence_after();
@@ -300,7 +342,7 @@ __global__ void k_split_reduce(const SplitReduceArgs a) {
 
 template <int NT>
 cudaError_t launch_nt(const SplitGemmArgs& a, cudaStream_t s) {
-  const int smem = stage_bytes(NT) * 2 + 64 + 1024;
+  const int smem = smem_bytes(NT);
   cudaError_t e = ensure_smem((const void*)k_project_split<NT>, smem);
   if (e != cudaSuccess) return e;
   dim3 grid(a.ntile * a.nmtile, a.nsplit, a.ntau);
@@ -310,7 +352,19 @@ cudaError_t launch_nt(const SplitGemmArgs& a, cudaStream_t s) {
 
 }  // namespace
 
-int project_split_smem_bytes(int NT) { return stage_bytes(NT) * 2 + 64 + 1024; }
+int project_split_smem_bytes(int NT) {
+  switch (NT) {
+    case 16: return smem_bytes(16);
+    case 32: return smem_bytes(32);
+    case 48: return smem_bytes(48);
+    case 64: return smem_bytes(64);
+    case 80: return smem_bytes(80);
+    case 96: return smem_bytes(96);
+    case 112: return smem_bytes(112);
+    case 128: return smem_bytes(128);
+    default: return smem_bytes(144);
+  }
+}
 
 cudaError_t launch_build_phases(const PhaseBuildArgs& a, cudaStream_t s) {
   const long long n = (long long)a.nmtile * a.nkstep * 128 * kKS;
