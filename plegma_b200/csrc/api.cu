@@ -8,6 +8,9 @@
 #include <string>
 #include <vector>
 
+#include <emmintrin.h>
+#include <omp.h>
+
 #include "../../include/plegma2pt.h"
 #include "kernels.cuh"
 #include "ctx.h"
@@ -141,6 +144,35 @@ Stager::Stager(p2_ctx* ctx, const p2_prop* pp, const p2_request* rr, const Work&
 
 namespace {
 size_t esz_of(const p2_prop& p) { return p.precision == P2_FP64 ? 16 : 8; }
+
+// Binary exponent e with max |Re|, |Im| < 2^e over component row 0 of slice j
+// of an FP64 host view (0 for an all-zero row): the host conversion stores the
+// slice times 2^-e, so its entries stay far inside FP32's range.
+int host_slice_exponent(const p2_prop& p, int j, long long V3) {
+  const double* row = (const double*)p.data + (size_t)j * V3 * 2;
+  double m = 0.0;
+  for (long long i = 0; i < 2 * V3; i++) m = std::max(m, std::fabs(row[i]));
+  int e = 0;
+  if (m > 0.0) std::frexp(m, &e);
+  return e;
+}
+
+// dst[i] = (float)(src[i] * scale) for n doubles; scale a power of two, so
+// the product is exact and the rounding is that of the plain conversion.
+// Streaming stores when dst is 16-byte aligned (the pinned staging is read
+// next by the copy engine, not by this core).
+void convert_row(const double* src, float* dst, size_t n, double scale) {
+  size_t i = 0;
+  if (((uintptr_t)dst & 15) == 0) {
+    const __m128d sc = _mm_set1_pd(scale);
+    for (; i + 4 <= n; i += 4) {
+      const __m128 lo = _mm_cvtpd_ps(_mm_mul_pd(_mm_loadu_pd(src + i), sc));
+      const __m128 hi = _mm_cvtpd_ps(_mm_mul_pd(_mm_loadu_pd(src + i + 2), sc));
+      _mm_stream_ps(dst + i, _mm_movelh_ps(lo, hi));
+    }
+  }
+  for (; i < n; i++) dst[i] = (float)(src[i] * scale);
+}
 }  // namespace
 
 // PropXf code of a view's load-time transform on global time t.
@@ -173,6 +205,14 @@ p2_status Stager::prepare(double* const* outs) {
         if (esz_max[f])
           P2_TRY(c, (f ? c->stage_d2[slot] : c->stage_u2[slot]).ensure((size_t)144 * w.max_n * c->V3 * esz_max[f]),
                  "staging alloc");
+    if (cvt32)
+      for (int hs = 0; hs < p2_ctx::kHostSlots; hs++) {
+        for (int f = 0; f < 2; f++)
+          P2_TRY(c, (f ? c->hstage_d[hs] : c->hstage_u[hs]).ensure((size_t)144 * w.max_n * c->V3 * 8),
+                 "pinned conversion buffer");
+        if (!c->hcopied[hs])
+          P2_TRY(c, cudaEventCreateWithFlags(&c->hcopied[hs], cudaEventDisableTiming), "conversion events");
+      }
     if (!c->copy_stream) {
       P2_TRY(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "copy stream");
       for (int i = 0; i < 2; i++) {
@@ -226,6 +266,21 @@ p2_status Stager::prepare(double* const* outs) {
       sd.xf[1] = prop_xf_code(props[r.prop_d], t);
     }
   }
+  if (cvt32) {
+    std::vector<int> conv;  // slices of the chunks converted on the host
+    for (size_t ci = 0; ci < w.chunks.size(); ci++)
+      if (converts((int)ci))
+        for (int i = 0; i < w.chunks[ci].n; i++) conv.push_back(w.chunks[ci].s0 + i);
+    const long long n = (long long)conv.size();
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long q = 0; q < 2 * n; q++) {
+      const int si = conv[q >> 1];
+      const SliceRef& s = w.sl[si];
+      const int f = (int)(q & 1);
+      const p2_request& r = reqs[s.req];
+      h[si].eh[f] = host_slice_exponent(props[f ? r.prop_d : r.prop_u], f ? s.jd : s.ju, c->V3);
+    }
+  }
   P2_TRY(c, c->sdesc.ensure(bytes), "descriptor alloc");
   P2_TRY(c, cudaMemcpyAsync(c->sdesc.p, h, bytes, cudaMemcpyHostToDevice, c->stream), "descriptor upload");
   if (!c->capturing) P2_TRY(c, cudaEventRecord(c->sdesc_copied, c->stream), "descriptor event");
@@ -238,6 +293,40 @@ p2_status Stager::issue(int ci) {
   const int slot = ci & 1;
   const Chunk& ch = w.chunks[ci];
   P2_TRY(c, cudaStreamWaitEvent(c->copy_stream, c->consumed[slot], 0), "copy wait");
+  if (converts(ci)) {
+    // the previous upload from this pinned slot has finished; convert the
+    // chunk into it (all host threads) and upload each flavour in one copy
+    const int hs = host_slot(ci);
+    P2_TRY(c, cudaEventSynchronize(c->hcopied[hs]), "conversion buffer reuse");
+    const p2::SliceDesc* h = (const p2::SliceDesc*)c->sdesc_host + ch.s0;
+    const long long V3 = c->V3;
+    const long long rows = 2LL * 144 * ch.n;
+#pragma omp parallel
+    {
+#pragma omp for schedule(static)
+      for (long long q = 0; q < rows; q++) {
+        const int f = (int)(q / (144LL * ch.n));
+        const int comp = (int)((q / ch.n) % 144), i = (int)(q % ch.n);
+        const SliceRef& s = w.sl[ch.s0 + i];
+        const p2_request& r = reqs[s.req];
+        const p2_prop& p = props[f ? r.prop_d : r.prop_u];
+        const double* src = (const double*)p.data + ((size_t)comp * p.nt + (f ? s.jd : s.ju)) * V3 * 2;
+        float* dst = (float*)(f ? c->hstage_d[hs] : c->hstage_u[hs]).p + ((size_t)comp * ch.n + i) * V3 * 2;
+        convert_row(src, dst, (size_t)V3 * 2, std::ldexp(1.0, -h[i].eh[f]));
+      }
+      _mm_sfence();
+    }
+    ProfScope ps(c, "h2d_upload", c->copy_stream);
+    for (int f = 0; f < 2; f++)
+      P2_TRY(c,
+             cudaMemcpyAsync((f ? c->stage_d2[slot] : c->stage_u2[slot]).p,
+                             (f ? c->hstage_d[hs] : c->hstage_u[hs]).p, (size_t)144 * ch.n * V3 * 8,
+                             cudaMemcpyHostToDevice, c->copy_stream),
+             "host propagator upload");
+    P2_TRY(c, cudaEventRecord(c->hcopied[hs], c->copy_stream), "copy event");
+    P2_TRY(c, cudaEventRecord(c->copied[slot], c->copy_stream), "copy event");
+    return P2_OK;
+  }
   ProfScope ps(c, "h2d_upload", c->copy_stream);
   for (int f = 0; f < 2; f++) {
     // runs of slices that are consecutive in one host view: one contiguous
@@ -589,6 +678,11 @@ p2_status p2_ctx_destroy(p2_ctx* c) {
     c->stage_d2[i].release();
     if (c->copied[i]) cudaEventDestroy(c->copied[i]);
     if (c->consumed[i]) cudaEventDestroy(c->consumed[i]);
+  }
+  for (int i = 0; i < p2_ctx::kHostSlots; i++) {
+    c->hstage_u[i].release();
+    c->hstage_d[i].release();
+    if (c->hcopied[i]) cudaEventDestroy(c->hcopied[i]);
   }
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   c->prof_collect();

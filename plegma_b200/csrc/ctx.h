@@ -11,6 +11,26 @@
 
 namespace p2host {
 
+// Pinned host buffer (cudaMallocHost), grown on demand.
+struct HostBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= n) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+    cudaError_t e = cudaMallocHost(&p, bytes);
+    if (e == cudaSuccess) n = bytes;
+    return e;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
 struct DevBuf {
   void* p = nullptr;
   size_t n = 0;
@@ -66,6 +86,11 @@ struct p2_ctx {
   // host-resident propagators: two staging slots per flavour, uploaded on a
   // copy stream while the previous chunk is contracted
   p2host::DevBuf stage_u2[2], stage_d2[2];
+  // host-side FP32 conversion of host views (split form): pinned buffers and
+  // the events of their last upload
+  static constexpr int kHostSlots = 3;
+  p2host::HostBuf hstage_u[kHostSlots], hstage_d[kHostSlots];
+  cudaEvent_t hcopied[kHostSlots] = {nullptr, nullptr, nullptr};
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
   // split form: phase tiles, per-slice exponents, component maxima, tables, partials, error flag
@@ -169,6 +194,17 @@ struct Stager {
   const p2_request* reqs;
   const Work& w;
   bool host = false;
+  // split form with every view on the host in FP64: the host converts each
+  // chunk to FP32 (times 2^-eh per slice and flavour, exact) into pinned
+  // buffers and uploads half the bytes
+  bool cvt32 = false;
+  // with cvt32, every kRawEvery-th chunk (from the first) goes up unconverted
+  // in FP64 instead: the link has room while the host cores convert, and the
+  // first upload starts without waiting for a conversion
+  static constexpr int kRawEvery = 6;
+  bool converts(int ci) const { return cvt32 && ci % kRawEvery != 0; }
+  // pinned buffer slot of converted chunk ci (the converted chunks before it, modulo the slots)
+  int host_slot(int ci) const { return (ci - (ci + kRawEvery - 1) / kRawEvery) % p2_ctx::kHostSlots; }
   p2::SliceDesc* dsl = nullptr;
   Stager(p2_ctx* ctx, const p2_prop* pp, const p2_request* rr, const Work& work);
   // outs[req]: device result pointer of each request (indexed like reqs)

@@ -25,6 +25,7 @@ struct SliceDesc {
   int totalT;              // window of the request (result layout)
   int x0[3];               // spatial source position of the request
   int xf[2];               // load-time transform of the u and d slice (prop_xf_code)
+  int eh[2];               // staged u, d entries are the view's times 2^-eh (host-converted FP32 staging), else 0
 };
 
 // Load-time propagator transform of one slice, see P2_PROP_* in plegma2pt.h:

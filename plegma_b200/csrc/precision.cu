@@ -171,6 +171,14 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
     if (props[r.prop_u].precision != props[r.prop_d].precision)
       return c->fail(P2_ERR_UNSUPPORTED, "u and d must share a precision");
   }
+  // FP64 views that all live on the host are converted to FP32 on the host
+  // (the contraction computes in FP32 either way; half the bytes cross PCIe)
+  bool all_host64 = true;
+  for (int q = 0; q < nidx; q++) {
+    const p2_request& r = reqs[idx[q]];
+    for (int pi : {r.prop_u, r.prop_d})
+      all_host64 = all_host64 && props[pi].location == P2_HOST && props[pi].precision == P2_FP64;
+  }
   const int fp32_in = props[r0.prop_u].precision == P2_FP32;
   const int K = pl.K;
   int nmtile = 0, nkstep = 0;
@@ -179,7 +187,8 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
 
   // chunk of slices: FP32 position buffer within the workspace budget
   const size_t per_slice = (size_t)K * c->V3 * 8;
-  const int tc = (int)std::max<size_t>(1, std::min<size_t>(c->ws_budget / std::max<size_t>(per_slice, 1), c->T));
+  int tc = (int)std::max<size_t>(1, std::min<size_t>(c->ws_budget / std::max<size_t>(per_slice, 1), c->T));
+  if (all_host64) tc = std::min(tc, 4);  // short chunks: the host conversion pipeline fills and drains faster
   const Work w = make_work(c, props, reqs, idx, nidx, tc);
   if (w.sl.empty()) return P2_OK;
   const int mx = w.max_n;
@@ -187,6 +196,7 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
   P2_TRY(c, c->expb.ensure((size_t)2 * mx * sizeof(int)), "exponent alloc");
   P2_TRY(c, c->cmaxb.ensure((size_t)mx * K * sizeof(int)), "maxima alloc");
   Stager sg(c, props, reqs, w);
+  sg.cvt32 = all_host64;
   if ((st = sg.prepare(outs)) != P2_OK) return st;
 
   for (int i = 0; i < 2; i++)
@@ -195,9 +205,10 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
     const int n = w.chunks[ci].n;
     const SliceDesc* dsl = sg.desc((int)ci);
     if ((st = sg.wait((int)ci)) != P2_OK) return st;
+    const int chunk_fp32 = fp32_in || sg.converts((int)ci);  // staged in FP32
     {
       ProfScope ps(c, "sample_exponents");
-      p2::SampleArgs sa{dsl, fp32_in, (int)c->V3, n, (int*)c->expb.p};
+      p2::SampleArgs sa{dsl, chunk_fp32, (int)c->V3, n, (int*)c->expb.p};
       P2_TRY(c, p2::launch_sample_exponents(sa, c->stream), "exponent sample");
     }
     P2_TRY(c, cudaMemsetAsync(c->cmaxb.p, 0, (size_t)n * K * sizeof(int), c->stream), "maxima clear");
@@ -213,7 +224,7 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
     a.cmax = (int*)c->cmaxb.p;
     {
       ProfScope ps(c, "contract_f32");
-      P2_TRY(c, p2::launch_contract_f32(a, fp32_in, 2 * c->nsm, c->stream), "contract kernel");
+      P2_TRY(c, p2::launch_contract_f32(a, chunk_fp32, 2 * c->nsm, c->stream), "contract kernel");
     }
     if ((st = sg.release((int)ci)) != P2_OK) return st;
     if ((st = sg.issue((int)ci + 2)) != P2_OK) return st;

@@ -320,11 +320,12 @@ __global__ void k_split_reduce(const SplitReduceArgs a) {
     const float mx = __int_as_float(a.cmax[(long long)tl * a.K + k]);
     int e = 0;
     if (mx > 0.f) frexpf(mx, &e);
-    const int pw = a.kexp[2 * k] * a.exps[2 * tl] + a.kexp[2 * k + 1] * a.exps[2 * tl + 1] - (14 - e);
+    const SliceDesc& sd = a.sl[tl];
+    const int pw = a.kexp[2 * k] * (a.exps[2 * tl] + sd.eh[0]) + a.kexp[2 * k + 1] * (a.exps[2 * tl + 1] + sd.eh[1]) -
+                   (14 - e);
     const double f = ldexp(1.0, pw);
     // S(p) = sum_x c e^{-i p.x}; the source phase: C(p) = e^{i p.x0} S(p), with
     // p.x0 / L reduced exactly in integers per dimension
-    const SliceDesc& sd = a.sl[tl];
     const Cx<double> v = cmul(cx<double>((cr + sg * si) * f, (ci - sg * sr) * f), source_phase(mr + 3, sd.x0, a.L));
     for (int b = 0; b < a.nblocks; b++) {
       const ScatterBlock& B = a.blk[b];

@@ -103,3 +103,26 @@ def test_split_delta_batched_set():
     err = per_t_error(out, what, 7, moms, ref, taus)
     assert err.max() < TOL, err
     ctx.close()
+
+
+@pytest.mark.parametrize("decay", [0.5, 15.0])
+def test_split_host_propagators_converted_on_host(decay):
+    """FP64 propagators on the host are converted to FP32 by the library
+    (each slice times an exact power of two) before the upload.  With decay
+    15 the entries fall to ~1e-46 across the window, below FP32's normal
+    range, so the per-slice scale is what keeps them: the result must equal
+    the device-resident FP64 run and meet the 1e-6 bound against the oracle,
+    with the window wrapping through t = 0."""
+    ctx = p2.Context((4, 3, 2, 8))
+    src = (1, 2, 0, 5)
+    bufs = device_props(ctx, [(33, 0), (33, 1)], t0=src[3], decay=decay)
+    what = p2.NUCLEON_CG5 | p2.MESON_G16
+    moms = p2.mom_list(2)
+    dev, _ = run(ctx, bufs, src, 8, what, moms=moms, mode=p2.P2_SPLIT_FP16)
+    host, _ = run(ctx, bufs, src, 8, what, moms=moms, mode=p2.P2_SPLIT_FP16, host_props=True, host_out=True)
+    assert np.array_equal(dev, host)
+    taus = list(range(8))
+    ref = oracle_blocks(ctx.L, bufs, src, moms, what, taus)
+    err = per_t_error(host, what, 8, moms, ref, taus)
+    assert err.max() < 1e-6, err
+    ctx.close()
