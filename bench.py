@@ -145,7 +145,7 @@ def run_reference(args, rank, world):
 # DRAM bytes (read + write) per site of the dominant kernel, measured with ncu
 # on the 32^3 x 16 case of the same kernel; traffic grows with the sites a
 # launch processes, so it scales to the benchmark's launches
-TRAFFIC_PER_SITE = {("contract_f32", "split"): 6916, ("contract_plain_fp64", "plain"): 9144}
+TRAFFIC_PER_SITE = {("contract_f32", "split"): 6861, ("contract_plain_fp64", "plain"): 9144}
 
 BATCHED = {
     # name: (lattice, sources, window range, |n|^2 max, propagator precision, decay, seed)
@@ -235,13 +235,16 @@ def run_batched(name, stream, steps, warmup, forms=("split",)):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="auto", choices=["auto", "split", "plain"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-source graph runs")
+    ap.add_argument("--tune-cache", default=None,
+                    help="tab-separated launch-shape cache: read if present, written after tuning "
+                         "(lets a profiler run skip the tuning launches)")
     ap.add_argument("--lattice", default=None,
                     help="Lx,Ly,Lz,Lt override for small profiling cases (not the benchmark workload)")
     args = ap.parse_args()
@@ -269,7 +272,7 @@ def main():
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
-    ctx.tune(True)  # launch shapes timed during the warm-up steps, cached in memory
+    ctx.tune(True, args.tune_cache)  # launch shapes timed during the warm-up steps, cached in memory
 
     seed = SEED + rank
     src = source_for(seed)
