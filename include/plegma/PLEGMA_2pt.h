@@ -611,6 +611,7 @@ class PLEGMA_Correlator {
     r.prop_c = idx[3];
     r.only_st = only_st;
     r.only_ch = only_ch;
+    r.mode = mode;
     const int nd = p2_udsc_datasets(&r, nullptr, 0);
     std::vector<char> text((size_t)64 * (nd + 1), 0);
     p2_udsc_datasets(&r, text.data(), text.size());

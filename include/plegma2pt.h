@@ -256,8 +256,11 @@ int p2_local_taus(p2_ctx* ctx, const p2_prop* props, int nprops, const p2_reques
  * flavour products run in the reference's order, skipping those that need a
  * propagator that is not given (index -1); only_st / only_ch keep only the
  * products containing s / c.  Result: [dataset][tau][mom] complex double,
- * datasets in the order of p2_udsc_datasets.  Plain FP64 form; FP64
- * device-resident propagators. */
+ * datasets in the order of p2_udsc_datasets.  Device-resident propagators:
+ * mode P2_PLAIN_FP64 (FP64 arithmetic, FP64 propagators) or P2_SPLIT_FP16
+ * (FP32 contraction of power-of-two scaled inputs and the hi+lo FP16
+ * tensor-core projection, FP64 or FP32 propagators, per-time-slice error
+ * <= 1e-6 of sum_x |c_d(x,t)|). */
 typedef struct {
   int source[4];
   int totalT;
@@ -268,6 +271,7 @@ typedef struct {
   int only_st, only_ch;
   double* out;
   int out_location;
+  int mode; /* P2_PLAIN_FP64 or P2_SPLIT_FP16 */
 } p2_udsc_request;
 
 /* Dataset names ("proton/Pp_Cg5_Cg5", ...) a request produces, one per line,

@@ -234,4 +234,8 @@ namespace p2 {
 p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request* reqs, const int* idx, int nidx,
                               const p2host::Plan& pl, double* const* outs);
 void precision_release(p2_ctx* c);
+// shared with the split form of the table-driven baryons (udsc.cu)
+p2_status split_prepare_tables(p2_ctx* c, const p2host::Plan& pl, unsigned what, int& nmtile, int& nkstep);
+p2_status split_project(p2_ctx* c, const p2host::Plan& pl, int K, int n, int nmtile, int nkstep, const SliceDesc* dsl,
+                        const int* exps, const int* kexp, const std::vector<ScatterBlock>& blocks);
 }  // namespace p2

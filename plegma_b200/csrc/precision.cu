@@ -100,10 +100,14 @@ PhaseRows phase_rows(const std::vector<int>& moms) {
   return pr;
 }
 
+}  // namespace
+
+namespace p2 {
+
 // Phase tiles, momentum rows and component exponents, rebuilt only when the
 // momentum list or the contraction set changes (the tiles have origin 0, so
-// every source shares them).
-p2_status prepare_tables(p2_ctx* c, const Plan& pl, unsigned what, int& nmtile, int& nkstep) {
+// every source shares them).  what = 0: tiles and rows only.
+p2_status split_prepare_tables(p2_ctx* c, const Plan& pl, unsigned what, int& nmtile, int& nkstep) {
   PhaseRows pr = phase_rows(pl.moms);
   const int nh = (int)pr.reps.size() / 3;
   const int nrows = (int)pr.row_h.size();
@@ -144,7 +148,7 @@ p2_status prepare_tables(p2_ctx* c, const Plan& pl, unsigned what, int& nmtile, 
     if ((st = upload_async(c, c->momrow, mr.data(), mr.size() * sizeof(int), "momentum rows")) != P2_OK) return st;
     c->split_moms_key = pl.moms;
   }
-  if (c->split_what_key != what) {
+  if (what && c->split_what_key != what) {
     std::vector<int> ke = component_exponents(what);
     if ((st = upload_async(c, c->kexp, ke.data(), ke.size() * sizeof(int), "component exponents")) != P2_OK) return st;
     c->split_what_key = what;
@@ -152,9 +156,91 @@ p2_status prepare_tables(p2_ctx* c, const Plan& pl, unsigned what, int& nmtile, 
   return P2_OK;
 }
 
-}  // namespace
-
-namespace p2 {
+// Projection of a chunk's FP32 position buffer c->cbuf ([n][K][V3], maxima in
+// c->cmaxb) on the tensor cores, launch shape from the autotuner, then the
+// FP64 reduction into the results of the slices dsl: per component k the
+// un-scaling exponent is kexp[2k] (exps[2t] + eh_u) + kexp[2k+1] (exps[2t+1] + eh_d).
+p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int nkstep, const SliceDesc* dsl,
+                        const int* exps, const int* kexp, const std::vector<ScatterBlock>& blocks) {
+  // projection GEMM candidates (N-tile width NT <= 144 components = 288
+  // TMEM columns, number of N-tiles, site splits, k-steps per split): the
+  // fewest N-tiles at ~2 waves first, then up to two more N-tiles at 1, 2
+  // and 4 waves
+  std::vector<std::vector<int>> cands;
+  for (int ntile = (K + 143) / 144, extra = 0; extra < 3; ntile++, extra++) {
+    const int NT = ((K + ntile - 1) / ntile + 15) / 16 * 16;
+    if ((ntile - 1) * NT >= K) continue;  // an empty N-tile
+    for (int waves : {2, 1, 4}) {
+      const int per = ntile * nmtile * n;
+      int nsplit = std::min(std::max(1, (waves * c->nsm + per - 1) / per), nkstep);
+      const int ks_per = (nkstep + nsplit - 1) / nsplit;
+      nsplit = (nkstep + ks_per - 1) / ks_per;
+      std::vector<int> v{NT, ntile, nsplit, ks_per};
+      if (std::find(cands.begin(), cands.end(), v) == cands.end()) cands.push_back(v);
+    }
+  }
+  size_t maxpart = 0;
+  for (const auto& v : cands) maxpart = std::max(maxpart, (size_t)v[2] * v[1] * 2 * v[0]);
+  P2_TRY(c, c->fpart.ensure((size_t)n * nmtile * 128 * maxpart * sizeof(float)), "partials alloc");
+  p2::SplitGemmArgs g{};
+  g.c = c->cbuf.p;
+  g.cmax = (const int*)c->cmaxb.p;
+  g.A = c->phaseA.p;
+  g.ntau = n;
+  g.K = K;
+  g.V3 = (int)c->V3;
+  g.nkstep = nkstep;
+  g.nmtile = nmtile;
+  g.part = (float*)c->fpart.p;
+  g.err = (int*)c->errflag.p;
+  auto set = [&](p2::SplitGemmArgs& q, const std::vector<int>& v) {
+    q.NT = v[0];
+    q.ntile = v[1];
+    q.nsplit = v[2];
+    q.ks_per_split = v[3];
+  };
+  char key[160];
+  std::snprintf(key, sizeof(key), "project_split V3=%lld K=%d rows=%d n=%d", c->V3, K, nmtile * 128, n);
+  std::vector<int> pick;
+  P2_TRY(c,
+         tune_choose(c->tuner.get(), key, cands, c->stream, !c->capturing,
+                     [&](const std::vector<int>& v) {
+                       p2::SplitGemmArgs q = g;
+                       set(q, v);
+                       return p2::launch_project_split(q, c->stream);
+                     },
+                     pick),
+         "projection tuning");
+  set(g, pick);
+  const int NT = g.NT, nsplit = g.nsplit;
+  const int ncols = g.ntile * 2 * NT;
+  {
+    ProfScope ps(c, "project_split_tc");
+    P2_TRY(c, p2::launch_project_split(g, c->stream), "tensor-core projection");
+  }
+  p2::SplitReduceArgs rd{};
+  rd.part = (const float*)c->fpart.p;
+  rd.ntau = n;
+  rd.nsplit = nsplit;
+  rd.nmtile = nmtile;
+  rd.ncols = ncols;
+  rd.NT = NT;
+  rd.nmom = pl.nmom;
+  rd.K = K;
+  rd.mom_row = (const int*)c->momrow.p;
+  for (int d = 0; d < 3; d++) rd.L[d] = c->g.L[d];
+  rd.cmax = (const int*)c->cmaxb.p;
+  rd.exps = exps;
+  rd.kexp = kexp;
+  rd.sl = dsl;
+  rd.nblocks = (int)blocks.size();
+  for (size_t b = 0; b < blocks.size(); b++) rd.blk[b] = blocks[b];
+  {
+    ProfScope ps(c, "split_reduce");
+    P2_TRY(c, p2::launch_split_reduce(rd, c->stream), "split reduction");
+  }
+  return P2_OK;
+}
 
 p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request* reqs, const int* idx, int nidx,
                               const Plan& pl, double* const* outs) {
@@ -182,7 +268,7 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
   const int fp32_in = props[r0.prop_u].precision == P2_FP32;
   const int K = pl.K;
   int nmtile = 0, nkstep = 0;
-  p2_status st = prepare_tables(c, pl, what, nmtile, nkstep);
+  p2_status st = split_prepare_tables(c, pl, what, nmtile, nkstep);
   if (st != P2_OK) return st;
 
   // chunk of slices: FP32 position buffer within the workspace budget
@@ -228,83 +314,9 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
     }
     if ((st = sg.release((int)ci)) != P2_OK) return st;
     if ((st = sg.issue((int)ci + 2)) != P2_OK) return st;
-    // projection GEMM candidates (N-tile width NT <= 144 components = 288
-    // TMEM columns, number of N-tiles, site splits, k-steps per split): the
-    // fewest N-tiles at ~2 waves first, then up to two more N-tiles at 1, 2
-    // and 4 waves
-    std::vector<std::vector<int>> cands;
-    for (int ntile = (K + 143) / 144, extra = 0; extra < 3; ntile++, extra++) {
-      const int NT = ((K + ntile - 1) / ntile + 15) / 16 * 16;
-      if ((ntile - 1) * NT >= K) continue;  // an empty N-tile
-      for (int waves : {2, 1, 4}) {
-        const int per = ntile * nmtile * n;
-        int nsplit = std::min(std::max(1, (waves * c->nsm + per - 1) / per), nkstep);
-        const int ks_per = (nkstep + nsplit - 1) / nsplit;
-        nsplit = (nkstep + ks_per - 1) / ks_per;
-        std::vector<int> v{NT, ntile, nsplit, ks_per};
-        if (std::find(cands.begin(), cands.end(), v) == cands.end()) cands.push_back(v);
-      }
-    }
-    size_t maxpart = 0;
-    for (const auto& v : cands) maxpart = std::max(maxpart, (size_t)v[2] * v[1] * 2 * v[0]);
-    P2_TRY(c, c->fpart.ensure((size_t)n * nmtile * 128 * maxpart * sizeof(float)), "partials alloc");
-    p2::SplitGemmArgs g{};
-    g.c = c->cbuf.p;
-    g.cmax = (const int*)c->cmaxb.p;
-    g.A = c->phaseA.p;
-    g.ntau = n;
-    g.K = K;
-    g.V3 = (int)c->V3;
-    g.nkstep = nkstep;
-    g.nmtile = nmtile;
-    g.part = (float*)c->fpart.p;
-    g.err = (int*)c->errflag.p;
-    auto set = [&](p2::SplitGemmArgs& q, const std::vector<int>& v) {
-      q.NT = v[0];
-      q.ntile = v[1];
-      q.nsplit = v[2];
-      q.ks_per_split = v[3];
-    };
-    char key[160];
-    std::snprintf(key, sizeof(key), "project_split V3=%lld K=%d rows=%d n=%d", c->V3, K, nmtile * 128, n);
-    std::vector<int> pick;
-    P2_TRY(c,
-           tune_choose(c->tuner.get(), key, cands, c->stream, !c->capturing,
-                       [&](const std::vector<int>& v) {
-                         p2::SplitGemmArgs q = g;
-                         set(q, v);
-                         return p2::launch_project_split(q, c->stream);
-                       },
-                       pick),
-           "projection tuning");
-    set(g, pick);
-    const int NT = g.NT, nsplit = g.nsplit;
-    const int ncols = g.ntile * 2 * NT;
-    {
-      ProfScope ps(c, "project_split_tc");
-      P2_TRY(c, p2::launch_project_split(g, c->stream), "tensor-core projection");
-    }
-    p2::SplitReduceArgs rd{};
-    rd.part = (const float*)c->fpart.p;
-    rd.ntau = n;
-    rd.nsplit = nsplit;
-    rd.nmtile = nmtile;
-    rd.ncols = ncols;
-    rd.NT = NT;
-    rd.nmom = pl.nmom;
-    rd.K = K;
-    rd.mom_row = (const int*)c->momrow.p;
-    for (int d = 0; d < 3; d++) rd.L[d] = c->g.L[d];
-    rd.cmax = (const int*)c->cmaxb.p;
-    rd.exps = (const int*)c->expb.p;
-    rd.kexp = (const int*)c->kexp.p;
-    rd.sl = dsl;
-    rd.nblocks = (int)pl.blocks.size();
-    for (size_t b = 0; b < pl.blocks.size(); b++) rd.blk[b] = pl.blocks[b];
-    {
-      ProfScope ps(c, "split_reduce");
-      P2_TRY(c, p2::launch_split_reduce(rd, c->stream), "split reduction");
-    }
+    if ((st = split_project(c, pl, K, n, nmtile, nkstep, dsl, (const int*)c->expb.p, (const int*)c->kexp.p,
+                            pl.blocks)) != P2_OK)
+      return st;
   }
   return P2_OK;
 }

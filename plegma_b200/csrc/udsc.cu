@@ -184,6 +184,223 @@ cudaError_t launch_contract_udsc(const UdscArgs& a, int grid, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// ---- split form --------------------------------------------------------------
+// The same lane streams in FP32 on the three views scaled by 2^-E (per slice
+// and view, exact), the FP32 tile in the padded row layout of RowF32 with the
+// views at blocks 0-15, 16-31, 32-47; per (slice, dataset) the maximum of
+// |Re|, |Im| for the hi+lo FP16 split of the tensor-core projection.
+constexpr int kRowU32 = 48 * 10 + 2;  // complex per FP32 site row (161 x 3 units: rows start in different bank groups)
+
+struct UdscArgsF32 {
+  const void* p[3];
+  long long vol[3];  // component strides of the views
+  const UdscSlice* sl;
+  int ntau, V3, nd;
+  const int* plan;
+  int* e3;          // [ntau][3]: view v of slice t is staged times 2^-e3[3t+v]
+  int* es;          // [ntau][2]: (sum of the slice's three exponents, 0), the un-scaling of every dataset
+  Cx<float>* out;   // [ntau][nd][V3]
+  int* cmax;        // [ntau][nd] max |Re|, |Im| as float bits
+};
+
+// Per slice and view the binary exponent of the largest of a strided sample
+// (every 7th component, every 97th site), plus one when the view is rotated.
+template <typename Tin>
+__global__ void k_sample_udsc(const UdscArgsF32 a) {
+  __shared__ int red[256];
+  const int tl = blockIdx.x;
+  const UdscSlice& sd = a.sl[tl];
+  int total = 0;
+  for (int f = 0; f < 3; f++) {
+    const Cx<Tin>* p = (const Cx<Tin>*)a.p[f] + sd.off[f];
+    int emax = -100000;
+    for (int i = threadIdx.x; i < 21 * 1024; i += blockDim.x) {
+      const int comp = (i % 21) * 7;
+      const long long x = ((long long)(i / 21) * 97) % a.V3;
+      const Cx<Tin> v = p[comp * a.vol[f] + x];
+      int e;
+      if (v.x != 0) {
+        frexp((double)v.x, &e);
+        emax = max(emax, e);
+      }
+      if (v.y != 0) {
+        frexp((double)v.y, &e);
+        emax = max(emax, e);
+      }
+    }
+    red[threadIdx.x] = emax;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) red[threadIdx.x] = max(red[threadIdx.x], red[threadIdx.x + s]);
+      __syncthreads();
+    }
+    const int E = (red[0] == -100000 ? 0 : red[0]) + ((sd.xf[f] & 3) ? 1 : 0);
+    total += E;
+    if (threadIdx.x == 0) a.e3[3 * tl + f] = E;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    a.es[2 * tl] = total;
+    a.es[2 * tl + 1] = 0;
+  }
+}
+
+template <typename Tin>
+__device__ __forceinline__ void issue_tile_u32(const UdscArgsF32& a, Cx<Tin>* st, long long tile, long long ntiles,
+                                               int tiles_per_tau) {
+  if (tile < ntiles) {
+    const int tl = (int)(tile / tiles_per_tau);
+    const int s = threadIdx.x & (kSitesU - 1);
+    const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesU + s;
+    const bool ok = x < a.V3;
+    const UdscSlice* sd = a.sl + tl;
+    // component-major staging [view * 144 + component][16 sites]: thread i
+    // copies component i/16 + 16 r of site i%16
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+      const Cx<Tin>* src = (const Cx<Tin>*)a.p[f] + sd->off[f] + (ok ? x : 0);
+#pragma unroll 3
+      for (int r = 0; r < 9; r++) {
+        const int comp = (threadIdx.x >> 4) + 16 * r;
+        Cx<Tin>* dst = st + (144 * f + comp) * kSitesU + s;
+        if (sizeof(Tin) == 8)
+          cp_async16(dst, src + comp * a.vol[f], ok ? 16 : 0);
+        else
+          cp_async8(dst, src + comp * a.vol[f], ok ? 8 : 0);
+      }
+    }
+  }
+  cp_async_commit();
+}
+
+template <typename Tin>
+__global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc_f32(const UdscArgsF32 a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<Tin>* st = (Cx<Tin>*)smem_raw;
+  Cx<float>* sf = (Cx<float>*)(smem_raw + 3 * 144 * kSitesU * sizeof(Cx<Tin>));
+  int* smx = (int*)(sf + kSitesU * kRowU32);  // [kMaxDs] maxima of the current slice
+  const int tid = threadIdx.x;
+  const int hw = tid >> 4, l = tid & 15;
+  const unsigned mask = halfwarp_mask();
+  const int tiles_per_tau = (a.V3 + kSitesU - 1) / kSitesU;
+  const long long ntiles = (long long)a.ntau * tiles_per_tau;
+  long long tile = blockIdx.x;
+  const int* stream0 = a.plan + a.plan[l];
+  if (tid < kMaxDs) smx[tid] = 0;
+
+  issue_tile_u32<Tin>(a, st, tile, ntiles, tiles_per_tau);
+  int cur = -1;
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int tl = (int)(tile / tiles_per_tau);
+    cp_async_wait<0>();
+    __syncthreads();
+    if (tl != cur) {
+      if (cur >= 0 && tid < a.nd) {
+        atomicMax(a.cmax + (long long)cur * a.nd + tid, smx[tid]);
+        smx[tid] = 0;
+      }
+      cur = tl;
+    }
+    // scale, transform and convert: thread (site s, transform groups
+    // q = c0 + 16 j of 108: 36 per view) -> the site's FP32 row
+    {
+      const UdscSlice& sd = a.sl[tl];
+      const int s = tid & (kSitesU - 1), c0 = tid >> 4;
+      Cx<float>* row = sf + s * kRowU32;
+#pragma unroll
+      for (int j = 0; j < 7; j++) {
+        const int q = c0 + 16 * j;
+        if (q < 108) {
+          const int f = q / 36;
+          const double sc = ldexp(1.0, -a.e3[3 * tl + f]);
+          int comp[4];
+          prop_group_comps(q - 36 * f, comp);
+          Cx<double> v[4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const Cx<Tin> x = st[(144 * f + comp[i]) * kSitesU + s];
+            v[i] = cx<double>((double)x.x, (double)x.y);
+          }
+          prop_group_transform(v[0], v[1], v[2], v[3], sd.xf[f]);
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const int blk = comp[i] / 9, col = comp[i] - 9 * blk;
+            row[2 * row32_unit(16 * f + blk, col >> 1) + (col & 1)] =
+                cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
+          }
+        }
+      }
+    }
+    __syncthreads();
+    issue_tile_u32<Tin>(a, st, tile + gridDim.x, ntiles, tiles_per_tau);
+    const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesU + hw;
+    if (x < a.V3) {
+      const RowF32 row{sf + hw * kRowU32};
+      Cx<float> acc[kMaxDs];
+#pragma unroll
+      for (int d = 0; d < kMaxDs; d++) acc[d] = czero<float>();
+      const int* q = stream0;
+      const int ntup = *q++;
+#pragma unroll 1
+      for (int t = 0; t < ntup; t++) {
+        const int head = q[0];
+        const unsigned cnt[4] = {(unsigned)q[1], (unsigned)q[2], (unsigned)q[3], (unsigned)q[4]};
+        q += 5;
+        Cx<float> g[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) g[i] = czero<float>();
+        diquark_acc(row, head & 255, (head >> 8) & 255, 0, 0, 1.f, 0, 0, g);
+#pragma unroll
+        for (int d = 0; d < kMaxDs; d++) {
+          if (d >= a.nd) break;
+          const int n = (int)((cnt[d >> 2] >> (8 * (d & 3))) & 255u);
+#pragma unroll 1
+          for (int e = 0; e < n; e++) {
+            const int blk = q[0];
+            const Cx<float> w = cx<float>(__int_as_float(q[1]), __int_as_float(q[2]));
+            q += 3;
+            Cx<float> z[9];
+            row.load9(blk, z);
+            Cx<float> dot = czero<float>();
+#pragma unroll
+            for (int i = 0; i < 9; i++) cmac(dot, g[i], z[i]);
+            cmac(acc[d], w, dot);
+          }
+        }
+      }
+      Cx<float>* o = a.out + (long long)tl * a.nd * a.V3 + x;
+#pragma unroll
+      for (int d = 0; d < kMaxDs; d++) {
+        if (d >= a.nd) break;
+        Cx<float> v = acc[d];
+        v = v + shfl_xor16(v, 1, mask);
+        v = v + shfl_xor16(v, 2, mask);
+        v = v + shfl_xor16(v, 4, mask);
+        v = v + shfl_xor16(v, 8, mask);
+        if (l == d) {
+          o[(long long)d * a.V3] = v;
+          atomicMax(smx + d, __float_as_int(fmaxf(fabsf(v.x), fabsf(v.y))));
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  if (cur >= 0 && tid < a.nd) atomicMax(a.cmax + (long long)cur * a.nd + tid, smx[tid]);
+}
+
+template <typename Tin>
+cudaError_t launch_udsc_split_t(const UdscArgsF32& a, int grid, cudaStream_t s) {
+  k_sample_udsc<Tin><<<a.ntau, 256, 0, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int smem = 3 * 144 * kSitesU * (int)sizeof(Cx<Tin>) + kSitesU * kRowU32 * (int)sizeof(Cx<float>) + 64;
+  e = ensure_smem((const void*)k_contract_udsc_f32<Tin>, smem);
+  if (e != cudaSuccess) return e;
+  k_contract_udsc_f32<Tin><<<grid, kThreadsU, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
 // Per-lane instruction streams of one flavour product (see the file comment).
 std::vector<int> build_plan(int prod) {
   const int d0 = kUdscDsBegin[prod], nd = kUdscDsBegin[prod + 1] - d0;
@@ -273,10 +490,10 @@ int prop_of(const p2_udsc_request& r, char f) {
 struct p2_udsc_cache {
   std::vector<p2host::DevBuf> plan;  // per product, built on first use
   p2host::DevBuf slices, desc;
+  p2host::DevBuf e3, es, kexp;  // split form: view exponents, un-scaling exponents, component multiplicities
   ~p2_udsc_cache() {
     for (auto& b : plan) b.release();
-    slices.release();
-    desc.release();
+    for (p2host::DevBuf* b : {&slices, &desc, &e3, &es, &kexp}) b->release();
   }
 };
 
@@ -313,6 +530,8 @@ p2_status p2_contract_udsc(p2_ctx* c, const p2_prop* props, int nprops, const p2
   if (!r->out) return c->fail(P2_ERR_INVALID_ARG, "null output");
   if (r->out_location != P2_DEVICE && r->out_location != P2_HOST)
     return c->fail(P2_ERR_INVALID_ARG, "bad out_location");
+  if (r->mode != P2_PLAIN_FP64 && r->mode != P2_SPLIT_FP16) return c->fail(P2_ERR_INVALID_ARG, "bad mode");
+  const bool split = r->mode == P2_SPLIT_FP16;
   p2_request base{};
   std::memcpy(base.source, r->source, sizeof(base.source));
   base.totalT = r->totalT;
@@ -331,7 +550,10 @@ p2_status p2_contract_udsc(p2_ctx* c, const p2_prop* props, int nprops, const p2
         return c->fail(P2_ERR_INVALID_ARG, "p2_contract_udsc: bad propagator view");
       if ((pr.transform & ~0xFu) || ((pr.transform & 1u) && (pr.transform & 2u)))
         return c->fail(P2_ERR_INVALID_ARG, "p2_contract_udsc: bad transform bits");
-      if (pr.precision != P2_FP64) return c->fail(P2_ERR_UNSUPPORTED, "p2_contract_udsc needs FP64 propagators");
+      if (pr.precision != P2_FP64 && !(split && pr.precision == P2_FP32))
+        return c->fail(P2_ERR_UNSUPPORTED, "p2_contract_udsc: FP32 propagators need the split form");
+      if (pr.precision != props[prop_of(*r, kUdscProduct[todo[0]][0])].precision)
+        return c->fail(P2_ERR_UNSUPPORTED, "p2_contract_udsc: all propagators must share a precision");
       if (pr.location != P2_DEVICE)
         return c->fail(P2_ERR_UNSUPPORTED, "p2_contract_udsc needs device-resident propagators");
     }
@@ -350,8 +572,23 @@ p2_status p2_contract_udsc(p2_ctx* c, const p2_prop* props, int nprops, const p2
     P2_TRY(c, cudaMemsetAsync(c->res.p, 0, total * 16, c->stream), "result clear");
     dres = (double*)c->res.p;
   }
+  int nmtile = 0, nkstep = 0;
+  if (split) {
+    if (c->project_split_smem_max < project_split_smem_bytes(144))
+      return c->fail(P2_ERR_UNSUPPORTED, "device shared memory per block too small for the tensor-core projection");
+    if (!c->errflag.p) {
+      P2_TRY(c, c->errflag.ensure(16), "error flag alloc");
+      P2_TRY(c, cudaMemsetAsync(c->errflag.p, 0, 16, c->stream), "error flag clear");
+    }
+    if ((st = split_prepare_tables(c, pl, 0, nmtile, nkstep)) != P2_OK) return st;
+    if (!U.kexp.p) {  // every dataset carries each of its three views once: (1, 0) against es
+      std::vector<int> ke(2 * kMaxDs, 0);
+      for (int k = 0; k < kMaxDs; k++) ke[2 * k] = 1;
+      if ((st = upload_async(c, U.kexp, ke.data(), ke.size() * sizeof(int), "udsc exponents")) != P2_OK) return st;
+    }
+  }
   // phase tables (origin 0; the scatter applies the source phase)
-  if (c->plain_moms_key != pl.moms) {
+  if (!split && c->plain_moms_key != pl.moms) {
     c->plain_moms_key.clear();
     std::vector<double> tabh = phase_tables(c, pl.moms.data(), pl.nmom, -1, pl.Lmax);
     if ((st = upload_async(c, c->ptab, tabh.data(), tabh.size() * sizeof(double), "phase table")) != P2_OK)
@@ -389,6 +626,62 @@ p2_status p2_contract_udsc(p2_ctx* c, const p2_prop* props, int nprops, const p2
       sl.push_back(s);
     }
     const int n_all = (int)taus.size();
+    if (split) {
+      const bool f32 = v[0]->precision == P2_FP32;
+      const size_t per32 = (size_t)nd * c->V3 * 8;
+      const int tc = (int)std::max<size_t>(1, std::min<size_t>(c->ws_budget / std::max<size_t>(per32, 1), (size_t)T));
+      for (int c0 = 0; c0 < n_all; c0 += tc) {
+        const int n = std::min(tc, n_all - c0);
+        P2_TRY(c, c->cbuf.ensure((size_t)n * per32), "position buffer alloc");
+        P2_TRY(c, c->cmaxb.ensure((size_t)n * nd * sizeof(int)), "maxima alloc");
+        P2_TRY(c, cudaMemsetAsync(c->cmaxb.p, 0, (size_t)n * nd * sizeof(int), c->stream), "maxima clear");
+        P2_TRY(c, U.e3.ensure((size_t)n * 3 * sizeof(int)), "exponent alloc");
+        P2_TRY(c, U.es.ensure((size_t)n * 2 * sizeof(int)), "exponent alloc");
+        P2_TRY(c, U.slices.ensure((size_t)n * sizeof(UdscSlice)), "slice alloc");
+        P2_TRY(c,
+               cudaMemcpyAsync(U.slices.p, sl.data() + c0, (size_t)n * sizeof(UdscSlice), cudaMemcpyHostToDevice,
+                               c->stream),
+               "slice upload");
+        std::vector<SliceDesc> desc(n);
+        for (int i = 0; i < n; i++) {
+          std::memset(&desc[i], 0, sizeof(SliceDesc));
+          desc[i].out = dres;
+          desc[i].tau = taus[c0 + i];
+          desc[i].totalT = r->totalT;
+          for (int d = 0; d < 3; d++) desc[i].x0[d] = r->source[d];
+        }
+        P2_TRY(c, U.desc.ensure((size_t)n * sizeof(SliceDesc)), "descriptor alloc");
+        P2_TRY(c,
+               cudaMemcpyAsync(U.desc.p, desc.data(), (size_t)n * sizeof(SliceDesc), cudaMemcpyHostToDevice,
+                               c->stream),
+               "descriptor upload");
+        UdscArgsF32 a{};
+        for (int k = 0; k < 3; k++) {
+          a.p[k] = v[k]->data;
+          a.vol[k] = c->V3 * v[k]->nt;
+        }
+        a.sl = (const UdscSlice*)U.slices.p;
+        a.ntau = n;
+        a.V3 = (int)c->V3;
+        a.nd = nd;
+        a.plan = (const int*)U.plan[p].p;
+        a.e3 = (int*)U.e3.p;
+        a.es = (int*)U.es.p;
+        a.out = (Cx<float>*)c->cbuf.p;
+        a.cmax = (int*)c->cmaxb.p;
+        {
+          ProfScope ps(c, "contract_udsc_f32");
+          P2_TRY(c, f32 ? launch_udsc_split_t<float>(a, c->nsm, c->stream) : launch_udsc_split_t<double>(a, c->nsm, c->stream),
+                 "udsc split contraction");
+        }
+        const std::vector<ScatterBlock> blocks{ScatterBlock{0, 1, nd, 1, (long long)ds_off}};
+        if ((st = split_project(c, pl, nd, n, nmtile, nkstep, (const SliceDesc*)U.desc.p, (const int*)U.es.p,
+                                (const int*)U.kexp.p, blocks)) != P2_OK)
+          return st;
+      }
+      ds_off += nd;
+      continue;
+    }
     const size_t per = (size_t)nd * c->V3 * 16;
     const int tc = (int)std::max<size_t>(1, std::min<size_t>(c->ws_budget / std::max<size_t>(per, 1), (size_t)T));
     for (int c0 = 0; c0 < n_all; c0 += tc) {

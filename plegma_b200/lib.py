@@ -75,7 +75,7 @@ class P2UdscRequest(C.Structure):
     _fields_ = [("source", C.c_int * 4), ("totalT", C.c_int), ("moms", C.POINTER(C.c_int)), ("nmom", C.c_int),
                 ("q2max", C.c_int), ("prop_u", C.c_int), ("prop_d", C.c_int), ("prop_s", C.c_int),
                 ("prop_c", C.c_int), ("only_st", C.c_int), ("only_ch", C.c_int), ("out", C.c_void_p),
-                ("out_location", C.c_int)]
+                ("out_location", C.c_int), ("mode", C.c_int)]
 
 
 class P2Block(C.Structure):
@@ -296,7 +296,8 @@ class Context:
 
     @staticmethod
     def udsc_request(source, totalT, out_ptr, out_location=P2_DEVICE, q2max=0, moms: Optional[np.ndarray] = None,
-                     prop_u=-1, prop_d=-1, prop_s=-1, prop_c=-1, only_st=False, only_ch=False) -> P2UdscRequest:
+                     prop_u=-1, prop_d=-1, prop_s=-1, prop_c=-1, only_st=False, only_ch=False,
+                     mode=P2_PLAIN_FP64) -> P2UdscRequest:
         """A table-driven baryon request (contractBaryonsUDSC); prop_* index the props list, -1 = not given."""
         r = P2UdscRequest()
         r.source[:] = list(source)
@@ -314,6 +315,7 @@ class Context:
         r.only_st, r.only_ch = int(only_st), int(only_ch)
         r.out = out_ptr
         r.out_location = out_location
+        r.mode = mode
         return r
 
     def contract_udsc(self, props: Sequence[P2Prop], req: P2UdscRequest):

@@ -105,7 +105,7 @@ def test_filters_and_window_views():
     ctx.close()
 
 
-def test_udsc_rejects_fp32_and_host_propagators():
+def test_udsc_rejects_fp32_plain_and_host_propagators():
     ctx = p2.Context((2, 2, 2, 4))
     (u,) = device_props(ctx, [(5, 0)], t0=0)
     out = torch.zeros(4 * 4, dtype=torch.complex128, device="cuda")
@@ -117,4 +117,69 @@ def test_udsc_rejects_fp32_and_host_propagators():
     with pytest.raises(p2.P2Error) as e:
         ctx.contract_udsc([ctx.prop(h.data_ptr(), location=p2.P2_HOST)], req)
     assert e.value.status == p2.P2_ERR_UNSUPPORTED
+    ctx.close()
+
+
+SPLIT_TOL = 1e-6
+
+
+def test_split_light_baryons_u_d():
+    """Split form (FP32 contraction, hi+lo FP16 tensor-core projection): u and
+    d, 28 datasets, window wrapping through t = 0."""
+    ctx = p2.Context((4, 4, 2, 6))
+    src = (1, 2, 0, 4)
+    u, d = device_props(ctx, [(73, 0), (73, 1)], t0=src[3])
+    moms = p2.mom_list(2)
+    W = 5
+    req = ctx.udsc_request(src, W, 0, moms=moms, prop_u=0, prop_d=1, mode=p2.P2_SPLIT_FP16)
+    n = len(p2.udsc_datasets(req))
+    out = torch.zeros(n * W * len(moms), dtype=torch.complex128, device="cuda")
+    req.out = out.data_ptr()
+    ctx.contract_udsc([ctx.prop(u.data_ptr()), ctx.prop(d.data_ptr())], req)
+    ctx.sync()
+    err = _check(ctx, {"u": u, "d": d}, src, W, moms, out.cpu().numpy(), req)
+    assert err < SPLIT_TOL, err
+    ctx.close()
+
+
+def test_split_all_products_host_output():
+    ctx = p2.Context((2, 3, 2, 4))
+    src = (1, 0, 1, 2)
+    bufs = device_props(ctx, [(83, 0), (83, 1), (84, 0), (84, 1)], t0=src[3])
+    flav = dict(zip("udsc", bufs))
+    moms = np.array([[0, 0, 0], [1, 0, 0], [0, -1, 1]], dtype=np.int32)
+    W = 3
+    req = ctx.udsc_request(src, W, 0, p2.P2_HOST, moms=moms, prop_u=0, prop_d=1, prop_s=2, prop_c=3,
+                           mode=p2.P2_SPLIT_FP16)
+    n = len(p2.udsc_datasets(req))
+    assert n == 200
+    out = np.zeros(n * W * len(moms), dtype=np.complex128)
+    req.out = out.ctypes.data
+    ctx.contract_udsc([ctx.prop(b.data_ptr()) for b in bufs], req)
+    err = _check(ctx, flav, src, W, moms, out, req)
+    assert err < SPLIT_TOL, err
+    ctx.close()
+
+
+def test_split_fp32_propagators_and_transforms():
+    """FP32 propagators (split form only), u rotated with s = +1 and d with
+    s = -1 plus the boundary sign, applied on load; the oracle runs on the
+    host-transformed FP32 entries."""
+    ctx = p2.Context((3, 2, 4, 4))
+    src = (2, 1, 3, 1)
+    u, d = device_props(ctx, [(75, 0), (75, 1)], t0=src[3], precision=p2.P2_FP32)
+    xu, xd = p2.PROP_ROTATE_PLUS | p2.PROP_BOUNDARY, p2.PROP_ROTATE_MINUS | p2.PROP_BOUNDARY
+    moms = p2.mom_list(1)
+    W = 4
+    req = ctx.udsc_request(src, W, 0, moms=moms, prop_u=0, prop_d=1, mode=p2.P2_SPLIT_FP16)
+    n = len(p2.udsc_datasets(req))
+    out = torch.zeros(n * W * len(moms), dtype=torch.complex128, device="cuda")
+    req.out = out.data_ptr()
+    ctx.contract_udsc([ctx.prop(u.data_ptr(), precision=p2.P2_FP32, transform=xu, boundary_t0=src[3]),
+                       ctx.prop(d.data_ptr(), precision=p2.P2_FP32, transform=xd, boundary_t0=src[3])], req)
+    ctx.sync()
+    hu = torch.from_numpy(orc.prop_transform(u.cpu().numpy().astype(np.complex128), ctx.V3, 0, 4, 4, xu, src[3]))
+    hd = torch.from_numpy(orc.prop_transform(d.cpu().numpy().astype(np.complex128), ctx.V3, 0, 4, 4, xd, src[3]))
+    err = _check(ctx, {"u": hu, "d": hd}, src, W, moms, out.cpu().numpy(), req)
+    assert err < SPLIT_TOL, err
     ctx.close()
