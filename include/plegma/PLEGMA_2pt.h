@@ -40,7 +40,8 @@ enum CORR_SPACE { POSITION_SPACE, MOMENTUM_SPACE };
 enum FILE_FORMAT { ASCII_FORMAT, HDF5_FORMAT, LIME_FORMAT, DEFAULT_FORMAT };
 enum ALLOCATION_FLAG { EVERY = -1, NONE = 0, HOST, DEVICE, BOTH };
 enum GHOST_FLAG { ALL_GHOSTS = -1, NO_GHOSTS, FIRST_SIDE, FIRST_CORNER, FIRST_VERTEX };
-enum FT_TYPE { FT_NAIVE, FT_GEMV, FT_FFT };
+// FT_SPLIT (not in the reference): the tensor-core projection of p2_ft_apply_split.
+enum FT_TYPE { FT_NAIVE, FT_GEMV, FT_FFT, FT_SPLIT };
 enum GAMMAS { ONE, G1, G2, G3, G4, G5, G5G1, G5G2, G5G3, G5G4, S12, S13, S23, S41, S42, S43 };
 enum CONTRACTION_MODE { PLAIN_FP64 = P2_PLAIN_FP64, SPLIT_FP16 = P2_SPLIT_FP16 };
 
@@ -314,8 +315,9 @@ class PLEGMA_FT {
     }
     std::vector<double> out((size_t)Nmoms() * dimT * dof * 2);
     std::vector<int> m = int_moms();
-    Runtime::check(p2_ft_apply(Runtime::context(), (const double*)f.D_elem(), dof, dimT, m.data(), Nmoms(), sign,
-                               out.data(), P2_HOST),
+    Runtime::check((type == FT_SPLIT ? p2_ft_apply_split : p2_ft_apply)(Runtime::context(), (const double*)f.D_elem(),
+                                                                        dof, dimT, m.data(), Nmoms(), sign,
+                                                                        out.data(), P2_HOST),
                    "PLEGMA_FT::apply");
     for (size_t i = 0; i < out.size(); i++) h[i] = accum ? h[i] + (Float)out[i] : (Float)out[i];
   }

@@ -201,6 +201,14 @@ p2_status p2_contract_position(p2_ctx* ctx, const p2_prop* props, int nprops, co
 p2_status p2_ft_apply(p2_ctx* ctx, const double* field, int dof, int nt, const int* moms, int nmom, int sign,
                       double* out, int out_location);
 
+/* The same transform on the tensor cores (the split projection of the
+ * contractions): each time slice of the field is scaled by 2^-e (e the binary
+ * exponent of its largest entry, exact), converted to FP32 and projected with
+ * hi+lo FP16 operands and FP32 accumulation; per (t, component, momentum) the
+ * error is <= 1e-6 of sum_x |field(x, t)| of that component. */
+p2_status p2_ft_apply_split(p2_ctx* ctx, const double* field, int dof, int nt, const int* moms, int nmom, int sign,
+                            double* out, int out_location);
+
 /* Allocation-free variant of p2_ft_apply (no counterpart in the reference).
  * For callers that cannot allocate device memory at call time, e.g. a host
  * framework that reserves all device memory for its own pool up front, or a

@@ -670,7 +670,7 @@ p2_status p2_ctx_destroy(p2_ctx* c) {
     return P2_OK;
   }
   cudaStreamSynchronize(c->stream);
-  for (DevBuf* b : {&c->cbuf, &c->part, &c->tab, &c->res, &c->moms, &c->sdesc, &c->ptab}) b->release();
+  for (DevBuf* b : {&c->cbuf, &c->part, &c->tab, &c->res, &c->moms, &c->sdesc, &c->ptab, &c->ft_kexp}) b->release();
   if (c->sdesc_host) cudaFreeHost(c->sdesc_host);
   if (c->sdesc_copied) cudaEventDestroy(c->sdesc_copied);
   for (int i = 0; i < 2; i++) {
@@ -913,6 +913,89 @@ p2_status p2_contract_position(p2_ctx* c, const p2_prop* props, int nprops, cons
                "position copy");
   }
   if (r->out_location == P2_HOST) P2_TRY(c, cudaStreamSynchronize(c->stream), "position download");
+  return P2_OK;
+}
+
+p2_status p2_ft_apply_split(p2_ctx* c, const double* field, int dof, int nt, const int* moms, int nmom, int sign,
+                            double* out, int out_location) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  if (!field || !out || dof < 1 || nt < 1 || nt > c->Ll[3] || !moms || nmom < 1)
+    return c->fail(P2_ERR_INVALID_ARG, "p2_ft_apply_split: bad arguments");
+  if (sign != 1 && sign != -1) return c->fail(P2_ERR_INVALID_ARG, "p2_ft_apply_split: sign must be +1 or -1");
+  if (out_location != P2_DEVICE && out_location != P2_HOST) return c->fail(P2_ERR_INVALID_ARG, "bad out_location");
+  if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
+  if (c->project_split_smem_max < p2::project_split_smem_bytes(144))
+    return c->fail(P2_ERR_UNSUPPORTED, "device shared memory per block too small for the tensor-core projection");
+  // exp(+i p.x) = exp(-i (-p).x): the projection's rows carry exp(-i p.x)
+  Plan pl;
+  pl.nmom = nmom;
+  pl.moms.assign(moms, moms + 3 * nmom);
+  if (sign == 1)
+    for (int& m : pl.moms) m = -m;
+  pl.Lmax = std::max(c->Ll[0], std::max(c->Ll[1], c->Ll[2]));
+  pl.K = dof;
+  pl.totalT = nt;
+  if (!c->errflag.p) {
+    P2_TRY(c, c->errflag.ensure(16), "error flag alloc");
+    P2_TRY(c, cudaMemsetAsync(c->errflag.p, 0, 16, c->stream), "error flag clear");
+  }
+  int nmtile = 0, nkstep = 0;
+  p2_status st = p2::split_prepare_tables(c, pl, 0, nmtile, nkstep);
+  if (st != P2_OK) return st;
+  const size_t total = (size_t)nt * dof * nmom;
+  double* dst = out;
+  if (out_location == P2_HOST) {
+    P2_TRY(c, c->res.ensure(total * 16), "result alloc");
+    dst = (double*)c->res.p;
+  }
+  // every component carries the slice scale once
+  if (c->ft_kexp_n < dof) {
+    std::vector<int> ke(2 * (size_t)dof, 0);
+    for (int k = 0; k < dof; k++) ke[2 * k] = 1;
+    if ((st = upload_async(c, c->ft_kexp, ke.data(), ke.size() * sizeof(int), "field exponents")) != P2_OK) return st;
+    c->ft_kexp_n = dof;
+  }
+  const size_t per = (size_t)dof * c->V3 * 8;
+  const int tc = (int)std::max<size_t>(1, std::min<size_t>(c->ws_budget / std::max<size_t>(per, 1), (size_t)nt));
+  for (int t0 = 0; t0 < nt; t0 += tc) {
+    const int n = std::min(tc, nt - t0);
+    P2_TRY(c, c->cbuf.ensure((size_t)n * per), "position buffer alloc");
+    P2_TRY(c, c->cmaxb.ensure((size_t)n * dof * sizeof(int)), "maxima alloc");
+    P2_TRY(c, c->expb.ensure((size_t)2 * n * sizeof(int)), "exponent alloc");
+    std::vector<p2::SliceDesc> desc(n);
+    for (int i = 0; i < n; i++) {
+      std::memset(&desc[i], 0, sizeof(p2::SliceDesc));
+      desc[i].tau = t0 + i;
+      desc[i].totalT = nt;
+    }
+    P2_TRY(c, c->sdesc.ensure((size_t)n * sizeof(p2::SliceDesc)), "descriptor alloc");
+    P2_TRY(c,
+           cudaMemcpyAsync(c->sdesc.p, desc.data(), (size_t)n * sizeof(p2::SliceDesc), cudaMemcpyHostToDevice,
+                           c->stream),
+           "descriptor upload");
+    p2::FieldF32Args fa{};
+    fa.field = field;
+    fa.vol = c->V3 * nt;
+    fa.t0 = t0;
+    fa.ntau = n;
+    fa.K = dof;
+    fa.V3 = (int)c->V3;
+    fa.exps = (int*)c->expb.p;
+    fa.c = (float*)c->cbuf.p;
+    fa.cmax = (int*)c->cmaxb.p;
+    {
+      ProfScope ps(c, "field_to_f32");
+      P2_TRY(c, p2::launch_field_to_f32(fa, c->nsm, c->stream), "field conversion");
+    }
+    if ((st = p2::split_project(c, pl, dof, n, nmtile, nkstep, (const p2::SliceDesc*)c->sdesc.p,
+                                (const int*)c->expb.p, (const int*)c->ft_kexp.p, {}, dst, (long long)dof * nmom,
+                                nmom)) != P2_OK)
+      return st;
+  }
+  if (out_location == P2_HOST) {
+    P2_TRY(c, cudaMemcpyAsync(out, dst, total * 16, cudaMemcpyDeviceToHost, c->stream), "result download");
+    P2_TRY(c, cudaStreamSynchronize(c->stream), "result download");
+  }
   return P2_OK;
 }
 

@@ -85,6 +85,8 @@ struct p2_ctx {
   bool capturing = false;              // recording a graph: no host synchronisation
   // host-resident propagators: two staging slots per flavour, uploaded on a
   // copy stream while the previous chunk is contracted
+  p2host::DevBuf ft_kexp;  // split field transform: (1, 0) per component
+  int ft_kexp_n = 0;
   p2host::DevBuf stage_u2[2], stage_d2[2];
   // host-side FP32 conversion of host views (split form): pinned buffers and
   // the events of their last upload
@@ -237,5 +239,6 @@ void precision_release(p2_ctx* c);
 // shared with the split form of the table-driven baryons (udsc.cu)
 p2_status split_prepare_tables(p2_ctx* c, const p2host::Plan& pl, unsigned what, int& nmtile, int& nkstep);
 p2_status split_project(p2_ctx* c, const p2host::Plan& pl, int K, int n, int nmtile, int nkstep, const SliceDesc* dsl,
-                        const int* exps, const int* kexp, const std::vector<ScatterBlock>& blocks);
+                        const int* exps, const int* kexp, const std::vector<ScatterBlock>& blocks,
+                        double* out = nullptr, long long oT = 0, long long oK = 0);
 }  // namespace p2

@@ -126,7 +126,24 @@ struct SplitReduceArgs {
   const SliceDesc* sl; // result location of each slice
   int nblocks;
   ScatterBlock blk[kMaxBlocks];  // base = block offset per unit of (totalT * nmom)
+  // generic [t][K][mom] layout when nblocks == 0: out[sl[tl].tau * oT + k * oK + p]
+  long long oT, oK;
+  double* out;
 };
+
+// Generic field for the split projection: FP64 [K][V3 * nt] (slices t0 ..
+// t0 + ntau - 1) to FP32 [ntau][K][V3] times 2^-exps[2t], exps[2t] the
+// binary exponent of the largest entry of the slice; max |Re|, |Im| per
+// (slice, component) into cmax.
+struct FieldF32Args {
+  const double* field;
+  long long vol;  // component stride of the field (V3 * nt)
+  int t0, ntau, K, V3;
+  int* exps;      // [ntau][2]
+  float* c;       // complex float
+  int* cmax;      // [ntau][K]
+};
+cudaError_t launch_field_to_f32(const FieldF32Args& a, int nsm, cudaStream_t s);
 
 cudaError_t launch_build_phases(const PhaseBuildArgs& a, cudaStream_t s);
 cudaError_t launch_project_split(const SplitGemmArgs& a, cudaStream_t s);

@@ -160,8 +160,10 @@ p2_status split_prepare_tables(p2_ctx* c, const Plan& pl, unsigned what, int& nm
 // c->cmaxb) on the tensor cores, launch shape from the autotuner, then the
 // FP64 reduction into the results of the slices dsl: per component k the
 // un-scaling exponent is kexp[2k] (exps[2t] + eh_u) + kexp[2k+1] (exps[2t+1] + eh_d).
+// With no blocks the results go to out[tau * oT + k * oK + p].
 p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int nkstep, const SliceDesc* dsl,
-                        const int* exps, const int* kexp, const std::vector<ScatterBlock>& blocks) {
+                        const int* exps, const int* kexp, const std::vector<ScatterBlock>& blocks, double* out,
+                        long long oT, long long oK) {
   // projection GEMM candidates (N-tile width NT <= 144 components = 288
   // TMEM columns, number of N-tiles, site splits, k-steps per split): the
   // fewest N-tiles at ~2 waves first, then up to two more N-tiles at 1, 2
@@ -235,6 +237,9 @@ p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int
   rd.sl = dsl;
   rd.nblocks = (int)blocks.size();
   for (size_t b = 0; b < blocks.size(); b++) rd.blk[b] = blocks[b];
+  rd.out = out;
+  rd.oT = oT;
+  rd.oK = oK;
   {
     ProfScope ps(c, "split_reduce");
     P2_TRY(c, p2::launch_split_reduce(rd, c->stream), "split reduction");

@@ -31,6 +31,8 @@
 // block-wide barrier inside the k-loop.
 #include <cuda_fp16.h>
 
+#include <climits>
+
 #include "kernels.cuh"
 #include "launch_util.h"
 #include "p2_common.cuh"
@@ -327,6 +329,7 @@ __global__ void k_split_reduce(const SplitReduceArgs a) {
     // S(p) = sum_x c e^{-i p.x}; the source phase: C(p) = e^{i p.x0} S(p), with
     // p.x0 / L reduced exactly in integers per dimension
     const Cx<double> v = cmul(cx<double>((cr + sg * si) * f, (ci - sg * sr) * f), source_phase(mr + 3, sd.x0, a.L));
+    if (a.nblocks == 0) ((Cx<double>*)a.out)[(long long)sd.tau * a.oT + (long long)k * a.oK + p] = v;
     for (int b = 0; b < a.nblocks; b++) {
       const ScatterBlock& B = a.blk[b];
       const int rel = k - B.k0;
@@ -387,6 +390,92 @@ cudaError_t launch_project_split(const SplitGemmArgs& a, cudaStream_t s) {
     case 144: return launch_nt<144>(a, s);
     default: return cudaErrorInvalidValue;
   }
+}
+
+namespace {
+
+// Blocks map to (component k, slice, site range): each reduces its range in
+// shared memory and issues one atomic.
+// Pass 1: binary exponent of the largest |Re|, |Im| of every slice.
+__global__ void k_field_exponent(const FieldF32Args a, int xchunk) {
+  __shared__ int red[256];
+  const int k = blockIdx.x, tl = blockIdx.y;
+  const long long x0 = (long long)blockIdx.z * xchunk, x1 = min((long long)a.V3, x0 + xchunk);
+  const double2* row = (const double2*)a.field + (long long)k * a.vol + (long long)(a.t0 + tl) * a.V3;
+  int emax = -100000;
+  for (long long x = x0 + threadIdx.x; x < x1; x += blockDim.x) {
+    const double2 v = row[x];
+    int e;
+    if (v.x != 0.0) {
+      frexp(v.x, &e);
+      emax = max(emax, e);
+    }
+    if (v.y != 0.0) {
+      frexp(v.y, &e);
+      emax = max(emax, e);
+    }
+  }
+  red[threadIdx.x] = emax;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = max(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && red[0] != -100000) atomicMax(a.exps + 2 * tl, red[0]);
+}
+
+// Pass 2: the FP32 copy times 2^-E of its slice (exact) and the per-component maxima.
+__global__ void k_field_to_f32(const FieldF32Args a, int xchunk) {
+  __shared__ float red[256];
+  const int k = blockIdx.x, tl = blockIdx.y;
+  const long long x0 = (long long)blockIdx.z * xchunk, x1 = min((long long)a.V3, x0 + xchunk);
+  const double2* row = (const double2*)a.field + (long long)k * a.vol + (long long)(a.t0 + tl) * a.V3;
+  float2* dst = (float2*)a.c + ((long long)tl * a.K + k) * a.V3;
+  const double sc = ldexp(1.0, -a.exps[2 * tl]);
+  float m = 0.f;
+  for (long long x = x0 + threadIdx.x; x < x1; x += blockDim.x) {
+    const double2 v = row[x];
+    const float2 f = make_float2((float)(v.x * sc), (float)(v.y * sc));
+    dst[x] = f;
+    m = fmaxf(m, fmaxf(fabsf(f.x), fabsf(f.y)));
+  }
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = fmaxf(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicMax(a.cmax + (long long)tl * a.K + k, __float_as_int(red[0]));
+}
+
+// exponents before pass 1 (INT_MIN: none seen yet) and after it (an all-zero slice keeps scale 1)
+__global__ void k_field_exps_init(int* exps, int ntau) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < ntau) {
+    exps[2 * t] = INT_MIN;
+    exps[2 * t + 1] = 0;
+  }
+}
+__global__ void k_field_exps_zero(int* exps, int ntau) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < ntau && exps[2 * t] == INT_MIN) exps[2 * t] = 0;
+}
+
+}  // namespace
+
+cudaError_t launch_field_to_f32(const FieldF32Args& a, int nsm, cudaStream_t s) {
+  const int tb = (a.ntau + 255) / 256;
+  k_field_exps_init<<<tb, 256, 0, s>>>(a.exps, a.ntau);
+  cudaError_t e = cudaMemsetAsync(a.cmax, 0, (size_t)a.ntau * a.K * sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  const long long rows = (long long)a.K * a.ntau;
+  const int nx = (int)std::max<long long>(1, std::min<long long>((a.V3 + 4095) / 4096, (8LL * nsm + rows - 1) / rows));
+  const int xchunk = (int)((a.V3 + nx - 1) / nx);
+  const dim3 grid(a.K, a.ntau, nx);
+  k_field_exponent<<<grid, 256, 0, s>>>(a, xchunk);
+  k_field_exps_zero<<<tb, 256, 0, s>>>(a.exps, a.ntau);
+  k_field_to_f32<<<grid, 256, 0, s>>>(a, xchunk);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_split_reduce(const SplitReduceArgs& a, cudaStream_t s) {

@@ -93,7 +93,7 @@ EXPORTS = ["p2_ctx_create", "p2_ctx_destroy", "p2_last_error", "p2_sync", "p2_se
            "p2_synth_propagator", "p2_profile_enable", "p2_profile_read", "p2_alloc", "p2_free", "p2_copy",
            "p2_ft_apply_noalloc", "p2_set_workspace", "p2_graph_create", "p2_graph_launch", "p2_graph_sync",
            "p2_graph_destroy", "p2_tune_enable", "p2_tune_count", "p2_udsc_datasets", "p2_contract_udsc", "p2_local_taus", "p2_prop_transform",
-           "p2_prop_absorb"]
+           "p2_prop_absorb", "p2_ft_apply_split"]
 
 _lib = None
 
@@ -135,6 +135,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
                                 C.c_void_p, C.c_int]
     lib.p2_synth_propagator.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int,
                                         C.c_double, C.c_int, C.c_int]
+    lib.p2_ft_apply_split.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int,
+                                      C.c_void_p, C.c_int]
     lib.p2_ft_apply_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int,
                                         C.c_int, C.c_void_p]
     lib.p2_alloc.argtypes = [C.c_void_p, C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]
@@ -350,11 +352,12 @@ class Context:
                                                 C.c_void_p(out_ptr)))
 
     def ft_apply(self, field_ptr: int, dof: int, nt: int, moms: np.ndarray, sign: int, out_ptr: int,
-                 out_location=P2_DEVICE):
+                 out_location=P2_DEVICE, mode=P2_PLAIN_FP64):
+        """p2_ft_apply (FP64), or p2_ft_apply_split (tensor cores) with mode=P2_SPLIT_FP16."""
         m = np.ascontiguousarray(moms, dtype=np.int32)
-        self.check(self.lib.p2_ft_apply(self.h, C.c_void_p(field_ptr), dof, nt,
-                                        m.ctypes.data_as(C.POINTER(C.c_int)), len(m), sign, C.c_void_p(out_ptr),
-                                        out_location))
+        fn = self.lib.p2_ft_apply_split if mode == P2_SPLIT_FP16 else self.lib.p2_ft_apply
+        self.check(fn(self.h, C.c_void_p(field_ptr), dof, nt, m.ctypes.data_as(C.POINTER(C.c_int)), len(m), sign,
+                      C.c_void_p(out_ptr), out_location))
 
 
 class Graph:

@@ -62,6 +62,10 @@ int main(int argc, char** argv) {
     FILE* f = std::fopen((out + "_ft_up.bin").c_str(), "wb");
     std::fwrite(ft.H_elem(), sizeof(double), (size_t)2 * ft.Nmoms() * ft.DimT() * 144, f);
     std::fclose(f);
+    ft.apply(up, FT_SPLIT, -1);  // the same transform on the tensor cores
+    f = std::fopen((out + "_ft_up_split.bin").c_str(), "wb");
+    std::fwrite(ft.H_elem(), sizeof(double), (size_t)2 * ft.Nmoms() * ft.DimT() * 144, f);
+    std::fclose(f);
 
     up.copyToHost();
     f = std::fopen((out + "_up.bin").c_str(), "wb");

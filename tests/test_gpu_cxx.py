@@ -136,6 +136,11 @@ def test_ft_apply(outputs):
     u = bufs[0].cpu().numpy()
     ref = orc.ft(L, u.reshape(144, -1), 144, L[3], moms, -1)
     assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-13
+    # FT_SPLIT: error per (t, component, momentum) within 1e-6 of sum_x |u|
+    raw = np.fromfile(prefix + "_ft_up_split.bin", dtype=np.float64)
+    got = (raw[0::2] + 1j * raw[1::2]).reshape(L[3], 144, len(moms))
+    asum = np.abs(u.reshape(144, L[3], -1)).sum(axis=2).T
+    assert (np.abs(got - ref).max(axis=2) / asum).max() < 1e-6
 
 
 def test_udsc_through_the_drop_in(outputs):

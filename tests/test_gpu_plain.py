@@ -195,3 +195,38 @@ def test_second_nucleon_interpolator(what, mode):
     err = per_t_error(out, what, 6, moms, ref, taus)
     assert err.max() < (TOL if mode == p2.P2_PLAIN_FP64 else 1e-6), err
     ctx.close()
+
+
+@pytest.mark.parametrize("decay", [0.0, 40.0])
+def test_ft_apply_split_matches_oracle(decay):
+    """p2_ft_apply_split (tensor-core projection): error per (t, component,
+    momentum) <= 1e-6 of sum_x |f(x, t)| of the component, both signs, host
+    and device output; with decay 40 the slices span 1e-35 .. 1, which the
+    per-slice power-of-two scale keeps inside FP32's range.  The known answer
+    of the reference's FT test (plegma/FT.cpp:18-34): a unit field gives
+    V3 at p = 0 and 0 elsewhere."""
+    import oracle_py as orc
+    ctx = p2.Context((4, 6, 5, 3))
+    dof, nt = 21, 3
+    rng = np.random.default_rng(6)
+    f = rng.standard_normal((dof, ctx.V3 * nt)) + 1j * rng.standard_normal((dof, ctx.V3 * nt))
+    f *= np.exp(-decay * np.repeat(np.arange(nt), ctx.V3))[None, :]
+    fd = torch.from_numpy(f.reshape(-1)).cuda()
+    moms = p2.mom_list(5)
+    asum = np.abs(f).reshape(dof, nt, ctx.V3).sum(axis=2).T  # [t][dof]
+    for sign in (-1, 1):
+        ref = orc.ft(ctx.L, f, dof, nt, moms, sign)
+        out = np.zeros(nt * dof * len(moms), dtype=np.complex128)
+        ctx.ft_apply(fd.data_ptr(), dof, nt, moms, sign, out.ctypes.data, p2.P2_HOST, mode=p2.P2_SPLIT_FP16)
+        err = np.abs(out.reshape(ref.shape) - ref).max(axis=2) / asum
+        assert err.max() < 1e-6, err.max()
+        outd = torch.zeros(nt * dof * len(moms), dtype=torch.complex128, device="cuda")
+        ctx.ft_apply(fd.data_ptr(), dof, nt, moms, sign, outd.data_ptr(), mode=p2.P2_SPLIT_FP16)
+        ctx.sync()
+        assert np.array_equal(outd.cpu().numpy(), out)
+    one = torch.ones(ctx.V3 * nt, dtype=torch.complex128, device="cuda")
+    out = np.zeros(nt * len(moms), dtype=np.complex128)
+    ctx.ft_apply(one.data_ptr(), 1, nt, moms, -1, out.ctypes.data, p2.P2_HOST, mode=p2.P2_SPLIT_FP16)
+    out = out.reshape(nt, len(moms))
+    assert np.abs(out[:, 0] - ctx.V3).max() < 1e-6 * ctx.V3 and np.abs(out[:, 1:]).max() < 1e-6 * ctx.V3
+    ctx.close()
