@@ -500,10 +500,28 @@ __device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt,
   const R third = R(1) / R(3);
   // iso-1/2 partial sums from G^{ud} / G^{du}, completed by the G^{uu} / G^{dd} terms
   // G^{ud} (A = u) and its lane transpose G^{du} (A = d; C g_k is symmetric)
+  // FP64: C g_1 and C g_2 from the shared diagonal products ga = P00 - P22,
+  // gb = P11 - P33 (8 products instead of 12); in FP32 holding ga and gb
+  // across the loop spills, which costs more than the 4 products it saves
+  constexpr bool kShare = sizeof(R) == 8;
+  Cx<R> ga[9], gb[9];
+  if (kShare) {
+#pragma unroll
+    for (int i = 0; i < 9; i++) ga[i] = gb[i] = czero<R>();
+    diquark_acc(row, kU, kD, 0, 0, R(1), xp, yp, ga);
+    diquark_acc(row, kU, kD, 2, 2, R(-1), xp, yp, ga);
+    diquark_acc(row, kU, kD, 1, 1, R(1), xp, yp, gb);
+    diquark_acc(row, kU, kD, 3, 3, R(-1), xp, yp, gb);
+  }
 #pragma unroll 1
   for (int g = 0; g < 3; g++) {
     Cx<R> q[9], D[9];
-    diquark_G(row, kU, kD, c_delta_sink[g], xp, yp, q);
+    if (kShare && g < 2) {
+#pragma unroll
+      for (int i = 0; i < 9; i++) q[i] = g == 0 ? ga[i] - gb[i] : ga[i] + gb[i];
+    } else {
+      diquark_G(row, kU, kD, c_delta_sink[g], xp, yp, q);
+    }
     const DiquarkLane dl = unpack_diquark_lane(g == 0 ? lt.delta[0] : g == 1 ? lt.delta[1] : lt.delta[2]);
     diquark_D(q, R(4 * dl.sN), mask, g == 2 ? 1 : 0, D);  // cN = 4, cL = 0
     part(g, 0, cscale(diquark_eval<true, true>(q, row, kU, dl, l, mask, -4, 0, 2, -2, D), third));
