@@ -230,3 +230,19 @@ def test_ft_apply_split_matches_oracle(decay):
     out = out.reshape(nt, len(moms))
     assert np.abs(out[:, 0] - ctx.V3).max() < 1e-6 * ctx.V3 and np.abs(out[:, 1:]).max() < 1e-6 * ctx.V3
     ctx.close()
+
+
+def test_ft_apply_split_odd_volume():
+    import oracle_py as orc
+    ctx = p2.Context((3, 5, 3, 2))  # V3 = 45
+    dof, nt = 5, 2
+    rng = np.random.default_rng(8)
+    f = rng.standard_normal((dof, ctx.V3 * nt)) + 1j * rng.standard_normal((dof, ctx.V3 * nt))
+    fd = torch.from_numpy(f.reshape(-1)).cuda()
+    moms = p2.mom_list(3)
+    ref = orc.ft(ctx.L, f, dof, nt, moms, -1)
+    out = np.zeros(nt * dof * len(moms), dtype=np.complex128)
+    ctx.ft_apply(fd.data_ptr(), dof, nt, moms, -1, out.ctypes.data, p2.P2_HOST, mode=p2.P2_SPLIT_FP16)
+    asum = np.abs(f).reshape(dof, nt, ctx.V3).sum(axis=2).T
+    assert (np.abs(out.reshape(ref.shape) - ref).max(axis=2) / asum).max() < 1e-6
+    ctx.close()

@@ -126,3 +126,22 @@ def test_split_host_propagators_converted_on_host(decay):
     err = per_t_error(host, what, 8, moms, ref, taus)
     assert err.max() < 1e-6, err
     ctx.close()
+
+
+def test_split_odd_spatial_volume():
+    """V3 = 27 (odd): site pairs of the projection are not 16-byte aligned,
+    tiles are ragged, and the host conversion writes unaligned rows; device
+    and host propagators give the same result within the bound."""
+    ctx = p2.Context((3, 3, 3, 6))
+    src = (2, 0, 1, 4)
+    bufs = device_props(ctx, [(41, 0), (41, 1)], t0=src[3])
+    what = p2.NUCLEON_CG5 | p2.MESON_G16 | p2.DELTA_ISO12
+    moms = p2.mom_list(2)
+    dev, _ = run(ctx, bufs, src, 6, what, moms=moms, mode=p2.P2_SPLIT_FP16)
+    host, _ = run(ctx, bufs, src, 6, what, moms=moms, mode=p2.P2_SPLIT_FP16, host_props=True, host_out=True)
+    assert np.array_equal(dev, host)
+    taus = list(range(6))
+    ref = oracle_blocks(ctx.L, bufs, src, moms, what, taus)
+    err = per_t_error(dev, what, 6, moms, ref, taus)
+    assert err.max() < 1e-6, err
+    ctx.close()

@@ -183,3 +183,21 @@ def test_split_fp32_propagators_and_transforms():
     err = _check(ctx, {"u": hu, "d": hd}, src, W, moms, out.cpu().numpy(), req)
     assert err < SPLIT_TOL, err
     ctx.close()
+
+
+@pytest.mark.parametrize("mode", [p2.P2_PLAIN_FP64, p2.P2_SPLIT_FP16])
+def test_odd_spatial_volume(mode):
+    ctx = p2.Context((3, 3, 3, 4))  # V3 = 27
+    src = (0, 2, 1, 3)
+    u, d = device_props(ctx, [(77, 0), (77, 1)], t0=src[3])
+    moms = p2.mom_list(1)
+    W = 4
+    req = ctx.udsc_request(src, W, 0, moms=moms, prop_u=0, prop_d=1, mode=mode)
+    n = len(p2.udsc_datasets(req))
+    out = torch.zeros(n * W * len(moms), dtype=torch.complex128, device="cuda")
+    req.out = out.data_ptr()
+    ctx.contract_udsc([ctx.prop(u.data_ptr()), ctx.prop(d.data_ptr())], req)
+    ctx.sync()
+    err = _check(ctx, {"u": u, "d": d}, src, W, moms, out.cpu().numpy(), req)
+    assert err < (TOL if mode == p2.P2_PLAIN_FP64 else SPLIT_TOL), err
+    ctx.close()
