@@ -258,6 +258,10 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
+    lw = int(os.environ.get("LOCAL_WORLD_SIZE", "1"))
+    if lw > 1 and "OMP_NUM_THREADS" not in os.environ:
+        # the host-side conversion of the end-to-end run: the node's cores shared between its ranks
+        os.environ["OMP_NUM_THREADS"] = str(max(1, (os.cpu_count() or lw) // lw))
     import torch
     torch.cuda.set_device(local)
     dist = None
@@ -382,7 +386,12 @@ def main():
         except Exception:
             avail = 0
         need = 2 * u.numel() * 16 + (8 << 30)
-        if avail > need:
+        ok = avail > need * int(os.environ.get("LOCAL_WORLD_SIZE", "1"))
+        if dist:  # every rank takes the same collective steps: all run it or none
+            flag = torch.tensor([1 if ok else 0], device="cuda")
+            dist.all_reduce(flag, op=dist.ReduceOp.MIN)
+            ok = bool(flag.item())
+        if ok:
             hu = torch.empty(u.numel(), dtype=torch.complex128, pin_memory=True)
             hd = torch.empty(u.numel(), dtype=torch.complex128, pin_memory=True)  # empty_like does not pin
             hu.copy_(u)
@@ -400,19 +409,26 @@ def main():
             torch.cuda.synchronize()
             ctx.profile(True)
             ctx.profile_read(reset=True)
+            if dist:
+                dist.barrier()
             t = time.perf_counter()
             n_e = max(1, min(args.steps, 3))
             for _ in range(n_e):
                 estep()
             torch.cuda.synchronize()
             el = (time.perf_counter() - t) / n_e
+            if dist:  # the slowest rank's wall clock
+                te = torch.tensor([el], device="cuda", dtype=torch.float64)
+                dist.all_reduce(te, op=dist.ReduceOp.MAX)
+                el = float(te.item())
             eprof = ctx.profile_read(reset=True)
             ctx.profile(False)
             e2e = {"value": sites * world / el, "unit": "sites/s", "h2d_bytes_per_step": 2 * hu.numel() * 16,
                    "d2h_bytes_per_step": total * 16, "steps": n_e, "timer": "host wall clock around the C-ABI call",
                    "device_ms_per_step": {k: v[1] / n_e for k, v in eprof.items()}}
         else:
-            e2e = {"value": None, "unit": "sites/s", "note": f"host memory {avail >> 30} GiB < {need >> 30} GiB"}
+            e2e = {"value": None, "unit": "sites/s",
+                   "note": f"host memory {avail >> 30} GiB < {need >> 30} GiB per rank on this node"}
 
     cpu = None
     if rank == 0 and not args.no_cpu:
