@@ -431,7 +431,7 @@ def main():
                    "note": f"host memory {avail >> 30} GiB < {need >> 30} GiB per rank on this node"}
 
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:  # the host baseline is reported at N = 1 only
         try:
             cpu = cpu_baseline_port(1)
         except Exception as ex:  # reported, not fatal
