@@ -29,6 +29,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../plegma2pt.h"
@@ -286,6 +287,14 @@ class PLEGMA_FT {
       momList.push_back(VFloat(m.begin(), m.end()));
     }
   }
+  // One momentum (lib/PLEGMA_FT.cu:23-31).
+  template <typename T, typename = typename std::enable_if<std::is_arithmetic<T>::value>::type>
+  PLEGMA_FT(std::vector<T> mom, int D3D4 = 3, bool accum = false, int dimT = -1)
+      : dims(D3D4), dimT(dimT < 0 ? Runtime::get().localL[DIM_T] : dimT), accum(accum) {
+    if (dims != 3) throw PLEGMA_exception("PLEGMA_FT: only 3-D transforms are supported");
+    if (mom.size() != 3) throw PLEGMA_exception("The size of the momentum vector does not match the dimensionality of FT");
+    momList.push_back(VFloat(mom.begin(), mom.end()));
+  }
   int Nmoms() const { return (int)momList.size(); }
   VVFloat MomList() const { return momList; }
   int Dims() const { return dims; }
@@ -503,6 +512,8 @@ class PLEGMA_Correlator {
   void setFixMomList(std::vector<std::vector<int>>& l) {
     corr_mom_space.reset(new PLEGMA_FT<Float>(l, 3, false, localT()));
   }
+  // One fixed momentum (include/PLEGMA_Correlator.h:135-138).
+  void setFixMomVec(std::vector<int>& v) { corr_mom_space.reset(new PLEGMA_FT<Float>(v, 3, false, localT())); }
   std::vector<std::vector<int>> getMomList() const {
     std::vector<std::vector<int>> out;
     if (corr_space != MOMENTUM_SPACE) return out;

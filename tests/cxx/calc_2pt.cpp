@@ -37,6 +37,14 @@ int main(int argc, char** argv) {
     mes.writeFile(out + "_mesons_all", DEFAULT_FORMAT);
     mes.writeFile(out + "_mesons_all", ASCII_FORMAT);
 
+    // one fixed momentum (the reference's setFixMomVec), nucleon
+    PLEGMA_Correlator<double> fix(MOMENTUM_SPACE, src, q2max, totalT);
+    std::vector<int> pfix{1, 0, -1};
+    fix.setFixMomVec(pfix);
+    fix.setMode(mode);
+    fix.contractBaryons(up, dn, false);
+    fix.writeFile(out + "_baryons_fixmom", DEFAULT_FORMAT);
+
     PLEGMA_Correlator<double> m10(MOMENTUM_SPACE, src, q2max, totalT);
     m10.setMode(mode);
     m10.contractMesons(up, dn);

@@ -197,3 +197,16 @@ def test_absorb(outputs):
     (base,) = device_props(ctx, [(5, 0)], t0=0)
     expect = orc.prop_absorb(base.cpu().numpy(), vec3, V3, 0, L[3], L[3], 1, 2, True, SRC[3])
     assert np.array_equal(sliced, expect)
+
+
+def test_fixed_momentum_vector(outputs):
+    """setFixMomVec({1, 0, -1}) (include/PLEGMA_Correlator.h:135-138): one
+    momentum, the same values as that momentum of the Q^2 list."""
+    prefix, ctx, bufs, moms = outputs
+    meta, v = load(prefix + "_baryons_fixmom")
+    assert meta["mvec"] == [[1, 0, -1]]
+    _, full = load(prefix + "_baryons")
+    p = [i for i, m in enumerate(moms.tolist()) if m == [1, 0, -1]][0]
+    ref = full.reshape(2, TOTALT, len(moms), 16)[:, :, p, :]
+    got = v.reshape(2, TOTALT, 1, 16)[:, :, 0, :]
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
