@@ -40,33 +40,55 @@ constexpr int kStage = kSitesPerTile * kRow;
 // CM = true: component-major [flavour * 144 + component][16 sites], written
 // without bank conflicts and transposed by the split kernel's conversion.
 template <typename Tin, bool CM = false>
-__device__ __forceinline__ void issue_tile(const ContractArgs& a, Cx<Tin>* st, long long tile, long long ntiles,
-                                           int tiles_per_tau, int f0 = 0, int f1 = 2) {
-  if (tile < ntiles) {
-    const int tl = (int)(tile / tiles_per_tau);
+__device__ __forceinline__ void issue_tile(const ContractArgs& a, Cx<Tin>* st, int tl, int x0, bool valid) {
+  if (valid) {
     const int s = threadIdx.x & (kSitesPerTile - 1);
-    const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + s;
+    const int x = x0 + s;
     const bool ok = x < a.V3;
     const SliceDesc* sd = a.sl + tl;
     // thread i copies component i/16 + 16 r of site i%16; with 256 threads
     // rows r < 9 are the u view's 144 components and r >= 9 the d view's
 #pragma unroll
-    for (int f = f0; f < f1; f++) {
-      const Cx<Tin>* src = (const Cx<Tin>*)(f ? sd->d : sd->u) + (f ? sd->off_d : sd->off_u) + (ok ? x : 0);
+    for (int f = 0; f < 2; f++) {
       const long long vol = f ? sd->vol_d : sd->vol_u;
+      const Cx<Tin>* src = (const Cx<Tin>*)(f ? sd->d : sd->u) + (f ? sd->off_d : sd->off_u) + (ok ? x : 0) +
+                           (threadIdx.x >> 4) * vol;
+      const long long step = 16 * vol;
 #pragma unroll 3
       for (int r = 0; r < 9; r++) {
         const int comp = (threadIdx.x >> 4) + 16 * r;
         Cx<Tin>* dst = CM ? st + (144 * f + comp) * kSitesPerTile + s : st + s * kRow + 144 * f + comp;
         if (sizeof(Tin) == 8)
-          cp_async16(dst, src + comp * vol, ok ? 16 : 0);
+          cp_async16(dst, src, ok ? 16 : 0);
         else
-          cp_async8(dst, src + comp * vol, ok ? 8 : 0);
+          cp_async8(dst, src, ok ? 8 : 0);
+        src += step;
       }
     }
   }
   cp_async_commit();
 }
+
+// Position (slice tl, tile rem of the slice) of a CTA's persistent walk over
+// the tiles, advanced by the grid size without divisions: gridDim.x =
+// q tiles_per_tau + r, so one step adds q slices and r tiles with a carry.
+struct TileCursor {
+  int tl, rem, q, r, tpt;
+  __device__ __forceinline__ TileCursor(int start, int step, int tiles_per_tau)
+      : tl(start / tiles_per_tau), rem(start % tiles_per_tau), q(step / tiles_per_tau), r(step % tiles_per_tau),
+        tpt(tiles_per_tau) {}
+  __device__ __forceinline__ TileCursor next() const {
+    TileCursor n = *this;
+    n.tl += q;
+    n.rem += r;
+    if (n.rem >= tpt) {
+      n.rem -= tpt;
+      n.tl++;
+    }
+    return n;
+  }
+  __device__ __forceinline__ int x0() const { return rem * kSitesPerTile; }
+};
 static_assert(kThreads == 256 && kSitesPerTile == 16, "issue_tile maps 256 threads onto 16 sites x 16 components");
 
 // Index of a diagonal structure in the 10-structure list (1, g5, g1..g4,
@@ -83,14 +105,18 @@ __device__ __forceinline__ int* smax_slot(Cx<float>* sf, int k) {
   return reinterpret_cast<int*>(sf + s * kRow32 + 2 * row32_unit(j, 4) + 1) + (k & 1);
 }
 
-// Split form, 16 x 16 mesons: the outputs of a tile are staged in shared
-// memory as [g2][g1][site] (rows of 16 sites padded to 17, so the 16 lanes of
-// a half-warp, which hold 16 different g1, write 16 different bank pairs) and
-// written to HBM row by row, 128 contiguous bytes per component, by
-// flush_g16 below; direct stores from the lanes would touch 16 component rows
-// per instruction.
-constexpr int kG16Row = 17;
-constexpr int kG16Bytes = 256 * kG16Row * (int)sizeof(Cx<float>);
+// Split form, 16 x 16 mesons: a half-warp reads only its own site's FP32 row,
+// so once its contraction is done it stages the site's 256 outputs in that
+// row, output j = 16 g2 + g1 at complex 10 (j >> 3) + (j & 7): the four data
+// units of every block (the colour-8 and spare slots keep their contents, the
+// spare slots holding the per-component maxima).  The flush after the tile
+// writes them to HBM, 128 contiguous bytes per component; direct stores from
+// the lanes would touch 16 component rows per instruction.  The staging
+// buffer stays free for the whole next tile's copies.
+__device__ __forceinline__ int g16_slot(int g1, int g2) {
+  const int j = 16 * g2 + g1;
+  return 10 * (j >> 3) + (j & 7);
+}
 
 template <typename R>
 struct Writer {
@@ -98,7 +124,7 @@ struct Writer {
   long long V3;
   float* rmax;          // split form: this lane's running maxima of its nucleon outputs (slots 0, 1)
   Cx<float>* smax_base;  // split form: tile whose spare slots hold the per-component maxima, or null
-  Cx<R>* g16;           // split form: the tile's 16 x 16 meson staging, or null (direct stores)
+  Cx<R>* g16;           // split form: this site's FP32 row, reused as its 16 x 16 meson staging; or null
   int site;             // site of the tile
   __device__ __forceinline__ void put(int k, Cx<R> v) const {
     out[(long long)k * V3] = v;
@@ -156,11 +182,12 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
     meson_site(row, kU, kD, lt, l, mask, c);
     if (a.what & 8u) {
       if (w.g16) {
+        __syncwarp(mask);  // every lane of the half-warp has finished reading the row
 #pragma unroll
-        for (int g2 = 0; g2 < 16; g2++) w.g16[(g2 * 16 + g1) * kG16Row + w.site] = c[g2];
-      } else {
+        for (int g2 = 0; g2 < 16; g2++) w.g16[g16_slot(g1, g2)] = c[g2];
+      } else {  // direct stores (plain form, or split form with the 10 diagonal structures: maxima in shared memory)
 #pragma unroll
-        for (int g2 = 0; g2 < 16; g2++) w.out[(long long)(a.k.g16 + g1 * 16 + g2) * w.V3] = c[g2];
+        for (int g2 = 0; g2 < 16; g2++) w.put(a.k.g16 + g1 * 16 + g2, c[g2]);
       }
     }
     if (a.what & 16u) {
@@ -207,17 +234,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
   const LaneTables lt = load_lane_tables(l);
 
   const int tiles_per_tau = (a.V3 + kSitesPerTile - 1) / kSitesPerTile;
-  const long long ntiles = (long long)a.ntau * tiles_per_tau;
-  long long tile = blockIdx.x;
+  TileCursor cur(blockIdx.x, gridDim.x, tiles_per_tau);
+  TileCursor nx2 = cur.next();
+  issue_tile<double>(a, sm, cur.tl, cur.x0(), cur.tl < a.ntau);
+  issue_tile<double>(a, sm + kStage, nx2.tl, nx2.x0(), nx2.tl < a.ntau);
 
-  issue_tile<double>(a, sm, tile, ntiles, tiles_per_tau);
-  issue_tile<double>(a, sm + kStage, tile + gridDim.x, ntiles, tiles_per_tau);
-
-  for (int it = 0; tile < ntiles; tile += gridDim.x, it++) {
+  for (int it = 0; cur.tl < a.ntau; cur = cur.next(), it++) {
     Cx<double>* st = sm + (it & 1) * kStage;
     cp_async_wait<1>();
     __syncthreads();
-    const int tl = (int)(tile / tiles_per_tau);
+    const int tl = cur.tl;
     {
       // load-time transform of the staged tile, in place (uniform per tile)
       const int xfu = a.sl[tl].xf[0], xfd = a.sl[tl].xf[1];
@@ -233,14 +259,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
         __syncthreads();
       }
     }
-    const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile + hw;
+    const int x = cur.x0() + hw;
     if (x < a.V3) {
       const RowF64 row{st + hw * kRow};
       const Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr, nullptr, nullptr, hw};
       contract_site<DELTA>(a, row, lt, l, mask, w);
     }
     __syncthreads();
-    issue_tile<double>(a, st, tile + 2LL * gridDim.x, ntiles, tiles_per_tau);
+    nx2 = nx2.next();  // two tiles ahead of the next iteration's
+    issue_tile<double>(a, st, nx2.tl, nx2.x0(), nx2.tl < a.ntau);
   }
   cp_async_wait<0>();
 }
@@ -248,9 +275,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
 // Split form: FP32 arithmetic on power-of-two scaled inputs.  One staging
 // buffer in the input precision (component-major) plus an FP32 copy of the
 // tile in the padded row layout of RowF32: the staging buffer is refilled
-// with the next tile's cp.async as soon as the current one is converted (the
-// part of it that holds the staged meson outputs after the flush), so two
-// CTAs (16 warps) fit on an SM.
+// with the whole next tile's cp.async as soon as the current one is
+// converted, so the copies overlap the contraction, and two CTAs (16 warps)
+// fit on an SM.
 constexpr int kStage32 = kSitesPerTile * kRow32;
 
 template <typename Tin, bool DELTA>
@@ -258,24 +285,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<Tin>* st = (Cx<Tin>*)smem_raw;
   Cx<float>* sf = (Cx<float>*)(smem_raw + kSitesPerTile * 288 * sizeof(Cx<Tin>));
-  // 16 x 16 meson staging: with FP64 inputs the d half of the staging buffer,
-  // which is idle while a tile is contracted (only the u half of the next
-  // tile is in flight then; the d half follows the flush); with FP32 inputs
-  // a buffer of its own after the FP32 tile
-  constexpr bool kAlias = sizeof(Tin) == 8;
-  Cx<float>* og = kAlias ? (Cx<float>*)(st + 144 * kSitesPerTile) : sf + kStage32;
-  const bool stage = !DELTA && (a.what & 8u);
+  // 16 x 16 meson outputs staged in the sites' own FP32 rows (not with the
+  // 10 diagonal structures, whose second pass reads the rows again)
+  const bool stage = !DELTA && (a.what & 8u) && !(a.what & 64u);
   const int tid = threadIdx.x;
   const int hw = tid >> 4, l = tid & 15;
   const unsigned mask = halfwarp_mask();
   const LaneTables lt = load_lane_tables(l);
 
   const int tiles_per_tau = (a.V3 + kSitesPerTile - 1) / kSitesPerTile;
-  const long long ntiles = (long long)a.ntau * tiles_per_tau;
-  long long tile = blockIdx.x;
+  TileCursor tc(blockIdx.x, gridDim.x, tiles_per_tau);
   for (int k = tid; k < a.K; k += kThreads) *smax_slot(sf, k) = 0;
 
-  issue_tile<Tin, true>(a, st, tile, ntiles, tiles_per_tau);
+  issue_tile<Tin, true>(a, st, tc.tl, tc.x0(), tc.tl < a.ntau);
 
   int cur = -1;  // slice whose maxima the spare slots hold
   // running maxima in registers: nucleon outputs of lane l (slots 0, 1) and
@@ -308,8 +330,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
       }
     }
   };
-  for (; tile < ntiles; tile += gridDim.x) {
-    const int tl = (int)(tile / tiles_per_tau);
+  for (; tc.tl < a.ntau; tc = tc.next()) {
+    const int tl = tc.tl;
     if (tl != cur && cur >= 0) flush_lane();
     cp_async_wait<0>();
     __syncthreads();
@@ -359,12 +381,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
     }
     __syncthreads();
     // the staged tile has been converted: refill the staging buffer while contracting
-    issue_tile<Tin, true>(a, st, tile + gridDim.x, ntiles, tiles_per_tau, 0, (kAlias && stage) ? 1 : 2);
-    const int x0 = (int)(tile - (long long)tl * tiles_per_tau) * kSitesPerTile;
+    {
+      const TileCursor nx = tc.next();
+      issue_tile<Tin, true>(a, st, nx.tl, nx.x0(), nx.tl < a.ntau);
+    }
+    const int x0 = tc.x0();
     if (x0 + hw < a.V3) {
       const RowF32 row{sf + hw * kRow32};
       const Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x0 + hw, a.V3, DELTA ? nullptr : rmax, sf,
-                            stage ? og : nullptr, hw};
+                            stage ? sf + hw * kRow32 : nullptr, hw};
       contract_site<DELTA>(a, row, lt, l, mask, w);
     }
     if constexpr (!DELTA) {
@@ -377,14 +402,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
           Cx<float>* o = (Cx<float>*)a.out + ((long long)tl * a.K + a.k.g16 + 16 * hw) * a.V3 + x0 + s;
 #pragma unroll
           for (int g2 = 0; g2 < 16; g2++) {
-            const Cx<float> v = og[(g2 * 16 + hw) * kG16Row + s];
+            const Cx<float> v = sf[s * kRow32 + g16_slot(hw, g2)];
             o[(long long)g2 * a.V3] = v;
             rmax[2 + g2] = fmaxf(rmax[2 + g2], fmaxf(fabsf(v.x), fabsf(v.y)));
           }
-        }
-        if (kAlias) {
-          __syncthreads();
-          issue_tile<Tin, true>(a, st, tile + gridDim.x, ntiles, tiles_per_tau, 1, 2);
         }
       }
     }
@@ -457,8 +478,7 @@ cudaError_t launch_plain_t(const ContractArgs& a, int grid, cudaStream_t s) {
 
 template <typename Tin, bool DELTA>
 cudaError_t launch_f32_t(const ContractArgs& a, int grid, cudaStream_t s) {
-  const int smem = kSitesPerTile * 288 * (int)sizeof(Cx<Tin>) + kStage32 * (int)sizeof(Cx<float>) +
-                   ((!DELTA && sizeof(Tin) == 4) ? kG16Bytes : 0);
+  const int smem = kSitesPerTile * 288 * (int)sizeof(Cx<Tin>) + kStage32 * (int)sizeof(Cx<float>);
   if (a.K > 2 * 32 * kSitesPerTile) return cudaErrorInvalidValue;  // more components than spare slots
   cudaError_t e = ensure_smem((const void*)k_contract_f32<Tin, DELTA>, smem);
   if (e != cudaSuccess) return e;
