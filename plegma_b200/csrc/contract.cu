@@ -69,26 +69,6 @@ __device__ __forceinline__ void issue_tile(const ContractArgs& a, Cx<Tin>* st, i
   cp_async_commit();
 }
 
-// Position (slice tl, tile rem of the slice) of a CTA's persistent walk over
-// the tiles, advanced by the grid size without divisions: gridDim.x =
-// q tiles_per_tau + r, so one step adds q slices and r tiles with a carry.
-struct TileCursor {
-  int tl, rem, q, r, tpt;
-  __device__ __forceinline__ TileCursor(int start, int step, int tiles_per_tau)
-      : tl(start / tiles_per_tau), rem(start % tiles_per_tau), q(step / tiles_per_tau), r(step % tiles_per_tau),
-        tpt(tiles_per_tau) {}
-  __device__ __forceinline__ TileCursor next() const {
-    TileCursor n = *this;
-    n.tl += q;
-    n.rem += r;
-    if (n.rem >= tpt) {
-      n.rem -= tpt;
-      n.tl++;
-    }
-    return n;
-  }
-  __device__ __forceinline__ int x0() const { return rem * kSitesPerTile; }
-};
 static_assert(kThreads == 256 && kSitesPerTile == 16, "issue_tile maps 256 threads onto 16 sites x 16 components");
 
 // Index of a diagonal structure in the 10-structure list (1, g5, g1..g4,

@@ -148,6 +148,27 @@ __device__ __forceinline__ Cx<R> shfl_idx16(Cx<R> v, int src, unsigned mask) {
   return cx<R>(__shfl_sync(mask, v.x, src, 16), __shfl_sync(mask, v.y, src, 16));
 }
 
+// Position (slice tl, tile rem of the slice) of a CTA's persistent walk over
+// the tiles, advanced by the grid size without divisions: gridDim.x =
+// q tiles_per_tau + r, so one step adds q slices and r tiles with a carry.
+struct TileCursor {
+  int tl, rem, q, r, tpt;
+  __device__ __forceinline__ TileCursor(int start, int step, int tiles_per_tau)
+      : tl(start / tiles_per_tau), rem(start % tiles_per_tau), q(step / tiles_per_tau), r(step % tiles_per_tau),
+        tpt(tiles_per_tau) {}
+  __device__ __forceinline__ TileCursor next() const {
+    TileCursor n = *this;
+    n.tl += q;
+    n.rem += r;
+    if (n.rem >= tpt) {
+      n.rem -= tpt;
+      n.tl++;
+    }
+    return n;
+  }
+  __device__ __forceinline__ int x0() const { return rem * 16; }  // first site of the 16-site tile
+};
+
 // Asynchronous global -> shared copies (LDGSTS).  Bytes beyond src_bytes are zero-filled.
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);

@@ -64,12 +64,11 @@ struct UdscArgs {
   Cx<double>* out;  // [ntau][nd][V3]
 };
 
-__device__ __forceinline__ void issue_tile_u(const UdscArgs& a, Cx<double>* st, long long tile, long long ntiles,
-                                             int tiles_per_tau) {
-  if (tile < ntiles) {
-    const int tl = (int)(tile / tiles_per_tau);
+__device__ __forceinline__ void issue_tile_u(const UdscArgs& a, Cx<double>* st, const TileCursor& t, int ntau) {
+  if (t.tl < ntau) {
+    const int tl = t.tl;
     const int s = threadIdx.x & (kSitesU - 1);
-    const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesU + s;
+    const int x = t.x0() + s;
     const bool ok = x < a.V3;
     const UdscSlice* sd = a.sl + tl;
     // thread i copies component i/16 + 16 r of site i%16: rows r < 9 are P1,
@@ -96,17 +95,17 @@ __global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc(const UdscArgs a
   const int hw = tid >> 4, l = tid & 15;
   const unsigned mask = halfwarp_mask();
   const int tiles_per_tau = (a.V3 + kSitesU - 1) / kSitesU;
-  const long long ntiles = (long long)a.ntau * tiles_per_tau;
-  long long tile = blockIdx.x;
+  TileCursor cur(blockIdx.x, gridDim.x, tiles_per_tau);
+  TileCursor nx2 = cur.next();
   const int* stream0 = a.plan + a.plan[l];
 
-  issue_tile_u(a, sm, tile, ntiles, tiles_per_tau);
-  issue_tile_u(a, sm + kStageU, tile + gridDim.x, ntiles, tiles_per_tau);
-  for (int it = 0; tile < ntiles; tile += gridDim.x, it++) {
+  issue_tile_u(a, sm, cur, a.ntau);
+  issue_tile_u(a, sm + kStageU, nx2, a.ntau);
+  for (int it = 0; cur.tl < a.ntau; cur = cur.next(), it++) {
     Cx<double>* st = sm + (it & 1) * kStageU;
     cp_async_wait<1>();
     __syncthreads();
-    const int tl = (int)(tile / tiles_per_tau);
+    const int tl = cur.tl;
     {
       // load-time transforms of the staged tile, in place (uniform per tile)
       const UdscSlice& sd = a.sl[tl];
@@ -122,7 +121,7 @@ __global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc(const UdscArgs a
         __syncthreads();
       }
     }
-    const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesU + hw;
+    const int x = cur.x0() + hw;
     if (x < a.V3) {
       const RowF64 row{st + hw * kRowU};
       Cx<double> acc[kMaxDs];
@@ -171,7 +170,8 @@ __global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc(const UdscArgs a
       }
     }
     __syncthreads();
-    issue_tile_u(a, st, tile + 2LL * gridDim.x, ntiles, tiles_per_tau);
+    nx2 = nx2.next();  // two tiles ahead of the next iteration's
+    issue_tile_u(a, st, nx2, a.ntau);
   }
   cp_async_wait<0>();
 }
@@ -246,12 +246,11 @@ __global__ void k_sample_udsc(const UdscArgsF32 a) {
 }
 
 template <typename Tin>
-__device__ __forceinline__ void issue_tile_u32(const UdscArgsF32& a, Cx<Tin>* st, long long tile, long long ntiles,
-                                               int tiles_per_tau) {
-  if (tile < ntiles) {
-    const int tl = (int)(tile / tiles_per_tau);
+__device__ __forceinline__ void issue_tile_u32(const UdscArgsF32& a, Cx<Tin>* st, const TileCursor& t, int ntau) {
+  if (t.tl < ntau) {
+    const int tl = t.tl;
     const int s = threadIdx.x & (kSitesU - 1);
-    const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesU + s;
+    const int x = t.x0() + s;
     const bool ok = x < a.V3;
     const UdscSlice* sd = a.sl + tl;
     // component-major staging [view * 144 + component][16 sites]: thread i
@@ -283,15 +282,14 @@ __global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc_f32(const UdscAr
   const int hw = tid >> 4, l = tid & 15;
   const unsigned mask = halfwarp_mask();
   const int tiles_per_tau = (a.V3 + kSitesU - 1) / kSitesU;
-  const long long ntiles = (long long)a.ntau * tiles_per_tau;
-  long long tile = blockIdx.x;
+  TileCursor tc(blockIdx.x, gridDim.x, tiles_per_tau);
   const int* stream0 = a.plan + a.plan[l];
   if (tid < kMaxDs) smx[tid] = 0;
 
-  issue_tile_u32<Tin>(a, st, tile, ntiles, tiles_per_tau);
+  issue_tile_u32<Tin>(a, st, tc, a.ntau);
   int cur = -1;
-  for (; tile < ntiles; tile += gridDim.x) {
-    const int tl = (int)(tile / tiles_per_tau);
+  for (; tc.tl < a.ntau; tc = tc.next()) {
+    const int tl = tc.tl;
     cp_async_wait<0>();
     __syncthreads();
     if (tl != cur) {
@@ -332,8 +330,8 @@ __global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc_f32(const UdscAr
       }
     }
     __syncthreads();
-    issue_tile_u32<Tin>(a, st, tile + gridDim.x, ntiles, tiles_per_tau);
-    const int x = (int)(tile - (long long)tl * tiles_per_tau) * kSitesU + hw;
+    issue_tile_u32<Tin>(a, st, tc.next(), a.ntau);
+    const int x = tc.x0() + hw;
     if (x < a.V3) {
       const RowF32 row{sf + hw * kRowU32};
       Cx<float> acc[kMaxDs];
