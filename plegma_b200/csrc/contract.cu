@@ -105,7 +105,6 @@ struct Writer {
   float* rmax;          // split form: this lane's running maxima of its nucleon outputs (slots 0, 1)
   Cx<float>* smax_base;  // split form: tile whose spare slots hold the per-component maxima, or null
   Cx<R>* g16;           // split form: this site's FP32 row, reused as its 16 x 16 meson staging; or null
-  int site;             // site of the tile
   __device__ __forceinline__ void put(int k, Cx<R> v) const {
     out[(long long)k * V3] = v;
     if (smax_base) {
@@ -242,7 +241,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
     const int x = cur.x0() + hw;
     if (x < a.V3) {
       const RowF64 row{st + hw * kRow};
-      const Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr, nullptr, nullptr, hw};
+      const Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr, nullptr, nullptr};
       contract_site<DELTA>(a, row, lt, l, mask, w);
     }
     __syncthreads();
@@ -369,7 +368,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
     if (x0 + hw < a.V3) {
       const RowF32 row{sf + hw * kRow32};
       const Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x0 + hw, a.V3, DELTA ? nullptr : rmax, sf,
-                            stage ? sf + hw * kRow32 : nullptr, hw};
+                            stage ? sf + hw * kRow32 : nullptr};
       contract_site<DELTA>(a, row, lt, l, mask, w);
     }
     if constexpr (!DELTA) {
