@@ -523,6 +523,7 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request* reqs, con
     sa.nsplit = pa.nsplit;
     sa.nmom = pl.nmom;
     sa.K = pl.K;
+    if (pl.blocks.size() > (size_t)p2::kMaxBlocks) return c->fail(P2_ERR_INVALID_ARG, "too many result blocks");
     sa.nblocks = (int)pl.blocks.size();
     for (size_t b = 0; b < pl.blocks.size(); b++) sa.blk[b] = pl.blocks[b];
     sa.sl = sg.desc((int)ci);

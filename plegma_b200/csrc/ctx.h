@@ -61,6 +61,8 @@ constexpr BlockDef kBlocks[] = {
     {P2_MESON_DIAG10, 1, 2, 10},
 };
 constexpr unsigned kAllBits = 0x3FFu;
+// every block of a request has a slot in the reduction kernels' argument structs
+static_assert(sizeof(kBlocks) / sizeof(kBlocks[0]) <= (size_t)p2::kMaxBlocks, "kMaxBlocks too small for kBlocks");
 
 }  // namespace p2host
 

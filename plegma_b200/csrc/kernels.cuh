@@ -6,7 +6,7 @@
 
 namespace p2 {
 
-constexpr int kMaxBlocks = 8;
+constexpr int kMaxBlocks = 10;  // contraction blocks of a request (one per P2_* bit)
 
 // Where each contraction block's components sit inside the K components of a site.
 struct CompOffsets {

@@ -235,6 +235,7 @@ p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int
   rd.exps = exps;
   rd.kexp = kexp;
   rd.sl = dsl;
+  if (blocks.size() > (size_t)p2::kMaxBlocks) return c->fail(P2_ERR_INVALID_ARG, "too many result blocks");
   rd.nblocks = (int)blocks.size();
   for (size_t b = 0; b < blocks.size(); b++) rd.blk[b] = blocks[b];
   rd.out = out;

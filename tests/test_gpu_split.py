@@ -145,3 +145,24 @@ def test_split_odd_spatial_volume():
     err = per_t_error(dev, what, 6, moms, ref, taus)
     assert err.max() < 1e-6, err
     ctx.close()
+
+
+@pytest.mark.parametrize("mode", [p2.P2_PLAIN_FP64, p2.P2_SPLIT_FP16])
+def test_every_contraction_block_in_one_request(mode):
+    """All ten blocks at once (K = 640: both kernel instantiations, the 16 x 16
+    mesons beside the 10 diagonal structures, the second nucleon
+    interpolator), host output, a window that wraps."""
+    ctx = p2.Context((4, 3, 4, 6))
+    src = (2, 1, 3, 4)
+    bufs = device_props(ctx, [(51, 0), (51, 1)], t0=src[3])
+    what = 0
+    for b in p2.BLOCKS:
+        what |= b[0]
+    assert p2.components(what) == 640
+    moms = p2.mom_list(1)
+    out, _ = run(ctx, bufs, src, 6, what, moms=moms, mode=mode, host_out=True)
+    taus = list(range(6))
+    ref = oracle_blocks(ctx.L, bufs, src, moms, what, taus)
+    err = per_t_error(out, what, 6, moms, ref, taus)
+    assert err.max() < (1e-12 if mode == p2.P2_PLAIN_FP64 else 1e-6), err
+    ctx.close()
