@@ -166,3 +166,22 @@ def test_every_contraction_block_in_one_request(mode):
     err = per_t_error(out, what, 6, moms, ref, taus)
     assert err.max() < (1e-12 if mode == p2.P2_PLAIN_FP64 else 1e-6), err
     ctx.close()
+
+
+@pytest.mark.parametrize("q2max", [0, 16])
+def test_split_momentum_list_extremes(q2max):
+    """One momentum (a single cos row) and |n|^2 <= 16 (257 momenta: 257 phase
+    rows in three 128-row tiles, the batched 64^3 x 128 configuration's
+    list) against the oracle."""
+    ctx = p2.Context((6, 5, 4, 4))
+    src = (3, 1, 2, 1)
+    bufs = device_props(ctx, [(61, 0), (61, 1)], t0=src[3])
+    what = p2.NUCLEON_CG5 | p2.MESON_G16
+    moms = p2.mom_list(q2max)
+    assert len(moms) == (1 if q2max == 0 else 257)
+    out, _ = run(ctx, bufs, src, 4, what, moms=moms, mode=p2.P2_SPLIT_FP16)
+    taus = list(range(4))
+    ref = oracle_blocks(ctx.L, bufs, src, moms, what, taus)
+    err = per_t_error(out, what, 4, moms, ref, taus)
+    assert err.max() < 1e-6, err
+    ctx.close()
