@@ -48,15 +48,18 @@ constexpr int kKS = 64;                   // sites per k-step
 constexpr int kATile = 128 * kKS * 2;     // bytes of one 128 x 64 FP16 tile
 
 __host__ __device__ constexpr int b_tile_bytes(int NT) { return 2 * NT * kKS * 2; }
-// phase (A) stages: three when they fit beside the two B stages, so that each
-// k-step's phase copy is issued one k-step ahead of its MMAs
+// Stage counts: B (converted operand) stages let the converters run ahead of
+// the MMAs, phase (A) stages let each k-step's phase copy be issued ahead.
+// Two B stages and, where they fit, three A stages: measured at 48^3 x 16,
+// three A stages beat three B stages (1.01 vs 1.08 ms at 123 momenta).
 constexpr int kSmemMax = 232448;
-__host__ __device__ constexpr int a_stages(int NT) {
-  return 2 * 2 * b_tile_bytes(NT) + 3 * 2 * kATile + 64 + 1024 <= kSmemMax ? 3 : 2;
+constexpr int kBarBytes = 128;  // mbarriers, TMEM address, error flag
+__host__ __device__ constexpr int stage_bytes(int NT, int nb, int na) {
+  return nb * 2 * b_tile_bytes(NT) + na * 2 * kATile + kBarBytes + 1024;
 }
-__host__ __device__ constexpr int smem_bytes(int NT) {
-  return 2 * 2 * b_tile_bytes(NT) + a_stages(NT) * 2 * kATile + 64 + 1024;
-}
+__host__ __device__ constexpr int b_stages(int) { return 2; }
+__host__ __device__ constexpr int a_stages(int NT) { return stage_bytes(NT, b_stages(NT), 3) <= kSmemMax ? 3 : 2; }
+__host__ __device__ constexpr int smem_bytes(int NT) { return stage_bytes(NT, b_stages(NT), a_stages(NT)); }
 __host__ __device__ constexpr int tmem_cols(int NT) {
   return 2 * NT <= 32 ? 32 : 2 * NT <= 64 ? 64 : 2 * NT <= 128 ? 128 : 2 * NT <= 256 ? 256 : 512;
 }
@@ -95,6 +98,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
   constexpr int NR = 2 * NT;                 // B rows (Re, Im per component)
   constexpr int BT = b_tile_bytes(NT);
   constexpr int NA = a_stages(NT);
+  constexpr int NB = b_stages(NT);
   constexpr int NH = NR > 256 ? 2 : 1;       // MMAs per product (N <= 256 each)
   constexpr int NM = NR / NH;
   constexpr uint32_t IDESC = tc::idesc_f16_f32(128, NM);
@@ -103,11 +107,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // the dynamic window is only guaranteed 16-byte aligned: round up to 1024
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char* sA = smem + 2 * 2 * BT;  // NA phase stages of 2 kATile (hi, lo) after the two B stages
+  unsigned char* sA = smem + NB * 2 * BT;  // NA phase stages of 2 kATile (hi, lo) after the NB B stages
   uint64_t* fullA = (uint64_t*)(sA + NA * 2 * kATile);
   uint64_t* done = fullA + 3;
-  uint64_t* fullB = done + 2;
-  uint32_t* tslot = (uint32_t*)(fullB + 2);
+  uint64_t* fullB = done + 3;
+  uint32_t* tslot = (uint32_t*)(fullB + 3);
   int* flag = (int*)(tslot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -123,7 +127,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
   }
   if (tid == 0) {
     for (int j = 0; j < NA; j++) tc::mbar_init(&fullA[j], 1);
-    for (int j = 0; j < 2; j++) {
+    for (int j = 0; j < NB; j++) {
       tc::mbar_init(&done[j], 1);
       tc::mbar_init(&fullB[j], kConvWarps);
     }
@@ -154,14 +158,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
         // whose MMAs must be complete
         const int next = i + NA - 2;
         if (next < nk && next > issued) {
-          if (next >= NA && !tc::mbar_wait(&done[(next - NA) & 1], ((next - NA) >> 1) & 1)) {
+          if (next >= NA && !tc::mbar_wait(&done[(next - NA) % NB], ((next - NA) / NB) & 1)) {
             failed = true;
             break;
           }
           issue_a(next);
         }
-        const int s = i & 1;
-        if (!tc::mbar_wait(&fullA[i % NA], (i / NA) & 1) || !tc::mbar_wait(&fullB[s], (i >> 1) & 1)) {
+        const int s = i % NB;
+        if (!tc::mbar_wait(&fullA[i % NA], (i / NA) & 1) || !tc::mbar_wait(&fullB[s], (i / NB) & 1)) {
           failed = true;
           break;
         }
@@ -186,7 +190,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
       }
       // the accumulators are complete (or, after a failure, no MMA or phase
       // copy is still in flight) before the block moves on
-      if (committed >= 0 && !tc::mbar_wait(&done[committed & 1], (committed >> 1) & 1)) failed = true;
+      if (committed >= 0 && !tc::mbar_wait(&done[committed % NB], (committed / NB) & 1)) failed = true;
       if (failed) {
         *flag = 1;
         for (int j = max(0, issued - NA + 1); j <= issued; j++)
@@ -238,9 +242,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
     };
     // one k-step; returns true when a wait timed out
     auto step = [&](int i, const float4 (&cur)[JN], float4 (&nxt)[JN]) -> bool {
-      const int s = i & 1;
+      const int s = i % NB;
       if (i + 1 < nk) load_b(ks0 + i + 1, nxt);
-      if (i >= 2 && !tc::mbar_wait(&done[s], ((i >> 1) - 1) & 1)) return true;
+      if (i >= NB && !tc::mbar_wait(&done[s], ((i / NB) - 1) & 1)) return true;
       unsigned char* Bh = smem + s * 2 * BT;
       unsigned char* Bl = Bh + BT;
 #pragma unroll
