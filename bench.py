@@ -120,7 +120,14 @@ def cpu_baseline_port(steps=1):
         orc.twopt(Ls, u, d, (1, 2, 3, 0), moms, 1 | 8, [1], want_abs=False)
         vals.append(V3 / (time.perf_counter() - t))
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": float(np.median(vals)), "unit": "sites/s", "cores": cores, "kind": "port",
+    model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            model = next((l.split(":", 1)[1].strip() for l in f if l.startswith("model name")), "")
+    except OSError:
+        pass
+    return {"value": float(np.median(vals)), "unit": "sites/s", "cores": cores, "cpu_model": model,
+            "nproc": os.cpu_count(), "kind": "port",
             "sample": f"1 time slice of 16^3 ({V3} sites), K=288, 123 momenta, FP64 oracle, median of {steps}"}
 
 
@@ -149,8 +156,8 @@ TRAFFIC_PER_SITE = {("contract_f32", "split"): 6857, ("contract_plain_fp64", "pl
 
 BATCHED = {
     # name: (lattice, sources, window range, |n|^2 max, propagator precision, decay, seed)
-    "batched_32x64": ((32, 32, 32, 64), 16, (8, 20), 9, "fp64", 0.5, 2024),
-    "batched_64x128": ((64, 64, 64, 128), 4, (32, 32), 16, "fp32", 0.4, 2025),
+    "batched_32x64": ((32, 32, 32, 64), 16, (8, 20), 9, "fp64", 0.5, 1004),
+    "batched_64x128": ((64, 64, 64, 128), 4, (32, 32), 16, "fp32", 0.4, 1005),
 }
 
 
@@ -226,6 +233,7 @@ def run_batched(name, stream, steps, warmup, forms=("split",)):
         g.close()
         del outs
     res["tuned_shapes"] = ctx.tune_count()
+    res["seed"] = seed
     ctx.close()
     del bufs
     torch.cuda.empty_cache()
@@ -456,7 +464,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "sites/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32+f16x2" if head == "split" else "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "form": head, "L": list(L), "K": K, "nmom": nmom,
+                "config": {"workload": WORKLOAD, "form": head, "L": list(L), "K": K, "nmom": nmom, "seed": SEED,
                            "sites_per_step": sites, "l2": "inputs (49 GB) larger than L2",
                            "parallelism": f"source-sharded x{world}"},
                 "forms": {k: {"ms_per_step": v["ms"], "sites_per_s": sites * world / (v["ms"] * 1e-3)}
