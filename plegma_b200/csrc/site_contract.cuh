@@ -265,41 +265,89 @@ __device__ __forceinline__ Cx<typename Row::R> diquark_slots(const Cx<typename R
                                                              const DiquarkLane& dl, int l, unsigned mask, int c1A,
                                                              int c1B, int c2A, int c2B) {
   typedef typename Row::R R;
-  const int mu = l >> 2, mup = l & 3;
   Cx<R> r = czero<R>();
-  if (S2) {
-    // slot 2 (reduce over x'): this lane's y' is mu'
-    const R f2 = R(c2A * dl.sA2 - c2B * dl.sB2);
+  // the four m of a slot reduced over four lanes as a reduce-scatter: the lane
+  // of bit b1 = bit hb of the lane index keeps m in {2 b1, 2 b1 + 1}, then the
+  // lane of bit b0 = bit lb keeps m = 2 b1 + b0
+  auto scatter = [&](Cx<R> (&P)[4], int hb, int lb) {
+    const bool b1 = (l >> hb) & 1, b0 = (l >> lb) & 1;
+    const Cx<R> s0 = b1 ? P[0] : P[2], s1 = b1 ? P[1] : P[3];
+    Cx<R> k0 = b1 ? P[2] : P[0], k1 = b1 ? P[3] : P[1];
+    k0 = k0 + shfl_xor16(s0, 1 << hb, mask);
+    k1 = k1 + shfl_xor16(s1, 1 << hb, mask);
+    const Cx<R> s = b0 ? k0 : k1;
+    const Cx<R> k = b0 ? k1 : k0;
+    return k + shfl_xor16(s, 1 << lb, mask);
+  };
+  if constexpr (sizeof(R) == 8) {
+    // FP64: one m at a time (four m of FP64 sums held at once spill)
+    const int mu = l >> 2, mup = l & 3;
+    if (S2) {
+      const R f2 = R(c2A * dl.sA2 - c2B * dl.sB2);
 #pragma unroll 1
+      for (int m = 0; m < 4; m++) {
+        Cx<R> z[9];
+        row.load9(Z + m * 4 + dl.z2, z);
+        Cx<R> p2 = czero<R>();
+#pragma unroll
+        for (int i = 0; i < 9; i++) cmac(p2, g[i], z[i]);
+        p2 = cscale(p2, f2);
+        p2 = p2 + shfl_xor16(p2, 4, mask);
+        p2 = p2 + shfl_xor16(p2, 8, mask);
+        if (m == mu) r = r + p2;
+      }
+    }
+    if (S1) {
+      const R f1 = R(-(c1A * dl.sA1 - c1B * dl.sB1));
+      const int src = mup << 2;
+#pragma unroll 1
+      for (int m = 0; m < 4; m++) {
+        Cx<R> z[9];
+        row.load9(Z + m * 4 + dl.z1, z);
+        Cx<R> p1 = czero<R>();
+#pragma unroll
+        for (int i = 0; i < 9; i++) cmac(p1, g[i], z[i]);
+        p1 = cscale(p1, f1);
+        p1 = p1 + shfl_xor16(p1, 1, mask);
+        p1 = p1 + shfl_xor16(p1, 2, mask);
+        const Cx<R> v = shfl_idx16(p1, src, mask);
+        if (m == mu) r = r + v;
+      }
+    }
+    return r;
+  }
+  if (S2) {
+    // slot 2 (sum over x'): lane (x', y' = mu') forms P[m] for T[m][mu'];
+    // after the scatter over x' (lane bits 3, 2) lane (x', mu') holds T[x'][mu']
+    const R f2 = R(c2A * dl.sA2 - c2B * dl.sB2);
+    Cx<R> P[4];
+#pragma unroll
     for (int m = 0; m < 4; m++) {
       Cx<R> z[9];
       row.load9(Z + m * 4 + dl.z2, z);
       Cx<R> p2 = czero<R>();
 #pragma unroll
       for (int i = 0; i < 9; i++) cmac(p2, g[i], z[i]);
-      p2 = cscale(p2, f2);
-      p2 = p2 + shfl_xor16(p2, 4, mask);
-      p2 = p2 + shfl_xor16(p2, 8, mask);
-      if (m == mu) r = r + p2;
+      P[m] = cscale(p2, f2);
     }
+    r = r + scatter(P, 3, 2);
   }
   if (S1) {
-    // slot 1 (reduce over y'): T[.][mu'] sits on lane (x' = mu', y' = 0)
+    // slot 1 (sum over y'): lane (x' = mu', y') forms P[m] for T[m][mu'];
+    // after the scatter over y' (lane bits 1, 0) lane (mu', y') holds
+    // T[y'][mu'], which lane (mu, mu') takes from the transposed lane
     const R f1 = R(-(c1A * dl.sA1 - c1B * dl.sB1));
-    const int src = mup << 2;
-#pragma unroll 1
+    Cx<R> P[4];
+#pragma unroll
     for (int m = 0; m < 4; m++) {
       Cx<R> z[9];
       row.load9(Z + m * 4 + dl.z1, z);
       Cx<R> p1 = czero<R>();
 #pragma unroll
       for (int i = 0; i < 9; i++) cmac(p1, g[i], z[i]);
-      p1 = cscale(p1, f1);
-      p1 = p1 + shfl_xor16(p1, 1, mask);
-      p1 = p1 + shfl_xor16(p1, 2, mask);
-      const Cx<R> v = shfl_idx16(p1, src, mask);
-      if (m == mu) r = r + v;
+      P[m] = cscale(p1, f1);
     }
+    r = r + shfl_idx16(scatter(P, 1, 0), ((l & 3) << 2) | (l >> 2), mask);
   }
   return r;
 }
