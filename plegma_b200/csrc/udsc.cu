@@ -20,8 +20,9 @@
 // and encodes one instruction stream per lane:
 //   per tuple: P1 block | P2 block << 8, four words of per-dataset entry
 //   counts (one byte each), then per entry: P3 block, Re w, Im w (float bits).
-// Each lane accumulates all datasets in registers; a half-warp reduction
-// gives the site's values, written to a [slice][dataset][site] buffer that
+// Each lane accumulates all datasets in registers; a half-warp reduce-scatter
+// (lane d ends with dataset d) gives the site's values, written to a
+// [slice][dataset][site] buffer that
 // the FP64 projection (project_fp64.cu) and the deterministic reduction
 // consume.
 #include <algorithm>
@@ -86,6 +87,23 @@ __device__ __forceinline__ void issue_tile_u(const UdscArgs& a, Cx<double>* st, 
     }
   }
   cp_async_commit();
+}
+
+// Sum of the 16 lanes' dataset accumulators, lane l ending with dataset l:
+// a reduce-scatter (8 + 4 + 2 + 1 exchanged values instead of 16 all-reduces).
+template <typename R>
+__device__ __forceinline__ Cx<R> reduce_scatter16(Cx<R> (&acc)[16], int l, unsigned mask) {
+#pragma unroll
+  for (int h = 8; h >= 1; h >>= 1) {
+    const bool up = (l & h) != 0;
+#pragma unroll
+    for (int j = 0; j < h; j++) {
+      const Cx<R> send = up ? acc[j] : acc[j + h];
+      const Cx<R> keep = up ? acc[j + h] : acc[j];
+      acc[j] = keep + shfl_xor16(send, h, mask);
+    }
+  }
+  return acc[0];
 }
 
 __global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc(const UdscArgs a) {
@@ -158,15 +176,21 @@ __global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc(const UdscArgs a
         }
       }
       Cx<double>* o = a.out + (long long)tl * a.nd * a.V3 + x;
+      if (a.nd > 4) {
+        static_assert(kMaxDs == 16, "the reduce-scatter spreads 16 datasets over the 16 lanes");
+        const Cx<double> v = reduce_scatter16(acc, l, mask);
+        if (l < a.nd) o[(long long)l * a.V3] = v;
+      } else {
 #pragma unroll
-      for (int d = 0; d < kMaxDs; d++) {
-        if (d >= a.nd) break;
-        Cx<double> v = acc[d];
-        v = v + shfl_xor16(v, 1, mask);
-        v = v + shfl_xor16(v, 2, mask);
-        v = v + shfl_xor16(v, 4, mask);
-        v = v + shfl_xor16(v, 8, mask);
-        if (l == d) o[(long long)d * a.V3] = v;
+        for (int d = 0; d < 4; d++) {
+          if (d >= a.nd) break;
+          Cx<double> v = acc[d];
+          v = v + shfl_xor16(v, 1, mask);
+          v = v + shfl_xor16(v, 2, mask);
+          v = v + shfl_xor16(v, 4, mask);
+          v = v + shfl_xor16(v, 8, mask);
+          if (l == d) o[(long long)d * a.V3] = v;
+        }
       }
     }
     __syncthreads();
@@ -367,17 +391,25 @@ __global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc_f32(const UdscAr
         }
       }
       Cx<float>* o = a.out + (long long)tl * a.nd * a.V3 + x;
+      if (a.nd > 4) {
+        const Cx<float> v = reduce_scatter16(acc, l, mask);
+        if (l < a.nd) {
+          o[(long long)l * a.V3] = v;
+          atomicMax(smx + l, __float_as_int(fmaxf(fabsf(v.x), fabsf(v.y))));
+        }
+      } else {
 #pragma unroll
-      for (int d = 0; d < kMaxDs; d++) {
-        if (d >= a.nd) break;
-        Cx<float> v = acc[d];
-        v = v + shfl_xor16(v, 1, mask);
-        v = v + shfl_xor16(v, 2, mask);
-        v = v + shfl_xor16(v, 4, mask);
-        v = v + shfl_xor16(v, 8, mask);
-        if (l == d) {
-          o[(long long)d * a.V3] = v;
-          atomicMax(smx + d, __float_as_int(fmaxf(fabsf(v.x), fabsf(v.y))));
+        for (int d = 0; d < 4; d++) {
+          if (d >= a.nd) break;
+          Cx<float> v = acc[d];
+          v = v + shfl_xor16(v, 1, mask);
+          v = v + shfl_xor16(v, 2, mask);
+          v = v + shfl_xor16(v, 4, mask);
+          v = v + shfl_xor16(v, 8, mask);
+          if (l == d) {
+            o[(long long)d * a.V3] = v;
+            atomicMax(smx + d, __float_as_int(fmaxf(fabsf(v.x), fabsf(v.y))));
+          }
         }
       }
     }
