@@ -158,7 +158,11 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
   const int g1 = lt.meson_g1();  // the sink Gamma of this lane's meson outputs
   if (a.what & (8u | 16u | 32u)) {
     Cx<R> c[16];
-    meson_site(row, kU, kD, lt, l, mask, c);
+    // staged 16 x 16 outputs leave their unit phases r_g1 r_g2 to the
+    // projection's reduction (g16_phase_deferred); the other blocks get them here
+    const bool phased = w.g16 == nullptr;
+    meson_site(row, kU, kD, lt, l, mask, phased, c);
+    auto val = [&](int g2) { return phased ? c[g2] : meson_phase(lt, g2, c[g2]); };
     if (a.what & 8u) {
       if (w.g16) {
         __syncwarp(mask);  // every lane of the half-warp has finished reading the row
@@ -170,32 +174,32 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
       }
     }
     if (a.what & 16u) {
-      if (g1 == 0) w.put(a.k.all34 + 0, c[0]);
-      if (g1 == 5) w.put(a.k.all34 + 1, c[5]);
+      if (g1 == 0) w.put(a.k.all34 + 0, val(0));
+      if (g1 == 5) w.put(a.k.all34 + 1, val(5));
       if (g1 >= 1 && g1 <= 4) {
 #pragma unroll
-        for (int g2 = 1; g2 <= 4; g2++) w.put(a.k.all34 + 2 + (g1 - 1) * 4 + (g2 - 1), c[g2]);
+        for (int g2 = 1; g2 <= 4; g2++) w.put(a.k.all34 + 2 + (g1 - 1) * 4 + (g2 - 1), val(g2));
       }
       if (g1 >= 6 && g1 <= 9) {
 #pragma unroll
-        for (int g2 = 6; g2 <= 9; g2++) w.put(a.k.all34 + 18 + (g1 - 6) * 4 + (g2 - 6), c[g2]);
+        for (int g2 = 6; g2 <= 9; g2++) w.put(a.k.all34 + 18 + (g1 - 6) * 4 + (g2 - 6), val(g2));
       }
     }
     if (a.what & 32u) {
       const int j = diag10_slot(g1);
 #pragma unroll
       for (int g2 = 0; g2 < 16; g2++)
-        if (g2 == g1 && j >= 0) w.put(a.k.new10 + j, c[g2]);
+        if (g2 == g1 && j >= 0) w.put(a.k.new10 + j, val(g2));
     }
   }
   if (a.what & 64u) {
     const int j = diag10_slot(g1);
     Cx<R> c[16];
-    meson_site(row, kU, kU, lt, l, mask, c);
+    meson_site(row, kU, kU, lt, l, mask, true, c);
 #pragma unroll
     for (int g2 = 0; g2 < 16; g2++)
       if (g2 == g1 && j >= 0) w.put(a.k.diag10 + j, c[g2]);
-    meson_site(row, kD, kD, lt, l, mask, c);
+    meson_site(row, kD, kD, lt, l, mask, true, c);
 #pragma unroll
     for (int g2 = 0; g2 < 16; g2++)
       if (g2 == g1 && j >= 0) w.put(a.k.diag10 + 10 + j, c[g2]);
@@ -266,7 +270,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
   Cx<float>* sf = (Cx<float>*)(smem_raw + kSitesPerTile * 288 * sizeof(Cx<Tin>));
   // 16 x 16 meson outputs staged in the sites' own FP32 rows (not with the
   // 10 diagonal structures, whose second pass reads the rows again)
-  const bool stage = !DELTA && (a.what & 8u) && !(a.what & 64u);
+  const bool stage = !DELTA && g16_phase_deferred(a.what);
   const int tid = threadIdx.x;
   const int hw = tid >> 4, l = tid & 15;
   const unsigned mask = halfwarp_mask();

@@ -242,5 +242,5 @@ void precision_release(p2_ctx* c);
 p2_status split_prepare_tables(p2_ctx* c, const p2host::Plan& pl, unsigned what, int& nmtile, int& nkstep);
 p2_status split_project(p2_ctx* c, const p2host::Plan& pl, int K, int n, int nmtile, int nkstep, const SliceDesc* dsl,
                         const int* exps, const int* kexp, const std::vector<ScatterBlock>& blocks,
-                        double* out = nullptr, long long oT = 0, long long oK = 0);
+                        double* out = nullptr, long long oT = 0, long long oK = 0, const int* kphase = nullptr);
 }  // namespace p2

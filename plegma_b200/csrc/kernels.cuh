@@ -8,6 +8,12 @@ namespace p2 {
 
 constexpr int kMaxBlocks = 10;  // contraction blocks of a request (one per P2_* bit)
 
+// Split form: the 16 x 16 meson outputs are staged through shared memory and
+// written without their unit phases r_g1 r_g2 (every Gamma row is r times a
+// Walsh character), which the projection's reduction applies per component,
+// whenever the 16 x 16 block is requested without the 10 diagonal structures.
+__host__ __device__ constexpr bool g16_phase_deferred(unsigned what) { return (what & 8u) && !(what & 64u); }
+
 // Where each contraction block's components sit inside the K components of a site.
 struct CompOffsets {
   int nuc, ntor, rton, rtor, diso12, diso32, g16, all34, new10, diag10;
@@ -123,6 +129,7 @@ struct SplitReduceArgs {
   const int* cmax;     // [ntau][K]
   const int* exps;     // [ntau][2]
   const int* kexp;     // [K][2]: powers of the u and d scales in component k
+  const int* kphase;   // [K]: component k is multiplied by i^kphase[k], or null
   const SliceDesc* sl; // result location of each slice
   int nblocks;
   ScatterBlock blk[kMaxBlocks];  // base = block offset per unit of (totalT * nmom)

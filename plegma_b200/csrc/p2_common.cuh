@@ -70,6 +70,33 @@ __device__ __forceinline__ Cx<R> cunit(Cx<R> a, int re, int im) {
   return cx<R>(R(re) * a.x - R(im) * a.y, R(re) * a.y + R(im) * a.x);
 }
 
+// Walsh factorisation of Gamma g (spin.gamma_walsh): G[d][d ^ m] = r (-1)^{popcount(s & d)}
+// with m = pi(0), r = G[0][m] and s read off rows 1 and 2; checked for every row.
+// Host side (device code indexes local copies of the tables).
+constexpr int gamma_class(int g) { return kGammaPerm[g][0]; }
+constexpr int gamma_char(int g) {
+  return (kGammaRe[g][1] == -kGammaRe[g][0] && kGammaIm[g][1] == -kGammaIm[g][0] ? 1 : 0) |
+         (kGammaRe[g][2] == -kGammaRe[g][0] && kGammaIm[g][2] == -kGammaIm[g][0] ? 2 : 0);
+}
+constexpr bool gamma_walsh_ok() {
+  for (int g = 0; g < 16; g++)
+    for (int d = 0; d < 4; d++) {
+      const int sd = gamma_char(g) & d, sg = ((sd ^ (sd >> 1)) & 1) ? -1 : 1;
+      if (kGammaPerm[g][d] != (d ^ gamma_class(g)) || kGammaRe[g][d] != sg * kGammaRe[g][0] ||
+          kGammaIm[g][d] != sg * kGammaIm[g][0])
+        return false;
+    }
+  return true;
+}
+static_assert(gamma_walsh_ok(), "a Gamma row is not a unit phase times a Walsh character");
+
+// Phase r_g1 r_g2 of C[g1][g2] as i^q, q in 0..3 (the projection's reduction
+// applies it when the contraction leaves it out).
+constexpr int gamma_phase_q(int g) {
+  return kGammaRe[g][0] == 1 ? 0 : kGammaIm[g][0] == 1 ? 1 : kGammaRe[g][0] == -1 ? 2 : 3;
+}
+constexpr int meson_phase_q(int g1, int g2) { return (gamma_phase_q(g1) + gamma_phase_q(g2)) & 3; }
+
 // Packed float pairs for the paired FP32 FMA (fma.rn.f32x2): one instruction
 // updates both halves of a register pair.
 typedef unsigned long long f32x2;

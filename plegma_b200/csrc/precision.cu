@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "ctx.h"
+#include "p2_common.cuh"
 
 using namespace p2host;
 
@@ -149,7 +150,16 @@ p2_status split_prepare_tables(p2_ctx* c, const Plan& pl, unsigned what, int& nm
     c->split_moms_key = pl.moms;
   }
   if (what && c->split_what_key != what) {
+    // [K][2] scale powers, then [K] unit phases i^q of the 16 x 16 mesons
+    // that the contraction leaves out (g16_phase_deferred)
     std::vector<int> ke = component_exponents(what);
+    const int K = (int)ke.size() / 2;
+    ke.resize(3 * (size_t)K, 0);
+    if (g16_phase_deferred(what)) {
+      const int k0 = offsets_of(what).g16;
+      for (int g1 = 0; g1 < 16; g1++)
+        for (int g2 = 0; g2 < 16; g2++) ke[2 * K + k0 + 16 * g1 + g2] = meson_phase_q(g1, g2);
+    }
     if ((st = upload_async(c, c->kexp, ke.data(), ke.size() * sizeof(int), "component exponents")) != P2_OK) return st;
     c->split_what_key = what;
   }
@@ -163,7 +173,7 @@ p2_status split_prepare_tables(p2_ctx* c, const Plan& pl, unsigned what, int& nm
 // With no blocks the results go to out[tau * oT + k * oK + p].
 p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int nkstep, const SliceDesc* dsl,
                         const int* exps, const int* kexp, const std::vector<ScatterBlock>& blocks, double* out,
-                        long long oT, long long oK) {
+                        long long oT, long long oK, const int* kphase) {
   // projection GEMM candidates (N-tile width NT <= 144 components = 288
   // TMEM columns, number of N-tiles, site splits, k-steps per split): the
   // fewest N-tiles at ~2 waves first, then up to two more N-tiles at 1, 2
@@ -234,6 +244,7 @@ p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int
   rd.cmax = (const int*)c->cmaxb.p;
   rd.exps = exps;
   rd.kexp = kexp;
+  rd.kphase = kphase;
   rd.sl = dsl;
   if (blocks.size() > (size_t)p2::kMaxBlocks) return c->fail(P2_ERR_INVALID_ARG, "too many result blocks");
   rd.nblocks = (int)blocks.size();
@@ -320,8 +331,9 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
     }
     if ((st = sg.release((int)ci)) != P2_OK) return st;
     if ((st = sg.issue((int)ci + 2)) != P2_OK) return st;
-    if ((st = split_project(c, pl, K, n, nmtile, nkstep, dsl, (const int*)c->expb.p, (const int*)c->kexp.p,
-                            pl.blocks)) != P2_OK)
+    const int* kexp = (const int*)c->kexp.p;
+    if ((st = split_project(c, pl, K, n, nmtile, nkstep, dsl, (const int*)c->expb.p, kexp, pl.blocks, nullptr, 0,
+                            0, g16_phase_deferred(what) ? kexp + 2 * K : nullptr)) != P2_OK)
       return st;
   }
   return P2_OK;

@@ -332,7 +332,12 @@ __global__ void k_split_reduce(const SplitReduceArgs a) {
     const double f = ldexp(1.0, pw);
     // S(p) = sum_x c e^{-i p.x}; the source phase: C(p) = e^{i p.x0} S(p), with
     // p.x0 / L reduced exactly in integers per dimension
-    const Cx<double> v = cmul(cx<double>((cr + sg * si) * f, (ci - sg * sr) * f), source_phase(mr + 3, sd.x0, a.L));
+    Cx<double> v = cmul(cx<double>((cr + sg * si) * f, (ci - sg * sr) * f), source_phase(mr + 3, sd.x0, a.L));
+    if (a.kphase) {
+      const int q = a.kphase[k];
+      if (q & 1) v = cx<double>(-v.y, v.x);
+      if (q & 2) v = cx<double>(-v.x, -v.y);
+    }
     if (a.nblocks == 0) ((Cx<double>*)a.out)[(long long)sd.tau * a.oT + (long long)k * a.oK + p] = v;
     for (int b = 0; b < a.nblocks; b++) {
       const ScatterBlock& B = a.blk[b];

@@ -30,6 +30,9 @@
 //   M_{a d}[b][z] = sum_{colour} A[a b] conj(B[d z])   (lane = (a, d), 144 products)
 //   N_{a d}[g2]   = sum_b G2[b][pi2(b)] M_{a d}[b][pi2(b)]
 //   C[g1][g2]     = sum_d G1[d][pi1(d)] N_{pi1(d) d}[g2]  (lane = g1, shuffles).
+// Every Gamma row is a unit phase times a Walsh character
+// (G[d][d ^ m] = r (-1)^{popcount(s & d)}), so both Gamma stages are 4-point
+// Walsh-Hadamard transforms and the phases r_g1 r_g2 factor out of the sums.
 #pragma once
 #include "p2_common.cuh"
 
@@ -44,8 +47,8 @@ struct DiquarkLane {
 // lane, so reading them from constant memory inside the site loop would
 // serialise the half-warp): a diquark lane descriptor as 8 fields of 4 bits
 // (value + 1), and the sink-Gamma stage of the mesons (spin.meson_lane_table):
-// the lane's sink Gamma g1 (4 bits), then Re + 1, Im + 1 of the phases D and
-// r (2 bits each).
+// the lane's sink Gamma g1 (4 bits), then Re + 1, Im + 1 of its phase r_g1
+// (2 bits each).
 struct LaneTables {
   unsigned nuc;       // nucleon C g5 descriptor
   unsigned delta[3];  // Delta C g_k descriptors, k = 1..3
@@ -58,7 +61,7 @@ struct LaneTables {
 __constant__ int c_nuc_lane[16][8] = P2_INIT_NucLane;
 __constant__ int c_delta_sink[3][4][3] = P2_INIT_DeltaSink;
 __constant__ int c_delta_lane[3][16][8] = P2_INIT_DeltaLane;
-__constant__ int c_meson_lane[16][5] = P2_INIT_MesonLane;
+__constant__ int c_meson_lane[16][3] = P2_INIT_MesonLane;
 __constant__ int c_light_lane[3][16][8] = P2_INIT_LightLane;
 __constant__ int c_light_g5[16][3] = P2_INIT_LightG5;
 
@@ -138,8 +141,7 @@ __device__ __forceinline__ LaneTables load_lane_tables(int l) {
   t.lg5 = (unsigned)(c_light_g5[l][0] + 1) | ((unsigned)(c_light_g5[l][1] + 1) << 2) |
           ((unsigned)(c_light_g5[l][2] + 1) << 4);
   t.mes = (unsigned)c_meson_lane[l][0] | ((unsigned)(c_meson_lane[l][1] + 1) << 4) |
-          ((unsigned)(c_meson_lane[l][2] + 1) << 6) | ((unsigned)(c_meson_lane[l][3] + 1) << 8) |
-          ((unsigned)(c_meson_lane[l][4] + 1) << 10);
+          ((unsigned)(c_meson_lane[l][2] + 1) << 6);
   return t;
 }
 
@@ -484,37 +486,57 @@ __device__ __forceinline__ void meson_M<RowF32>(const RowF32& row, int A, int B,
     for (int j = 0; j < 4; j++) f2unpack(M[i][j], Mo[i][j].x, Mo[i][j].y);
 }
 
+// v * r_g2 * r_g1, g2 a compile-time constant after unrolling, g1 the lane's sink Gamma.
+template <typename R>
+__device__ __forceinline__ Cx<R> meson_phase(const LaneTables& lt, int g2, Cx<R> v) {
+  constexpr int GR[16][4] = P2_INIT_GammaRe;
+  constexpr int GI[16][4] = P2_INIT_GammaIm;
+  const int rre = (int)((lt.mes >> 4) & 3u) - 1, rim = (int)((lt.mes >> 6) & 3u) - 1;
+  return cunit(cunit(v, GR[g2][0], GI[g2][0]), rre, rim);
+}
+
 // Generic meson block of the lines A and B (block offsets): the lane gets
 // C[g1][g2] for g2 = 0..15 in out[], g1 = lt.meson_g1() (a permutation of the
-// lanes).  Lane (al, de) first forms N_{al de}[g2] = sum_b G2[b][pi2(b)]
-// M[b][pi2(b)]; the sink Gamma C[g1][g2] = sum_d G1[d][pi1(d)] N_{pi1(d) d}[g2]
-// then runs as a Walsh-Hadamard transform over the 4 lanes of the lane's
-// class (spin.meson_lane_table): phase D, two butterflies (xor 5, xor 10),
-// phase r.
+// lanes), times conj(r_g1 r_g2) when phased is false.  Lane (al, de) first
+// forms, per source class m2, the Walsh-Hadamard transform over b of
+// M[b][b ^ m2] (N[g2] / r_g2 at index s_g2); the sink Gamma then runs as a
+// Walsh-Hadamard transform over the 4 lanes of the lane's class (two
+// butterflies, xor 5 and xor 10), which leaves C[g1][g2] / (r_g1 r_g2) on the
+// lane whose spin index de is s_g1 (spin.meson_lane_table).
 template <typename Row>
 __device__ __forceinline__ void meson_site(const Row& row, int A, int B, const LaneTables& lt, int l, unsigned mask,
-                                           Cx<typename Row::R> out[16]) {
+                                           bool phased, Cx<typename Row::R> out[16]) {
   typedef typename Row::R R;
   const int al = l >> 2, de = l & 3;
-  Cx<R> M[4][4];
-  meson_M(row, A, B, al, de, M);
+  Cx<R> W[4][4];
+  {
+    Cx<R> M[4][4];
+    meson_M(row, A, B, al, de, M);
+#pragma unroll
+    for (int m2 = 0; m2 < 4; m2++) {
+      const Cx<R> a0 = M[0][m2] + M[1][1 ^ m2], a1 = M[0][m2] - M[1][1 ^ m2];
+      const Cx<R> a2 = M[2][2 ^ m2] + M[3][3 ^ m2], a3 = M[2][2 ^ m2] - M[3][3 ^ m2];
+      W[m2][0] = a0 + a2;
+      W[m2][1] = a1 + a3;
+      W[m2][2] = a0 - a2;
+      W[m2][3] = a1 - a3;
+    }
+  }
+  // local copies: the namespace-scope tables are not addressable in device code
   constexpr int GP[16][4] = P2_INIT_GammaPerm;
   constexpr int GR[16][4] = P2_INIT_GammaRe;
   constexpr int GI[16][4] = P2_INIT_GammaIm;
-  const int dre = (int)((lt.mes >> 4) & 3u) - 1, dim = (int)((lt.mes >> 6) & 3u) - 1;
-  const int rre = (int)((lt.mes >> 8) & 3u) - 1, rim = (int)((lt.mes >> 10) & 3u) - 1;
   const R s0 = (de & 1) ? R(-1) : R(1), s1 = (de & 2) ? R(-1) : R(1);
 #pragma unroll
   for (int g2 = 0; g2 < 16; g2++) {
-    Cx<R> n = czero<R>();
-#pragma unroll
-    for (int b = 0; b < 4; b++) n = n + cunit(M[b][GP[g2][b]], GR[g2][b], GI[g2][b]);
-    Cx<R> x = cunit(n, dre, dim);
+    const int ch = (GR[g2][1] == -GR[g2][0] && GI[g2][1] == -GI[g2][0] ? 1 : 0) |
+                   (GR[g2][2] == -GR[g2][0] && GI[g2][2] == -GI[g2][0] ? 2 : 0);  // gamma_char(g2)
+    Cx<R> x = W[GP[g2][0]][ch];
     Cx<R> p = shfl_xor16(x, 5, mask);
     x = cx<R>(fma(s0, x.x, p.x), fma(s0, x.y, p.y));
     p = shfl_xor16(x, 10, mask);
     x = cx<R>(fma(s1, x.x, p.x), fma(s1, x.y, p.y));
-    out[g2] = cunit(x, rre, rim);
+    out[g2] = phased ? meson_phase(lt, g2, x) : x;
   }
 }
 

@@ -314,41 +314,37 @@ def _c_array(name, ctype, data, fmt="{}"):
             f"static constexpr {ctype} {name}{dims} = {macro};\n")
 
 
+def gamma_walsh(g: int):
+    """Every Gamma is a signed permutation pi_g(d) = d xor m_g whose
+    coefficients are a unit phase times a Walsh character:
+        Gamma_g[d][d xor m_g] = r_g * (-1)^{popcount(s_g & d)}.
+    Returns (m_g, s_g, r_g)."""
+    perm, vals = signed_permutation(GAMMA16[g])
+    m = perm[0]
+    assert all(perm[d] == d ^ m for d in range(4))
+    r = vals[0]
+    s = (1 if abs(vals[1] + r) < 1e-12 else 0) | (2 if abs(vals[2] + r) < 1e-12 else 0)
+    for d in range(4):
+        assert abs(vals[d] - r * (-1) ** bin(s & d).count("1")) < 1e-12, (g, d)
+    return m, s, r
+
+
 def meson_lane_table():
     """Sink-Gamma stage of the lane-parallel mesons as a Walsh-Hadamard transform.
 
-    Every Gamma is a signed permutation with pi_g(d) = d xor m_g (m_g in 0..3),
-    and within a class m the coefficients factorise as
-        G_g[d][d xor m] = r_g * (-1)^{popcount(s_g & d)} * D_m(d)
-    with unit phases r_g, D_m(d) and distinct s_g in 0..3.  Lane l = (a, d) =
-    (l >> 2, l & 3) belongs to class m = a xor d; after multiplying its value
-    by D_m(d), a 4-point transform over the lanes of its class (xor masks 5
-    and 10) leaves on it sum_d' (-1)^{popcount(d & d')} D_m(d') N(d'), which is
-    C[g] / r_g for the Gamma g of class m with s_g = d.
-    Returns per lane (g, Re D, Im D, Re r, Im r)."""
-    classes = {}
-    for g, M in enumerate(GAMMA16):
-        perm, vals = signed_permutation(M)
-        m = perm[0]
-        assert all(perm[d] == d ^ m for d in range(4))
-        classes.setdefault(m, []).append((g, np.array(vals)))
+    Lane l = (a, d) = (l >> 2, l & 3) belongs to class m = a xor d; a 4-point
+    transform over the lanes of its class (xor masks 5 and 10) leaves on it
+    sum_d' (-1)^{popcount(d & d')} N(d'), which by the factorisation of
+    gamma_walsh is C[g] / r_g for the Gamma g of class m with s_g = d.
+    Returns per lane (g, Re r_g, Im r_g)."""
     lanes = []
     for l in range(16):
         a, d = l >> 2, l & 3
-        m = a ^ d
-        lst = classes[m]
-        D = lst[0][1]
-        chosen = None
-        for g, v in lst:
-            w = v / D
-            for s in range(4):
-                chi = np.array([(-1) ** bin(s & x).count("1") for x in range(4)])
-                r = w[0]
-                if np.allclose(w, r * chi) and s == d:
-                    chosen = (g, r)
-        assert chosen is not None, (l, m)
-        g, r = chosen
-        lanes.append([g, int(round(D[d].real)), int(round(D[d].imag)), int(round(r.real)), int(round(r.imag))])
+        found = [g for g in range(16) if gamma_walsh(g)[:2] == (a ^ d, d)]
+        assert len(found) == 1, (l, found)
+        g = found[0]
+        r = gamma_walsh(g)[2]
+        lanes.append([g, int(round(r.real)), int(round(r.imag))])
     assert sorted(x[0] for x in lanes) == list(range(16))
     return lanes
 

@@ -84,3 +84,43 @@ def test_second_nucleon_interpolator_tables_match_reference(digests, key, name):
     rows = spin.light_nucleon_tables()[name]
     assert spin.table_digest([r[:-1] for r in rows]) == digests[key + "_indices"]
     assert spin.table_digest([r[-1] for r in rows]) == digests[key + "_values"]
+
+
+def test_meson_walsh_stage_matches_direct_sum():
+    """The lane-parallel Gamma stages of the mesons (site_contract.cuh
+    meson_site): per lane (a, d) the Walsh-Hadamard transform over b of
+    M[b][b ^ m2], two butterflies over the lanes l ^ 5 and l ^ 10 with the
+    signs of d's bits, then lane l holds C[g1][g2] / (r_g1 r_g2) for g1 of
+    spin.meson_lane_table; the phase i^q of the deferred form restores it.
+    Checked against C[g1][g2] = sum_d G1[d][pi1(d)] sum_b G2[b][pi2(b)]
+    M_{pi1(d) d}[b][pi2(b)] on random M."""
+    rng = np.random.default_rng(5)
+    M = rng.standard_normal((4, 4, 4, 4)) + 1j * rng.standard_normal((4, 4, 4, 4))  # [a][d][b][z]
+    G = [np.array(g) for g in spin.GAMMA16]
+    direct = np.zeros((16, 16), dtype=complex)
+    for g1 in range(16):
+        for g2 in range(16):
+            p1, v1 = spin.signed_permutation(G[g1])
+            p2, v2 = spin.signed_permutation(G[g2])
+            direct[g1, g2] = sum(v1[d] * v2[b] * M[p1[d], d, b, p2[b]] for d in range(4) for b in range(4))
+    walsh = [spin.gamma_walsh(g) for g in range(16)]
+    chi = lambda s, b: (-1) ** bin(s & b).count("1")
+    lanes = spin.meson_lane_table()
+    emu = np.zeros((16, 16), dtype=complex)
+    for g2 in range(16):
+        m2, s2, _ = walsh[g2]
+        x = np.array([sum(chi(s2, b) * M[l >> 2, l & 3, b, b ^ m2] for b in range(4)) for l in range(16)])
+        s0 = np.array([-1 if (l & 1) else 1 for l in range(16)])
+        s1 = np.array([-1 if (l & 2) else 1 for l in range(16)])
+        x = s0 * x + x[[l ^ 5 for l in range(16)]]
+        x = s1 * x + x[[l ^ 10 for l in range(16)]]
+        for l in range(16):
+            g1 = lanes[l][0]
+            assert complex(lanes[l][1], lanes[l][2]) == walsh[g1][2]
+            emu[g1, g2] = x[l] * (1j) ** ((spin_phase_q(walsh, g1) + spin_phase_q(walsh, g2)) % 4)
+    assert np.allclose(emu, direct, atol=1e-12)
+
+
+def spin_phase_q(walsh, g):
+    """q with r_g = i^q (the deferred phase code of the projection's reduction)."""
+    return {1: 0, 1j: 1, -1: 2, -1j: 3}[complex(np.round(walsh[g][2], 12))]
