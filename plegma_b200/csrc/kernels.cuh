@@ -13,6 +13,13 @@ constexpr int kMaxBlocks = 10;  // contraction blocks of a request (one per P2_*
 // Walsh character), which the projection's reduction applies per component,
 // whenever the 16 x 16 block is requested without the 10 diagonal structures.
 __host__ __device__ constexpr bool g16_phase_deferred(unsigned what) { return (what & 8u) && !(what & 64u); }
+// ... and, when neither the 34 pairs nor the 10 diagonal structures of the
+// same lanes are requested, the sink Gamma stage as well: the lanes stage
+// their values before the butterflies and the tile flush forms the 4-point
+// transforms (signs sigma of the flush table folded into the phases).
+__host__ __device__ constexpr bool g16_flush_wht(unsigned what) {
+  return g16_phase_deferred(what) && !(what & (16u | 32u));
+}
 
 // Where each contraction block's components sit inside the K components of a site.
 struct CompOffsets {

@@ -158,7 +158,9 @@ p2_status split_prepare_tables(p2_ctx* c, const Plan& pl, unsigned what, int& nm
     if (g16_phase_deferred(what)) {
       const int k0 = offsets_of(what).g16;
       for (int g1 = 0; g1 < 16; g1++)
-        for (int g2 = 0; g2 < 16; g2++) ke[2 * K + k0 + 16 * g1 + g2] = meson_phase_q(g1, g2);
+        for (int g2 = 0; g2 < 16; g2++)
+          ke[2 * K + k0 + 16 * g1 + g2] =
+              (meson_phase_q(g1, g2) + (g16_flush_wht(what) && meson_flush_sign(g1) < 0 ? 2 : 0)) & 3;
     }
     if ((st = upload_async(c, c->kexp, ke.data(), ke.size() * sizeof(int), "component exponents")) != P2_OK) return st;
     c->split_what_key = what;

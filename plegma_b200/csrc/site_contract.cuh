@@ -62,6 +62,7 @@ __constant__ int c_nuc_lane[16][8] = P2_INIT_NucLane;
 __constant__ int c_delta_sink[3][4][3] = P2_INIT_DeltaSink;
 __constant__ int c_delta_lane[3][16][8] = P2_INIT_DeltaLane;
 __constant__ int c_meson_lane[16][3] = P2_INIT_MesonLane;
+__constant__ int c_meson_flush[4][4][2] = P2_INIT_MesonFlush;
 __constant__ int c_light_lane[3][16][8] = P2_INIT_LightLane;
 __constant__ int c_light_g5[16][3] = P2_INIT_LightG5;
 
@@ -497,7 +498,9 @@ __device__ __forceinline__ Cx<R> meson_phase(const LaneTables& lt, int g2, Cx<R>
 
 // Generic meson block of the lines A and B (block offsets): the lane gets
 // C[g1][g2] for g2 = 0..15 in out[], g1 = lt.meson_g1() (a permutation of the
-// lanes), times conj(r_g1 r_g2) when phased is false.  Lane (al, de) first
+// lanes), times conj(r_g1 r_g2) when phased is false; with sink false the
+// lane keeps its values before the sink stage (the tile flush forms it,
+// spin.meson_flush_table).  Lane (al, de) first
 // forms, per source class m2, the Walsh-Hadamard transform over b of
 // M[b][b ^ m2] (N[g2] / r_g2 at index s_g2); the sink Gamma then runs as a
 // Walsh-Hadamard transform over the 4 lanes of the lane's class (two
@@ -505,7 +508,7 @@ __device__ __forceinline__ Cx<R> meson_phase(const LaneTables& lt, int g2, Cx<R>
 // lane whose spin index de is s_g1 (spin.meson_lane_table).
 template <typename Row>
 __device__ __forceinline__ void meson_site(const Row& row, int A, int B, const LaneTables& lt, int l, unsigned mask,
-                                           bool phased, Cx<typename Row::R> out[16]) {
+                                           bool sink, bool phased, Cx<typename Row::R> out[16]) {
   typedef typename Row::R R;
   const int al = l >> 2, de = l & 3;
   Cx<R> W[4][4];
@@ -526,12 +529,20 @@ __device__ __forceinline__ void meson_site(const Row& row, int A, int B, const L
   constexpr int GP[16][4] = P2_INIT_GammaPerm;
   constexpr int GR[16][4] = P2_INIT_GammaRe;
   constexpr int GI[16][4] = P2_INIT_GammaIm;
+  auto source_value = [&](int g2) {
+    const int ch = (GR[g2][1] == -GR[g2][0] && GI[g2][1] == -GI[g2][0] ? 1 : 0) |
+                   (GR[g2][2] == -GR[g2][0] && GI[g2][2] == -GI[g2][0] ? 2 : 0);  // gamma_char(g2)
+    return W[GP[g2][0]][ch];
+  };
+  if (!sink) {
+#pragma unroll
+    for (int g2 = 0; g2 < 16; g2++) out[g2] = source_value(g2);
+    return;
+  }
   const R s0 = (de & 1) ? R(-1) : R(1), s1 = (de & 2) ? R(-1) : R(1);
 #pragma unroll
   for (int g2 = 0; g2 < 16; g2++) {
-    const int ch = (GR[g2][1] == -GR[g2][0] && GI[g2][1] == -GI[g2][0] ? 1 : 0) |
-                   (GR[g2][2] == -GR[g2][0] && GI[g2][2] == -GI[g2][0] ? 2 : 0);  // gamma_char(g2)
-    Cx<R> x = W[GP[g2][0]][ch];
+    Cx<R> x = source_value(g2);
     Cx<R> p = shfl_xor16(x, 5, mask);
     x = cx<R>(fma(s0, x.x, p.x), fma(s0, x.y, p.y));
     p = shfl_xor16(x, 10, mask);
