@@ -215,18 +215,33 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
     }
     const Cx<float>* cb = (const Cx<float>*)a.c + (long long)tau * a.K * a.V3;
     const bool even = (a.V3 & 1) == 0;  // site pairs 16-byte aligned
+    // swizzled byte offsets of this thread's (component, site pair) in a B
+    // tile, fixed over the k-steps: the Re row 2 kk at
+    //   256 kk + 16 ((sp >> 2) ^ 2 (kk & 3)) + 4 (sp & 3)   (tc::sw128_offset(2 kk, 2 sp)),
+    // the Im row 2 kk + 1 a fixed 128 +- 16 bytes further
+    uint32_t boff[JN];
+#pragma unroll
+    for (int j = 0; j < JN; j++) boff[j] = tc::sw128_offset(2 * (kg + kConvWarps * j), 2 * sp);
+    const uint32_t dim = tc::sw128_offset(1, 2 * sp) - tc::sw128_offset(0, 2 * sp);
     // B values of two consecutive k-steps (register double buffer, the two
     // halves swapping roles every k-step: the loads of step i + 1 stay in
     // flight while step i is split)
     float4 b0[JN], b1[JN];
+    // components this thread converts (bit j: component k0 + kg + 15 j exists)
+    unsigned jok = 0;
+#pragma unroll
+    for (int j = 0; j < JN; j++)
+      if (kg + kConvWarps * j < NT && k0 + kg + kConvWarps * j < a.K) jok |= 1u << j;
+    const Cx<float>* cthr = cb + (long long)(k0 + kg) * a.V3 + 2 * sp;
+    const long long cstride = (long long)kConvWarps * a.V3;
     auto load_b = [&](int ks, float4 (&r)[JN]) {
       const long long x = (long long)ks * kKS + 2 * sp;
+      const Cx<float>* cks = cthr + (long long)ks * kKS;
 #pragma unroll
       for (int j = 0; j < JN; j++) {
-        const int k = k0 + kg + kConvWarps * j;
         r[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (kg + kConvWarps * j < NT && k < a.K && x < a.V3) {
-          const Cx<float>* src = cb + (long long)k * a.V3 + x;
+        if (((jok >> j) & 1u) && x < a.V3) {
+          const Cx<float>* src = cks + j * cstride;
           if (even) {
             r[j] = *reinterpret_cast<const float4*>(src);
           } else {
@@ -258,8 +273,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
         const float2 fr = __half22float2(hr), fi = __half22float2(hi_);
         const __half2 lr = __floats2half2_rn(r0 - fr.x, r1 - fr.y);
         const __half2 li = __floats2half2_rn(i0 - fi.x, i1 - fi.y);
-        const uint32_t ore = tc::sw128_offset(2 * kk, 2 * sp);
-        const uint32_t oim = tc::sw128_offset(2 * kk + 1, 2 * sp);
+        const uint32_t ore = boff[j];
+        const uint32_t oim = ore + dim;
         *(__half2*)(Bh + ore) = hr;
         *(__half2*)(Bh + oim) = hi_;
         *(__half2*)(Bl + ore) = lr;
