@@ -348,22 +348,22 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
         const int q = c0 + 16 * j;
         if (q < 72) {
           const int f = q >= 36;
-          int comp[4];
-          prop_group_comps(q - 36 * f, comp);
+          int b, cc;
+          prop_group_base(q - 36 * f, b, cc);
+          // the group's four components at fixed offsets from one staging and one row index
+          const Cx<Tin>* src = st + (144 * f + 9 * b + cc) * kSitesPerTile + s;
+          Cx<float>* dst = row + 2 * row32_unit(16 * f + b, cc >> 1) + (cc & 1);
           Cx<double> v[4];
 #pragma unroll
           for (int i = 0; i < 4; i++) {
-            const Cx<Tin> x = st[(144 * f + comp[i]) * kSitesPerTile + s];
+            const Cx<Tin> x = src[9 * group_blk(i) * kSitesPerTile];
             v[i] = cx<double>((double)x.x, (double)x.y);
           }
           prop_group_transform(v[0], v[1], v[2], v[3], f ? xfd : xfu);
           const double sc = f ? sd : su;
 #pragma unroll
-          for (int i = 0; i < 4; i++) {
-            const int blk = comp[i] / 9, col = comp[i] - 9 * blk;
-            row[2 * row32_unit(16 * f + blk, col >> 1) + (col & 1)] =
-                cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
-          }
+          for (int i = 0; i < 4; i++)
+            dst[2 * row32_unit(group_blk(i), 0)] = cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
         }
       }
     }

@@ -166,6 +166,14 @@ __device__ __forceinline__ void prop_group_comps(int q, int comp[4]) {
   comp[3] = (b + 10) * 9 + cc;
 }
 
+// The same group as (first block b, colour cc): the four components are
+// colour cc of blocks b + group_blk(i).
+__host__ __device__ constexpr int group_blk(int i) { return i == 0 ? 0 : i == 1 ? 2 : i == 2 ? 8 : 10; }
+__device__ __forceinline__ void prop_group_base(int q, int& b, int& cc) {
+  cc = q >> 2;
+  b = ((q & 3) >> 1) * 4 + (q & 1);
+}
+
 // Index of spin block (mu, nu) in a site's 144 components; colour (a, b) adds a*3 + b.
 __host__ __device__ constexpr int sblk(int mu, int nu) { return (mu * 4 + nu) * 9; }
 

@@ -335,21 +335,20 @@ __global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc_f32(const UdscAr
         if (q < 108) {
           const int f = q / 36;
           const double sc = ldexp(1.0, -a.e3[3 * tl + f]);
-          int comp[4];
-          prop_group_comps(q - 36 * f, comp);
+          int b, cc;
+          prop_group_base(q - 36 * f, b, cc);
+          const Cx<Tin>* src = st + (144 * f + 9 * b + cc) * kSitesU + s;
+          Cx<float>* dst = row + 2 * row32_unit(16 * f + b, cc >> 1) + (cc & 1);
           Cx<double> v[4];
 #pragma unroll
           for (int i = 0; i < 4; i++) {
-            const Cx<Tin> x = st[(144 * f + comp[i]) * kSitesU + s];
+            const Cx<Tin> x = src[9 * group_blk(i) * kSitesU];
             v[i] = cx<double>((double)x.x, (double)x.y);
           }
           prop_group_transform(v[0], v[1], v[2], v[3], sd.xf[f]);
 #pragma unroll
-          for (int i = 0; i < 4; i++) {
-            const int blk = comp[i] / 9, col = comp[i] - 9 * blk;
-            row[2 * row32_unit(16 * f + blk, col >> 1) + (col & 1)] =
-                cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
-          }
+          for (int i = 0; i < 4; i++)
+            dst[2 * row32_unit(group_blk(i), 0)] = cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
         }
       }
     }

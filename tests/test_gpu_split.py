@@ -214,3 +214,25 @@ def test_two_site_spatial_volume(mode):
     asum = np.abs(f).reshape(144, 4, -1).sum(axis=2).T
     assert (np.abs(ftd.reshape(ref.shape) - ref).max(axis=2) / asum).max() < (1e-12 if mode == p2.P2_PLAIN_FP64 else 1e-6)
     ctx.close()
+
+
+@pytest.mark.parametrize("what", [
+    p2.MESON_G16,                                       # sink Gamma stage in the tile flush
+    p2.MESON_G16 | p2.MESON_ALL34 | p2.MESON_NEW10,     # staged, sink stage in the lanes, phases in the reduction
+    p2.MESON_G16 | p2.MESON_DIAG10,                     # direct stores with phases
+    p2.MESON_ALL34 | p2.MESON_NEW10,                    # no 16 x 16 block
+])
+def test_split_meson_paths(what):
+    """The split kernel's four ways of finishing the 16 x 16 meson Gamma
+    stages (which lanes or threads form the sink transform, where the unit
+    phases r_g1 r_g2 are applied) against the oracle."""
+    ctx = p2.Context((5, 4, 3, 6))
+    src = (4, 1, 2, 3)
+    bufs = device_props(ctx, [(71, 0), (71, 1)], t0=src[3])
+    moms = p2.mom_list(2)
+    out, _ = run(ctx, bufs, src, 6, what, moms=moms, mode=SPLIT)
+    taus = list(range(6))
+    ref = oracle_blocks(ctx.L, bufs, src, moms, what, taus)
+    err = per_t_error(out, what, 6, moms, ref, taus)
+    assert err.max() < TOL, err
+    ctx.close()
