@@ -581,9 +581,10 @@ __device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt,
   const R third = R(1) / R(3);
   // iso-1/2 partial sums from G^{ud} / G^{du}, completed by the G^{uu} / G^{dd} terms
   // G^{ud} (A = u) and its lane transpose G^{du} (A = d; C g_k is symmetric)
-  // FP64: C g_1 and C g_2 from the shared diagonal products ga = P00 - P22,
-  // gb = P11 - P33 (8 products instead of 12); in FP32 holding ga and gb
-  // across the loop spills, which costs more than the 4 products it saves
+  // C g_1 and C g_2 from the shared diagonal products ga = P00 - P22,
+  // gb = P11 - P33 (8 products instead of 12).  FP64: ga and gb formed up
+  // front; FP32 (registers are tighter): C g_3 first, then ga and gb, with
+  // only C g_2's sum ga + gb held over C g_1's evaluation
   constexpr bool kShare = sizeof(R) == 8;
   Cx<R> ga[9], gb[9];
   if (kShare) {
@@ -594,12 +595,30 @@ __device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt,
     diquark_acc(row, kU, kD, 1, 1, R(1), xp, yp, gb);
     diquark_acc(row, kU, kD, 3, 3, R(-1), xp, yp, gb);
   }
+  Cx<R> q1[9];  // FP32: C g_2's G^{ud}, formed with C g_1's
 #pragma unroll 1
-  for (int g = 0; g < 3; g++) {
+  for (int it = 0; it < 3; it++) {
+    const int g = kShare ? it : (it == 0 ? 2 : it - 1);
     Cx<R> q[9], D[9];
     if (kShare && g < 2) {
 #pragma unroll
       for (int i = 0; i < 9; i++) q[i] = g == 0 ? ga[i] - gb[i] : ga[i] + gb[i];
+    } else if (!kShare && it == 1) {
+#pragma unroll
+      for (int i = 0; i < 9; i++) q[i] = q1[i] = czero<R>();
+      diquark_acc(row, kU, kD, 0, 0, R(1), xp, yp, q);
+      diquark_acc(row, kU, kD, 2, 2, R(-1), xp, yp, q);
+      diquark_acc(row, kU, kD, 1, 1, R(1), xp, yp, q1);
+      diquark_acc(row, kU, kD, 3, 3, R(-1), xp, yp, q1);
+#pragma unroll
+      for (int i = 0; i < 9; i++) {
+        const Cx<R> t = q[i];
+        q[i] = t - q1[i];
+        q1[i] = t + q1[i];
+      }
+    } else if (!kShare && it == 2) {
+#pragma unroll
+      for (int i = 0; i < 9; i++) q[i] = q1[i];
     } else {
       diquark_G(row, kU, kD, c_delta_sink[g], xp, yp, q);
     }
