@@ -51,6 +51,7 @@ struct DiquarkLane {
 // (2 bits each).
 struct LaneTables {
   unsigned nuc;       // nucleon C g5 descriptor
+  unsigned nucT;      // the same for the transposed lane ((l & 3) << 2) | (l >> 2)
   unsigned delta[3];  // Delta C g_k descriptors, k = 1..3
   unsigned light[3];  // NtoR, RtoN, RtoR descriptors (spin.light_lane_tables)
   unsigned lg5;       // their g5 signs, 2 bits each (value + 1)
@@ -135,6 +136,7 @@ __device__ __forceinline__ DiquarkLane unpack_diquark_lane(unsigned v) {
 __device__ __forceinline__ LaneTables load_lane_tables(int l) {
   LaneTables t;
   t.nuc = pack_diquark_lane(c_nuc_lane, l);
+  t.nucT = pack_diquark_lane(c_nuc_lane, ((l & 3) << 2) | (l >> 2));
 #pragma unroll
   for (int g = 0; g < 3; g++) t.delta[g] = pack_diquark_lane(c_delta_lane[g], l);
 #pragma unroll
@@ -355,6 +357,58 @@ __device__ __forceinline__ Cx<typename Row::R> diquark_slots(const Cx<typename R
   return r;
 }
 
+// Slot-1 terms of the Wick-transposed diquark G^{YX}(x', y') = sign G^{XY}(y', x')
+// without moving G: lane (a, b) holds G^{XY}(a, b) and forms the terms of
+// the transposed lane (x', y') = (b, a) with that lane's descriptor dlT,
+//   P[m] = f1(dlT) sign sum_ce G^{XY}(a, b)[c][e] Z[m][z1(dlT)][c][e];
+// their sum over y' = a (lane bits 3, 2) leaves T[a][b] on lane (a, b),
+// which is T[mu][mu'] of the lane itself.
+template <typename Row>
+__device__ __forceinline__ Cx<typename Row::R> diquark_slot1_transposed(const Cx<typename Row::R> g[9], const Row& row,
+                                                                        int Z, const DiquarkLane& dlT, int l,
+                                                                        unsigned mask, int c1A, int c1B,
+                                                                        typename Row::R sign) {
+  typedef typename Row::R R;
+  const R f1 = sign * R(-(c1A * dlT.sA1 - c1B * dlT.sB1));
+  if constexpr (sizeof(R) == 8) {
+    const int mu = l >> 2;
+    Cx<R> r = czero<R>();
+#pragma unroll 1
+    for (int m = 0; m < 4; m++) {
+      Cx<R> z[9];
+      row.load9(Z + m * 4 + dlT.z1, z);
+      Cx<R> p = czero<R>();
+#pragma unroll
+      for (int i = 0; i < 9; i++) cmac(p, g[i], z[i]);
+      p = cscale(p, f1);
+      p = p + shfl_xor16(p, 4, mask);
+      p = p + shfl_xor16(p, 8, mask);
+      if (m == mu) r = r + p;
+    }
+    return r;
+  } else {
+    Cx<R> P[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      Cx<R> z[9];
+      row.load9(Z + m * 4 + dlT.z1, z);
+      Cx<R> p = czero<R>();
+#pragma unroll
+      for (int i = 0; i < 9; i++) cmac(p, g[i], z[i]);
+      P[m] = cscale(p, f1);
+    }
+    // reduce-scatter over lane bits 3, 2: lane (a, b) keeps m = a
+    const bool b1 = (l >> 3) & 1, b0 = (l >> 2) & 1;
+    const Cx<R> s0 = b1 ? P[0] : P[2], s1 = b1 ? P[1] : P[3];
+    Cx<R> k0 = b1 ? P[2] : P[0], k1 = b1 ? P[3] : P[1];
+    k0 = k0 + shfl_xor16(s0, 8, mask);
+    k1 = k1 + shfl_xor16(s1, 8, mask);
+    const Cx<R> sv = b0 ? k0 : k1;
+    const Cx<R> kv = b0 ? k1 : k0;
+    return kv + shfl_xor16(sv, 4, mask);
+  }
+}
+
 // Type-a terms: D = sum over the 16 lanes of fa G (all lanes get D; fa is
 // zero outside the lane class of l0), then the lane's
 // T[mu][mu'] = sum_ce D[c][e] Z[mu][mu'][c][e].
@@ -401,8 +455,9 @@ __device__ __forceinline__ void nucleon_site(const Row& row, const LaneTables& l
   constexpr int l0 = typea_lane(kNucLane);
   diquark_D(g, R(dl.sN), mask, l0, D);  // cN = 1, cL = 0
   out[0] = diquark_eval<true, false>(g, row, kU, dl, l, mask, -1, 0, 0, 0, D);
-  diquark_transpose<R>(g, l, mask, R(-1));  // G^{du}; its type-a sum is (-1)(tau = -1) D
-  out[1] = diquark_eval<true, false>(g, row, kD, dl, l, mask, -1, 0, 0, 0, D);
+  // G^{du}(x', y') = -G^{ud}(y', x'); its type-a sum is (-1)(tau = -1) D
+  out[1] = diquark_slot1_transposed(g, row, kD, unpack_diquark_lane(lt.nucT), l, mask, -1, 0, R(-1)) +
+           diquark_typea(D, row, kD, l);
 }
 
 // M_{al de}[b][z] = sum over colour of A[al][b] conj(B[de][z]).
