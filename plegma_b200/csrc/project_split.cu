@@ -50,14 +50,15 @@ constexpr int kATile = 128 * kKS * 2;     // bytes of one 128 x 64 FP16 tile
 __host__ __device__ constexpr int b_tile_bytes(int NT) { return 2 * NT * kKS * 2; }
 // Stage counts: B (converted operand) stages let the converters run ahead of
 // the MMAs, phase (A) stages let each k-step's phase copy be issued ahead.
-// Two B stages and, where they fit, three A stages: measured at 48^3 x 16,
+// Three A stages where they fit, and three B stages only beside them (N-tiles
+// of up to 80 components): measured at 48^3 x 16 with 96-component tiles,
 // three A stages beat three B stages (1.01 vs 1.08 ms at 123 momenta).
 constexpr int kSmemMax = 232448;
 constexpr int kBarBytes = 128;  // mbarriers, TMEM address, error flag
 __host__ __device__ constexpr int stage_bytes(int NT, int nb, int na) {
   return nb * 2 * b_tile_bytes(NT) + na * 2 * kATile + kBarBytes + 1024;
 }
-__host__ __device__ constexpr int b_stages(int) { return 2; }
+__host__ __device__ constexpr int b_stages(int NT) { return stage_bytes(NT, 3, 3) <= kSmemMax ? 3 : 2; }
 __host__ __device__ constexpr int a_stages(int NT) { return stage_bytes(NT, b_stages(NT), 3) <= kSmemMax ? 3 : 2; }
 __host__ __device__ constexpr int smem_bytes(int NT) { return stage_bytes(NT, b_stages(NT), a_stages(NT)); }
 __host__ __device__ constexpr int tmem_cols(int NT) {
