@@ -445,28 +445,41 @@ __global__ void k_sample_exponents(const SampleArgs a) {
   const long long vol = f ? sd.vol_d : sd.vol_u;
   const long long j = f ? sd.off_d : sd.off_u;
   int emax = -100000;
-  for (int i = threadIdx.x; i < 21 * 1024; i += blockDim.x) {
-    const int comp = (i % 21) * 7;
-    const long long x = ((long long)(i / 21) * 97) % a.V3;
-    const long long idx = (long long)comp * vol + j + x;
-    double re, im;
-    if (a.fp32) {
-      const float2 v = ((const float2*)p)[idx];
-      re = v.x;
-      im = v.y;
-    } else {
-      const double2 v = ((const double2*)p)[idx];
-      re = v.x;
-      im = v.y;
+  // 8 independent loads in flight per thread (the samples are scattered, so
+  // each is a separate DRAM access)
+  constexpr int kSamples = 21 * 1024, kBatch = 8;
+  for (int i0 = threadIdx.x; i0 < kSamples; i0 += kBatch * blockDim.x) {
+    double re[kBatch], im[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; u++) {
+      const int i = i0 + u * blockDim.x;
+      re[u] = im[u] = 0.0;
+      if (i < kSamples) {
+        const int comp = (i % 21) * 7;
+        const long long x = ((long long)(i / 21) * 97) % a.V3;
+        const long long idx = (long long)comp * vol + j + x;
+        if (a.fp32) {
+          const float2 v = ((const float2*)p)[idx];
+          re[u] = v.x;
+          im[u] = v.y;
+        } else {
+          const double2 v = ((const double2*)p)[idx];
+          re[u] = v.x;
+          im[u] = v.y;
+        }
+      }
     }
-    int e;
-    if (re != 0.0) {
-      frexp(re, &e);
-      emax = max(emax, e);
-    }
-    if (im != 0.0) {
-      frexp(im, &e);
-      emax = max(emax, e);
+#pragma unroll
+    for (int u = 0; u < kBatch; u++) {
+      int e;
+      if (re[u] != 0.0) {
+        frexp(re[u], &e);
+        emax = max(emax, e);
+      }
+      if (im[u] != 0.0) {
+        frexp(im[u], &e);
+        emax = max(emax, e);
+      }
     }
   }
   red[threadIdx.x] = emax;

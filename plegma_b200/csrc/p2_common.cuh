@@ -232,7 +232,7 @@ __device__ __forceinline__ Cx<double> source_phase(const int* p, const int* x0, 
   double frac = 0.0;
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    int m = (int)(((long long)p[d] * x0[d]) % L[d]);
+    int m = ((p[d] % L[d]) * x0[d]) % L[d];  // |p mod L| and x0 below L: no overflow
     if (m < 0) m += L[d];
     frac += (double)m / (double)L[d];
   }
