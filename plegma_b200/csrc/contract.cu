@@ -22,7 +22,11 @@
 //    along the site axis of the SoA propagator, into shared memory as
 //    [site][flavour*144 + component] (row padded to 289 complex);
 //  - two stages: tile i+1's copies are in flight while tile i is contracted;
-//  - half-warp h contracts site h of the tile (site_contract.cuh).
+//  - half-warp h contracts site h of the tile (site_contract.cuh);
+//  - split form: the tile is converted once into padded FP32 rows (component-
+//    major staging, one buffer), and the 16 x 16 meson outputs go back through
+//    the sites' rows to a tile-wide flush that writes 128-byte component rows
+//    (and, when nothing else needs the lanes' sink stage, forms it).
 #include "kernels.cuh"
 #include "launch_util.h"
 #include "site_contract.cuh"
@@ -87,7 +91,9 @@ __device__ __forceinline__ int* smax_slot(Cx<float>* sf, int k) {
 
 // Split form, 16 x 16 mesons: a half-warp reads only its own site's FP32 row,
 // so once its contraction is done it stages the site's 256 outputs in that
-// row, output j = 16 g2 + g1 at complex 10 (j >> 3) + (j & 7): the four data
+// row (C[g1][g2] of lane g1, or with the flush's sink stage the value of lane
+// l before it, in the slot of g1 = l), output j = 16 g2 + g1 at complex
+// 10 (j >> 3) + (j & 7): the four data
 // units of every block (the colour-8 and spare slots keep their contents, the
 // spare slots holding the per-component maxima).  The flush after the tile
 // writes them to HBM, 128 contiguous bytes per component; direct stores from
