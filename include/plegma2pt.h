@@ -294,8 +294,11 @@ p2_status p2_contract_udsc(p2_ctx* ctx, const p2_prop* props, int nprops, const 
  * are written), then records them; the graph keeps its own workspaces, so
  * other calls on the context may run between replays.  Propagator and result
  * pointers are those given at creation: refill the propagator buffers in place
- * between launches.  Device-resident propagators and results only.  Errors
- * are reported on the parent context.  No counterpart in the reference (it
+ * between launches.  Device-resident propagators and results only.  The
+ * requests must form one batch (same form, contraction set, momentum list and
+ * propagator precisions; any sources and windows): P2_ERR_UNSUPPORTED
+ * otherwise, make one graph per batch.  Errors are reported on the parent
+ * context.  No counterpart in the reference (it
  * launches each kernel from the host and synchronises after each,
  * lib/kernels/PLEGMA_baryons.cuh:134-164). */
 typedef struct p2_graph p2_graph;

@@ -807,6 +807,11 @@ p2_status p2_contract_project(p2_ctx* c, const p2_prop* props, int nprops, const
       done[j] = 1;
       idx.push_back(j);
     }
+    // a recorded graph holds one batch: its slice descriptors and tables are
+    // uploaded once, from buffers a second batch would overwrite
+    if (c->capturing && (int)idx.size() != nreq)
+      return c->fail(P2_ERR_UNSUPPORTED,
+                     "a graph records one batch: requests must share form, contractions, momenta and precision");
     // device result of each request; host results go through one device buffer
     std::vector<double*> outs(nreq, nullptr);
     size_t host_total = 0;

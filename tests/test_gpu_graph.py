@@ -82,6 +82,28 @@ def test_graph_rejects_host_buffers():
     ctx.close()
 
 
+def test_graph_rejects_two_batches():
+    """A graph records one batch (its descriptors and tables are uploaded
+    once): requests with different contraction sets are refused, and the
+    context still runs them eagerly."""
+    ctx = p2.Context((4, 4, 4, 8))
+    bufs = device_props(ctx, [(5, 0), (5, 1)], t0=1)
+    props = [ctx.prop(b.data_ptr()) for b in bufs]
+    moms = p2.mom_list(1)
+    outs, reqs = [], []
+    for what in (NUC, p2.MESON_G16):
+        out = torch.zeros(p2.block_info(what, 8, len(moms))[1], dtype=torch.complex128, device="cuda")
+        outs.append(out)
+        reqs.append(ctx.request((0, 1, 2, 1), 8, what, out.data_ptr(), moms=moms, mode=p2.P2_SPLIT_FP16))
+    with pytest.raises(p2.P2Error) as e:
+        ctx.graph(props, reqs)
+    assert e.value.status == p2.P2_ERR_UNSUPPORTED
+    assert "one batch" in str(e.value)
+    ctx.contract_project(props, reqs)
+    ctx.sync()
+    ctx.close()
+
+
 @pytest.mark.parametrize("mode", [p2.P2_PLAIN_FP64, p2.P2_SPLIT_FP16])
 def test_tuner_caches_choices_and_stays_accurate(tmp_path, mode):
     path = str(tmp_path / "tune.tsv")
