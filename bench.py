@@ -99,11 +99,13 @@ def peaks():
         return 6650.0, 1590.0, "fallback"
 
 
-def cpu_baseline_port(steps=1):
+def cpu_baseline_port(steps=1, seconds=10.0):
     """The FP64 oracle (faithful restatement of the reference loops, OpenMP on
-    all host cores) on a bounded sample: one time slice of a 16^3 spatial
+    all host cores) on a bounded sample: time slices of a 16^3 spatial
     lattice with the same K = 288 components and 123 momenta (cost per site
-    does not depend on the volume)."""
+    does not depend on the volume), repeated for about `seconds` per step;
+    the step's value is its sites over its time, the result the median over
+    steps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as orc
     from plegma_b200 import spin
@@ -114,11 +116,18 @@ def cpu_baseline_port(steps=1):
     d = (rng.standard_normal((144, V3 * 4)) + 1j * rng.standard_normal((144, V3 * 4)))
     moms = np.array(spin.create_mom(Q2MAX), dtype=np.int32)
     orc.twopt(Ls, u, d, (1, 2, 3, 0), moms, 1 | 8, [0], want_abs=False)  # warm-up (page-in, thread pool)
-    vals = []
+    vals, nslice = [], 0
     for _ in range(steps):
         t = time.perf_counter()
-        orc.twopt(Ls, u, d, (1, 2, 3, 0), moms, 1 | 8, [1], want_abs=False)
-        vals.append(V3 / (time.perf_counter() - t))
+        n = 0
+        while True:
+            orc.twopt(Ls, u, d, (1, 2, 3, 0), moms, 1 | 8, [n % 4], want_abs=False)
+            n += 1
+            el = time.perf_counter() - t
+            if el >= seconds:
+                break
+        vals.append(n * V3 / el)
+        nslice += n
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     model = ""
     try:
@@ -128,16 +137,18 @@ def cpu_baseline_port(steps=1):
         pass
     return {"value": float(np.median(vals)), "unit": "sites/s", "cores": cores, "cpu_model": model,
             "nproc": os.cpu_count(), "kind": "port",
-            "sample": f"1 time slice of 16^3 ({V3} sites), K=288, 123 momenta, FP64 oracle, median of {steps}"}
+            "sample": f"time slices of 16^3 ({V3} sites each), K=288, 123 momenta, FP64 oracle: {nslice} slices "
+                      f"in {steps} step(s) of ~{seconds:g} s, median over steps"}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    for _ in range(args.warmup):
-        cpu_baseline_port(1)
+    # each step a ~2 s sample of the workload, so that --steps 40 ends in under two minutes
+    if args.warmup > 0:
+        cpu_baseline_port(args.warmup, seconds=2.0)
     t = time.perf_counter()
-    cb = cpu_baseline_port(args.steps)
+    cb = cpu_baseline_port(args.steps, seconds=2.0)
     el = time.perf_counter() - t
     v = cb["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "sites/s", "n_gpus": args.gpus,
@@ -441,7 +452,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:  # the host baseline is reported at N = 1 only
         try:
-            cpu = cpu_baseline_port(1)
+            cpu = cpu_baseline_port(1, seconds=10.0)
         except Exception as ex:  # reported, not fatal
             cpu = {"value": None, "error": str(ex)}
 
