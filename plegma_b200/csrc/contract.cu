@@ -292,8 +292,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
 
   int cur = -1;  // slice whose maxima the spare slots hold
   // running maxima in registers: nucleon outputs of lane l (slots 0, 1) and
-  // the staged meson outputs this thread writes out (slots 2 + g2); the
-  // Delta instantiation tracks its maxima in shared memory only
+  // the staged meson outputs this thread writes out (slots 2 + g2, or
+  // 2 + 4 u + j with the flush's sink stage); the Delta instantiation tracks
+  // its maxima in shared memory only
   constexpr int kSlots = DELTA ? 1 : 18;
   float rmax[kSlots];
 #pragma unroll
