@@ -246,3 +246,23 @@ def test_ft_apply_split_odd_volume():
     asum = np.abs(f).reshape(dof, nt, ctx.V3).sum(axis=2).T
     assert (np.abs(out.reshape(ref.shape) - ref).max(axis=2) / asum).max() < 1e-6
     ctx.close()
+
+
+@pytest.mark.parametrize("mode", [p2.P2_PLAIN_FP64, p2.P2_SPLIT_FP16])
+def test_window_outside_the_views_is_empty(ctx_small, mode):
+    """Views that store none of the request's window slices (the reference
+    skips slices outside its time slab the same way): the call succeeds,
+    launches nothing and leaves the result untouched; a window that overlaps
+    the views in part fills exactly the overlapping slices."""
+    ctx = ctx_small
+    T = ctx.L[3]
+    bufs = device_props(ctx, [(23, 0), (23, 1)], t0=2, t_first=5, nt=2)  # slices 5, 6
+    what = NUC | p2.MESON_G16
+    out, moms = run(ctx, bufs, (1, 0, 2, 1), 3, what, q2max=1, mode=mode, t_first=5, nt=2)  # slices 1, 2, 3
+    assert not np.any(out)
+    out, moms = run(ctx, bufs, (1, 0, 2, 4), 3, what, q2max=1, mode=mode, t_first=5, nt=2)  # slices 4, 5, 6
+    g = p2.result_blocks(what, 3, len(moms), out)
+    for bit in g:
+        assert not np.any(g[bit][:, :, 0]), bit  # tau 0 = slice 4: not stored
+        assert np.all(np.any(g[bit][:, :, 1:] != 0, axis=(-1, -2))), bit
+    assert T == 8
