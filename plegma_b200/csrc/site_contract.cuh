@@ -253,6 +253,32 @@ static_assert(typea_tau(kDeltaLane[0]) == 1 && typea_tau(kDeltaLane[1]) == 1 && 
 static_assert(typea_lane(kDeltaLane[0]) == 0 && typea_lane(kDeltaLane[1]) == 0 && typea_lane(kDeltaLane[2]) == 1,
               "Delta type-a lanes");
 
+// sum_i g[i] z[i] over the 9 colour entries.  FP32: paired FMAs with two
+// accumulators, (gx zx, gx zy) and (gy zx, gy zy), so that z enters as the
+// natural (Re, Im) pair of its shared-memory load and only g is broadcast
+// (once per g for all the dot products it takes part in).
+template <typename R>
+__device__ __forceinline__ Cx<R> cdot9(const Cx<R> g[9], const Cx<R> z[9]) {
+  Cx<R> r = czero<R>();
+#pragma unroll
+  for (int i = 0; i < 9; i++) cmac(r, g[i], z[i]);
+  return r;
+}
+template <>
+__device__ __forceinline__ Cx<float> cdot9<float>(const Cx<float> g[9], const Cx<float> z[9]) {
+  f32x2 px = f2pack(0.f, 0.f), py = f2pack(0.f, 0.f);
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    const f32x2 zz = f2pack(z[i].x, z[i].y);
+    px = f2fma(f2pack(g[i].x, g[i].x), zz, px);
+    py = f2fma(f2pack(g[i].y, g[i].y), zz, py);
+  }
+  float a, b, c, d;
+  f2unpack(px, a, b);
+  f2unpack(py, c, d);
+  return cx<float>(a - d, b + c);
+}
+
 // G^{YX} from G^{XY}: move lane (y', x') to lane (x', y') with the table's sign.
 template <typename R>
 __device__ __forceinline__ void diquark_transpose(Cx<R> q[9], int l, unsigned mask, R sign) {
@@ -330,10 +356,7 @@ __device__ __forceinline__ Cx<typename Row::R> diquark_slots(const Cx<typename R
     for (int m = 0; m < 4; m++) {
       Cx<R> z[9];
       row.load9(Z + m * 4 + dl.z2, z);
-      Cx<R> p2 = czero<R>();
-#pragma unroll
-      for (int i = 0; i < 9; i++) cmac(p2, g[i], z[i]);
-      P[m] = cscale(p2, f2);
+      P[m] = cscale(cdot9(g, z), f2);
     }
     r = r + scatter(P, 3, 2);
   }
@@ -347,10 +370,7 @@ __device__ __forceinline__ Cx<typename Row::R> diquark_slots(const Cx<typename R
     for (int m = 0; m < 4; m++) {
       Cx<R> z[9];
       row.load9(Z + m * 4 + dl.z1, z);
-      Cx<R> p1 = czero<R>();
-#pragma unroll
-      for (int i = 0; i < 9; i++) cmac(p1, g[i], z[i]);
-      P[m] = cscale(p1, f1);
+      P[m] = cscale(cdot9(g, z), f1);
     }
     r = r + shfl_idx16(scatter(P, 1, 0), ((l & 3) << 2) | (l >> 2), mask);
   }
@@ -392,10 +412,7 @@ __device__ __forceinline__ Cx<typename Row::R> diquark_slot1_transposed(const Cx
     for (int m = 0; m < 4; m++) {
       Cx<R> z[9];
       row.load9(Z + m * 4 + dlT.z1, z);
-      Cx<R> p = czero<R>();
-#pragma unroll
-      for (int i = 0; i < 9; i++) cmac(p, g[i], z[i]);
-      P[m] = cscale(p, f1);
+      P[m] = cscale(cdot9(g, z), f1);
     }
     // reduce-scatter over lane bits 3, 2: lane (a, b) keeps m = a
     const bool b1 = (l >> 3) & 1, b0 = (l >> 2) & 1;
@@ -428,10 +445,7 @@ __device__ __forceinline__ Cx<typename Row::R> diquark_typea(const Cx<typename R
   typedef typename Row::R R;
   Cx<R> z[9];
   row.load9(Z + (l >> 2) * 4 + (l & 3), z);
-  Cx<R> r = czero<R>();
-#pragma unroll
-  for (int i = 0; i < 9; i++) cmac(r, D[i], z[i]);
-  return r;
+  return cdot9(D, z);
 }
 
 // All Wick terms of one group: slot terms with the Wick coefficients
