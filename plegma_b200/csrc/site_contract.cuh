@@ -199,15 +199,68 @@ __device__ __forceinline__ void diquark_acc_ct(const Row& row, int X, int Y, int
   constexpr int nu = sink_entry(S, iA, 0), lam = sink_entry(S, iA, 1), sg = sink_entry(S, iA, 2);
   diquark_acc(row, X, Y, nu, lam, typename Row::R(sg), xp, yp, q);
 }
+// FP32 tile: the same products with paired FMAs and two accumulators per
+// output, (ax bx, ax by) and (ay bx, ay by): b enters as its natural (Re, Im)
+// pair (and its negation for the subtracted terms), a as broadcasts shared
+// by its four terms.
+template <int S, int iA>
+__device__ __forceinline__ void diquark_acc_ct_f32(const RowF32& row, int X, int Y, int xp, int yp, f32x2 px[9],
+                                                   f32x2 py[9]) {
+  constexpr int nu = sink_entry(S, iA, 0), lam = sink_entry(S, iA, 1), sg = sink_entry(S, iA, 2);
+  Cx<float> a[9], b[9];
+  row.load9(X + nu * 4 + xp, a);
+  row.load9(Y + lam * 4 + yp, b);
+  f32x2 bp[9], bn[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    bp[i] = f2pack(b[i].x, b[i].y);
+    bn[i] = f2pack(-b[i].x, -b[i].y);
+  }
+  auto term = [&](int o, int ia, int ib, int sign) {
+    const f32x2 bb = sign * sg > 0 ? bp[ib] : bn[ib];
+    px[o] = f2fma(f2pack(a[ia].x, a[ia].x), bb, px[o]);
+    py[o] = f2fma(f2pack(a[ia].y, a[ia].y), bb, py[o]);
+  };
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      const int e1 = (e + 1) % 3, e2 = (e + 2) % 3, o = c * 3 + e;
+      term(o, c1 * 3 + e1, c2 * 3 + e2, 1);
+      term(o, c1 * 3 + e2, c2 * 3 + e1, -1);
+      term(o, c2 * 3 + e1, c1 * 3 + e2, -1);
+      term(o, c2 * 3 + e2, c1 * 3 + e1, 1);
+    }
+  }
+}
+
 template <int S, typename Row>
 __device__ __forceinline__ void diquark_G_ct(const Row& row, int X, int Y, int xp, int yp, Cx<typename Row::R> q[9]) {
   typedef typename Row::R R;
+  if constexpr (sizeof(R) == 4) {
+    f32x2 px[9], py[9];
 #pragma unroll
-  for (int i = 0; i < 9; i++) q[i] = czero<R>();
-  diquark_acc_ct<S, 0>(row, X, Y, xp, yp, q);
-  diquark_acc_ct<S, 1>(row, X, Y, xp, yp, q);
-  diquark_acc_ct<S, 2>(row, X, Y, xp, yp, q);
-  diquark_acc_ct<S, 3>(row, X, Y, xp, yp, q);
+    for (int i = 0; i < 9; i++) px[i] = py[i] = f2pack(0.f, 0.f);
+    diquark_acc_ct_f32<S, 0>(row, X, Y, xp, yp, px, py);
+    diquark_acc_ct_f32<S, 1>(row, X, Y, xp, yp, px, py);
+    diquark_acc_ct_f32<S, 2>(row, X, Y, xp, yp, px, py);
+    diquark_acc_ct_f32<S, 3>(row, X, Y, xp, yp, px, py);
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+      float ax, ay, bx, by;
+      f2unpack(px[i], ax, ay);  // (sum ax bx, sum ax by)
+      f2unpack(py[i], bx, by);  // (sum ay bx, sum ay by)
+      q[i] = cx<float>(ax - by, ay + bx);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 9; i++) q[i] = czero<R>();
+    diquark_acc_ct<S, 0>(row, X, Y, xp, yp, q);
+    diquark_acc_ct<S, 1>(row, X, Y, xp, yp, q);
+    diquark_acc_ct<S, 2>(row, X, Y, xp, yp, q);
+    diquark_acc_ct<S, 3>(row, X, Y, xp, yp, q);
+  }
 }
 
 // Type-a weights fa = cN sN - cL sL of every source table vanish outside one
