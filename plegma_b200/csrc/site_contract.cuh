@@ -60,7 +60,6 @@ struct LaneTables {
 };
 
 __constant__ int c_nuc_lane[16][8] = P2_INIT_NucLane;
-__constant__ int c_delta_sink[3][4][3] = P2_INIT_DeltaSink;
 __constant__ int c_delta_lane[3][16][8] = P2_INIT_DeltaLane;
 __constant__ int c_meson_lane[16][3] = P2_INIT_MesonLane;
 __constant__ int c_meson_flush[4][4][2] = P2_INIT_MesonFlush;
@@ -176,18 +175,8 @@ __device__ __forceinline__ void diquark_acc(const Row& row, int X, int Y, int nu
   }
 }
 
-// G^{XY} = sum over a sink table sink[iA] = (nu, lam, sA) of sA P^{XY}_{(nu, lam)}.
-template <typename Row>
-__device__ __forceinline__ void diquark_G(const Row& row, int X, int Y, const int (*sink)[3], int xp, int yp,
-                                          Cx<typename Row::R> q[9]) {
-  typedef typename Row::R R;
-#pragma unroll
-  for (int i = 0; i < 9; i++) q[i] = czero<R>();
-#pragma unroll 1
-  for (int iA = 0; iA < 4; iA++) diquark_acc(row, X, Y, sink[iA][0], sink[iA][1], R(sink[iA][2]), xp, yp, q);
-}
-
-// The same with a sink table known at compile time (S = 0: nucleon C g5,
+// G^{XY} = sum over a sink table sink[iA] = (nu, lam, sA) of sA P^{XY}_{(nu, lam)},
+// the table known at compile time (S = 0: nucleon C g5,
 // 1..3: Delta C g_k, 4: C): signs fold into the products, block offsets into
 // the load addresses.
 __host__ __device__ constexpr int sink_entry(int S, int i, int f) {
@@ -203,10 +192,9 @@ __device__ __forceinline__ void diquark_acc_ct(const Row& row, int X, int Y, int
 // output, (ax bx, ax by) and (ay bx, ay by): b enters as its natural (Re, Im)
 // pair (and its negation for the subtracted terms), a as broadcasts shared
 // by its four terms.
-template <int S, int iA>
-__device__ __forceinline__ void diquark_acc_ct_f32(const RowF32& row, int X, int Y, int xp, int yp, f32x2 px[9],
-                                                   f32x2 py[9]) {
-  constexpr int nu = sink_entry(S, iA, 0), lam = sink_entry(S, iA, 1), sg = sink_entry(S, iA, 2);
+template <int nu, int lam, int sg>
+__device__ __forceinline__ void dq_acc_f32(const RowF32& row, int X, int Y, int xp, int yp, f32x2 px[9],
+                                           f32x2 py[9]) {
   Cx<float> a[9], b[9];
   row.load9(X + nu * 4 + xp, a);
   row.load9(Y + lam * 4 + yp, b);
@@ -235,6 +223,42 @@ __device__ __forceinline__ void diquark_acc_ct_f32(const RowF32& row, int X, int
   }
 }
 
+template <int S, int iA>
+__device__ __forceinline__ void diquark_acc_ct_f32(const RowF32& row, int X, int Y, int xp, int yp, f32x2 px[9],
+                                                   f32x2 py[9]) {
+  dq_acc_f32<sink_entry(S, iA, 0), sink_entry(S, iA, 1), sink_entry(S, iA, 2)>(row, X, Y, xp, yp, px, py);
+}
+__device__ __forceinline__ void dq_fin_f32(const f32x2 px[9], const f32x2 py[9], Cx<float> q[9]) {
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    float ax, ay, bx, by;
+    f2unpack(px[i], ax, ay);  // (sum ax bx, sum ax by)
+    f2unpack(py[i], bx, by);  // (sum ay bx, sum ay by)
+    q[i] = cx<float>(ax - by, ay + bx);
+  }
+}
+
+// q = s1 P^{XY}_{(nu1, lam1)} + s2 P^{XY}_{(nu2, lam2)} (the Delta's shared
+// diagonal pairs), paired FMAs on the FP32 tile
+template <int nu1, int lam1, int s1, int nu2, int lam2, int s2, typename Row>
+__device__ __forceinline__ void diquark_pair_ct(const Row& row, int X, int Y, int xp, int yp,
+                                                Cx<typename Row::R> q[9]) {
+  typedef typename Row::R R;
+  if constexpr (sizeof(R) == 4) {
+    f32x2 px[9], py[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) px[i] = py[i] = f2pack(0.f, 0.f);
+    dq_acc_f32<nu1, lam1, s1>(row, X, Y, xp, yp, px, py);
+    dq_acc_f32<nu2, lam2, s2>(row, X, Y, xp, yp, px, py);
+    dq_fin_f32(px, py, q);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 9; i++) q[i] = czero<R>();
+    diquark_acc(row, X, Y, nu1, lam1, R(s1), xp, yp, q);
+    diquark_acc(row, X, Y, nu2, lam2, R(s2), xp, yp, q);
+  }
+}
+
 template <int S, typename Row>
 __device__ __forceinline__ void diquark_G_ct(const Row& row, int X, int Y, int xp, int yp, Cx<typename Row::R> q[9]) {
   typedef typename Row::R R;
@@ -246,13 +270,7 @@ __device__ __forceinline__ void diquark_G_ct(const Row& row, int X, int Y, int x
     diquark_acc_ct_f32<S, 1>(row, X, Y, xp, yp, px, py);
     diquark_acc_ct_f32<S, 2>(row, X, Y, xp, yp, px, py);
     diquark_acc_ct_f32<S, 3>(row, X, Y, xp, yp, px, py);
-#pragma unroll
-    for (int i = 0; i < 9; i++) {
-      float ax, ay, bx, by;
-      f2unpack(px[i], ax, ay);  // (sum ax bx, sum ax by)
-      f2unpack(py[i], bx, by);  // (sum ay bx, sum ay by)
-      q[i] = cx<float>(ax - by, ay + bx);
-    }
+    dq_fin_f32(px, py, q);
   } else {
 #pragma unroll
     for (int i = 0; i < 9; i++) q[i] = czero<R>();
@@ -726,12 +744,8 @@ __device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt,
 #pragma unroll
       for (int i = 0; i < 9; i++) q[i] = g == 0 ? ga[i] - gb[i] : ga[i] + gb[i];
     } else if (!kShare && it == 1) {
-#pragma unroll
-      for (int i = 0; i < 9; i++) q[i] = q1[i] = czero<R>();
-      diquark_acc(row, kU, kD, 0, 0, R(1), xp, yp, q);
-      diquark_acc(row, kU, kD, 2, 2, R(-1), xp, yp, q);
-      diquark_acc(row, kU, kD, 1, 1, R(1), xp, yp, q1);
-      diquark_acc(row, kU, kD, 3, 3, R(-1), xp, yp, q1);
+      diquark_pair_ct<0, 0, 1, 2, 2, -1>(row, kU, kD, xp, yp, q);
+      diquark_pair_ct<1, 1, 1, 3, 3, -1>(row, kU, kD, xp, yp, q1);
 #pragma unroll
       for (int i = 0; i < 9; i++) {
         const Cx<R> t = q[i];
@@ -742,7 +756,7 @@ __device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt,
 #pragma unroll
       for (int i = 0; i < 9; i++) q[i] = q1[i];
     } else {
-      diquark_G(row, kU, kD, c_delta_sink[g], xp, yp, q);
+      diquark_G_ct<3>(row, kU, kD, xp, yp, q);  // g = 2 (C g_3) in both forms
     }
     const DiquarkLane dl = unpack_diquark_lane(g == 0 ? lt.delta[0] : g == 1 ? lt.delta[1] : lt.delta[2]);
     diquark_D(q, R(4 * dl.sN), mask, g == 2 ? 1 : 0, D);  // cN = 4, cL = 0
@@ -756,12 +770,8 @@ __device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt,
     const int X = pair == 0 ? kU : kD;
     const int O = pair == 0 ? kD : kU;
     Cx<R> ga[9], gb[9];
-#pragma unroll
-    for (int i = 0; i < 9; i++) ga[i] = gb[i] = czero<R>();
-    diquark_acc(row, X, X, 0, 0, R(1), xp, yp, ga);
-    diquark_acc(row, X, X, 2, 2, R(-1), xp, yp, ga);
-    diquark_acc(row, X, X, 1, 1, R(1), xp, yp, gb);
-    diquark_acc(row, X, X, 3, 3, R(-1), xp, yp, gb);
+    diquark_pair_ct<0, 0, 1, 2, 2, -1>(row, X, X, xp, yp, ga);
+    diquark_pair_ct<1, 1, 1, 3, 3, -1>(row, X, X, xp, yp, gb);
 #pragma unroll
     for (int i = 0; i < 9; i++) {
       const Cx<R> t = ga[i];
@@ -775,10 +785,7 @@ __device__ __forceinline__ void delta_site(const Row& row, const LaneTables& lt,
 #pragma unroll
         for (int i = 0; i < 9; i++) q[i] = g == 0 ? ga[i] : gb[i];
       } else {
-#pragma unroll
-        for (int i = 0; i < 9; i++) q[i] = czero<R>();
-        diquark_acc(row, X, X, 0, 1, R(1), xp, yp, q);
-        diquark_acc(row, X, X, 2, 3, R(-1), xp, yp, q);
+        diquark_pair_ct<0, 1, 1, 2, 3, -1>(row, X, X, xp, yp, q);
         Cx<R> t[9];
 #pragma unroll
         for (int i = 0; i < 9; i++) t[i] = q[i];
