@@ -144,3 +144,25 @@ def test_udsc_dataset_selection_follows_the_reference_filters():
     only_ch = p2.udsc_datasets(R((0, 0, 0, 0), 4, 0, prop_u=0, prop_d=1, prop_s=2, prop_c=3, only_ch=True))
     assert only_ch == [n for k, dss in prods if "c" in k for n, _, _ in dss]
     assert p2.udsc_datasets(R((0, 0, 0, 0), 4, 0, prop_s=0, only_ch=True)) == []
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/plegma2pt.h compiles as C99 (the boundary a cgo, JNI or
+    N-API stub would include) and links against the library."""
+    src = tmp_path / "abi.c"
+    src.write_text('#include "plegma2pt.h"\n'
+                   "int main(void) {\n"
+                   "  int moms[3 * 19];\n"
+                   "  if (p2_components(P2_NUCLEON_CG5 | P2_MESON_G16) != 288) return 1;\n"
+                   "  if (p2_mom_list(2, moms) != 19) return 2;\n"
+                   "  return 0;\n"
+                   "}\n")
+    exe = tmp_path / "abi"
+    libdir = os.path.dirname(p2.LIB_PATH)
+    import subprocess
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                        str(exe), "-L", libdir, "-lplegma2pt", "-Wl,-rpath," + libdir],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, (r.returncode, r.stderr)
