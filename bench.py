@@ -163,7 +163,7 @@ def run_reference(args, rank, world):
 # DRAM bytes (read + write) per site of the dominant kernel, measured with ncu
 # on the 32^3 x 16 case of the same kernel; traffic grows with the sites a
 # launch processes, so it scales to the benchmark's launches
-TRAFFIC_PER_SITE = {("contract_f32", "split"): 6863, ("contract_plain_fp64", "plain"): 9134}
+TRAFFIC_PER_SITE = {("contract_f32", "split"): 6863, ("contract_plain_fp64", "plain"): 9129}
 
 BATCHED = {
     # name: (lattice, sources, window range, |n|^2 max, propagator precision, decay, seed)
