@@ -22,8 +22,12 @@
 // Swapping the two diquark lines transposes the lanes: G^{YX}(y',x') =
 // sign G^{XY}(x',y'), sign -1 for C g5 (antisymmetric), +1 for C g_k.
 //   nucleon, per dataset: direct term = type a (cN = 1), exchange = slot 1 (c1A = -1)
-//   -> 144 + 45 products per lane for the first dataset, 45 for the second;
+//   -> 144 + 45 products per lane for the first dataset, 45 for the second
+//   (formed on the transposed lanes, so G^{ud} never moves between lanes);
 //   the reference spends ~1.1e5 per site and dataset.
+// On the FP32 tile the colour sums run as paired FMAs (fma.rn.f32x2) with two
+// accumulators per complex output: the shared-memory operand enters as its
+// natural (Re, Im) pair and only the register operand is broadcast.
 //
 // Mesons, all 16 x 16 (G_sink, G_src):
 //   C[g1][g2] = sum G1[d][a] A[a][b] G2[b][z] conj(B[d][z]) over spin and colour.
