@@ -99,35 +99,35 @@ def peaks():
         return 6650.0, 1590.0, "fallback"
 
 
-def cpu_baseline_port(steps=1, seconds=10.0):
+def cpu_baseline_port(steps=1, slices_per_step=4):
     """The FP64 oracle (faithful restatement of the reference loops, OpenMP on
-    all host cores) on a bounded sample: time slices of a 16^3 spatial
-    lattice with the same K = 288 components and 123 momenta (cost per site
-    does not depend on the volume), repeated for about `seconds` per step;
-    the step's value is its sites over its time, the result the median over
-    steps."""
+    all host cores) timed on full 48^3 time slices of the benchmark workload
+    (K = 288 components, 123 momenta; 110,592 sites per slice, 255 MB per
+    slice and flavour, far larger than the host caches).  Each step
+    contracts and projects `slices_per_step` slices; the step's value is its
+    sites over its time, the result the median over steps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as orc
     from plegma_b200 import spin
-    Ls = (16, 16, 16, 4)
-    V3 = 16 ** 3
+    nsl = 4
+    Ls = (48, 48, 48, nsl)
+    V3 = 48 ** 3
     rng = np.random.default_rng(SEED)
-    u = (rng.standard_normal((144, V3 * 4)) + 1j * rng.standard_normal((144, V3 * 4)))
-    d = (rng.standard_normal((144, V3 * 4)) + 1j * rng.standard_normal((144, V3 * 4)))
+    u = np.empty((144, V3 * nsl), dtype=np.complex128)
+    d = np.empty_like(u)
+    for a in (u, d):
+        a.real = rng.standard_normal(a.shape)
+        a.imag = rng.standard_normal(a.shape)
     moms = np.array(spin.create_mom(Q2MAX), dtype=np.int32)
-    orc.twopt(Ls, u, d, (1, 2, 3, 0), moms, 1 | 8, [0], want_abs=False)  # warm-up (page-in, thread pool)
-    vals, nslice = [], 0
+    src = (1, 2, 3, 0)
+    orc.twopt((16, 16, 16, 1), u[:, :4096], d[:, :4096], src, moms, 1 | 8, [0], want_abs=False)  # thread pool up
+    vals, n = [], 0
     for _ in range(steps):
         t = time.perf_counter()
-        n = 0
-        while True:
-            orc.twopt(Ls, u, d, (1, 2, 3, 0), moms, 1 | 8, [n % 4], want_abs=False)
+        for _ in range(slices_per_step):
+            orc.twopt(Ls, u, d, src, moms, 1 | 8, [n % nsl], want_abs=False)
             n += 1
-            el = time.perf_counter() - t
-            if el >= seconds:
-                break
-        vals.append(n * V3 / el)
-        nslice += n
+        vals.append(slices_per_step * V3 / (time.perf_counter() - t))
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     model = ""
     try:
@@ -137,18 +137,59 @@ def cpu_baseline_port(steps=1, seconds=10.0):
         pass
     return {"value": float(np.median(vals)), "unit": "sites/s", "cores": cores, "cpu_model": model,
             "nproc": os.cpu_count(), "kind": "port",
-            "sample": f"time slices of 16^3 ({V3} sites each), K=288, 123 momenta, FP64 oracle: {nslice} slices "
-                      f"in {steps} step(s) of ~{seconds:g} s, median over steps"}
+            "sample": f"full 48^3 time slices ({V3} sites each), K=288, 123 momenta, FP64 oracle: {n} slices in "
+                      f"{steps} step(s) of {slices_per_step}, median over steps"}
+
+
+class SliceChecker:
+    """Per-time-slice error of a run's own output against the FP64 oracle,
+    evaluated outside the timed region on a few slices (the source slice,
+    its neighbours, the middle of the lattice and the slice farthest from
+    the source, where the baryons are smallest):
+        err(t) = max_{p,k} |C(t,p,k) - C_oracle(t,p,k)| / sum_x |c_k(x,t)|.
+    The oracle runs once per slice on a host copy of that slice only."""
+
+    def __init__(self, u, d, src, moms, what, T, V3):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_py as orc
+        from plegma_b200 import lib as p2
+        self.p2, self.moms, self.what, self.T = p2, moms, what, T
+        far = 0 if src[3] >= T - 1 - src[3] else T - 1
+        self.taus = sorted({0, 1, T // 2, T - 1, (far - src[3]) % T})
+        self.ref = {}
+        for tau in self.taus:
+            t = (src[3] + tau) % T
+            hu = u.view(144, -1, V3)[:, t, :].cpu().numpy()
+            hd = d.view(144, -1, V3)[:, t, :].cpu().numpy()
+            out, asum, _ = orc.twopt(L, hu, hd, src, moms, what, [tau], t_first=t)
+            self.ref[tau] = (out[0], asum[0])
+
+    def errors(self, flat):
+        p2 = self.p2
+        res = p2.result_blocks(self.what, self.T, len(self.moms), flat)
+        errs = []
+        for tau in self.taus:
+            out, asum = self.ref[tau]
+            k0, e = 0, 0.0
+            for bit, g, ds, c, _ in p2.block_info(self.what, 1, len(self.moms))[0]:
+                n = g * ds * c
+                ref = out[:, k0:k0 + n].reshape(len(self.moms), g, ds, c).transpose(1, 2, 0, 3)
+                diff = np.abs(res[bit][:, :, tau] - ref).max(axis=2)
+                e = max(e, float((diff / np.maximum(asum[k0:k0 + n].reshape(g, ds, c), 1e-300)).max()))
+                k0 += n
+            errs.append(e)
+        return {"taus": self.taus, "err_t": errs, "max_err_t": max(errs)}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    # each step a ~2 s sample of the workload, so that --steps 40 ends in under two minutes
+    # each step one full 48^3 time slice of the workload (about a second on 16
+    # host cores), so that --steps 40 ends in about a minute
     if args.warmup > 0:
-        cpu_baseline_port(args.warmup, seconds=2.0)
+        cpu_baseline_port(args.warmup, slices_per_step=1)
     t = time.perf_counter()
-    cb = cpu_baseline_port(args.steps, seconds=2.0)
+    cb = cpu_baseline_port(args.steps, slices_per_step=1)
     el = time.perf_counter() - t
     v = cb["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "sites/s", "n_gpus": args.gpus,
@@ -164,6 +205,9 @@ def run_reference(args, rank, world):
 # on the 32^3 x 16 case of the same kernel; traffic grows with the sites a
 # launch processes, so it scales to the benchmark's launches
 TRAFFIC_PER_SITE = {("contract_f32", "split"): 6863, ("contract_plain_fp64", "plain"): 9129}
+# executed FP64 flop per site of the plain site contraction (2 per DFMA, 1 per
+# DADD / DMUL, from the ncu instruction counters of the 32^3 x 16 case)
+FP64_FLOP_PER_SITE = {"contract_plain_fp64": None}
 
 BATCHED = {
     # name: (lattice, sources, window range, |n|^2 max, propagator precision, decay, seed)
@@ -261,6 +305,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-source graph runs")
+    ap.add_argument("--no-check", action="store_true", help="skip the per-slice error check against the oracle")
     ap.add_argument("--tune-cache", default=None,
                     help="tab-separated launch-shape cache: read if present, written after tuning "
                          "(lets a profiler run skip the tuning launches)")
@@ -324,6 +369,12 @@ def main():
 
     results = {}
     hbm, bf16, peak_kind = peaks()
+    # FP64 FMA rate of this device (the plain form's FP64 roofline), clocks sampled meanwhile
+    with ClockSampler(local) as clk64:
+        fp64_tflops, fp64_ms = ctx.fp64_rate()
+    fp64 = {"tflops": fp64_tflops, "kernel": "k_fp64_fma_rate (8 FMA chains/thread, 8 x 256 threads/SM)",
+            "launch_ms": fp64_ms, "clocks": clk64.summary()}
+    checker = SliceChecker(u, d, src, moms, what, L[3], V3) if (rank == 0 and not args.no_check) else None
     for name, mode in forms.items():
         try:
             step(mode)
@@ -357,6 +408,8 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
         results[name] = {"ms": ms, "prof": prof, "clocks": clk.summary()}
+        if checker is not None:  # the timed run's own output, checked after the timed region
+            results[name]["err"] = checker.errors(out.cpu().numpy())
 
     head = "split" if "split" in results else "plain"
     r = results[head]
@@ -395,6 +448,29 @@ def main():
                      "unit": "TFLOP/s", "algorithmic_flop_per_launch": flop / max(n, 1)}
         if head == "split":
             roof_proj.update({"peak": bf16, "frac": ach / bf16, "peak_kind": peak_kind + " dense bf16 (= fp16)"})
+
+    # the plain form's FP64 kernels against the measured FP64 FMA rate: the
+    # projection's algorithmic 8 nmom K flop per site, and the contraction's
+    # executed FP64 flop per site (2 per DFMA, 1 per DADD/DMUL) from ncu
+    roof64 = None
+    if "plain" in results:
+        pp = results["plain"]["prof"]
+        roof64 = {"peak": fp64_tflops, "unit": "TFLOP/s", "peak_kind": "measured (p2_measure_fp64_rate)"}
+        for kname, kms in pp.items():
+            if kname.startswith("project"):
+                fl = 8.0 * nmom * K
+            elif kname.startswith("contract") and FP64_FLOP_PER_SITE.get(kname):
+                fl = FP64_FLOP_PER_SITE[kname]
+            else:
+                continue
+            ach = fl * sites * args.steps / (kms[1] * 1e-3) / 1e12
+            roof64[kname] = {"achieved": ach, "frac": ach / fp64_tflops, "flop_per_site": fl,
+                             "flop_kind": "algorithmic" if kname.startswith("project") else "executed (ncu)"}
+        if "contract_plain_fp64" in pp:
+            n, kms = pp["contract_plain_fp64"]
+            ach = 2 * 144 * 16 * sites * args.steps / (kms * 1e-3) / 1e9
+            roof64["contract_plain_fp64_hbm"] = {"achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                                                 "target_frac": 0.7}
 
     # end to end through the C ABI with host buffers (pinned), copies inside the timed region
     e2e = None
@@ -452,7 +528,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:  # the host baseline is reported at N = 1 only
         try:
-            cpu = cpu_baseline_port(1, seconds=10.0)
+            cpu = cpu_baseline_port(1, slices_per_step=4)
         except Exception as ex:  # reported, not fatal
             cpu = {"value": None, "error": str(ex)}
 
@@ -478,8 +554,12 @@ def main():
                 "config": {"workload": WORKLOAD, "form": head, "L": list(L), "K": K, "nmom": nmom, "seed": SEED,
                            "sites_per_step": sites, "l2": "inputs (49 GB) larger than L2",
                            "parallelism": f"source-sharded x{world}"},
-                "forms": {k: {"ms_per_step": v["ms"], "sites_per_s": sites * world / (v["ms"] * 1e-3)}
-                          for k, v in results.items()},
+                "forms": {k: {"ms_per_step": v["ms"], "sites_per_s": sites * world / (v["ms"] * 1e-3),
+                              "error": v.get("err")} for k, v in results.items()},
+                "max_err_t": (r.get("err") or {}).get("max_err_t"),
+                "err_note": "max over the checked slices of max_{p,k} |C - C_oracle| / sum_x |c_k(x,t)|, "
+                            "FP64 oracle, this run's own output",
+                "fp64_peak": fp64, "roofline_fp64": roof64,
                 "roofline": roof, "roofline_projection": roof_proj, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": r["clocks"], "batched": batched}
         print(json.dumps(line), flush=True)

@@ -345,6 +345,14 @@ p2_status p2_profile_enable(p2_ctx* ctx, int on);
 /* Fills up to max entries, returns the number of kernels seen; reset != 0 clears. */
 int p2_profile_read(p2_ctx* ctx, p2_kernel_time* out, int max, int reset);
 
+/* FP64 FMA rate of the context's device, the roofline denominator of the
+ * plain form's FP64 kernels: an FMA loop (8 independent chains per thread,
+ * 8 CTAs of 256 threads per SM) timed with CUDA events on the context's
+ * stream, best of five launches after one warm-up.  *tflops = 2 x FMAs /
+ * time; *ms (may be NULL) the launch time.  Synchronises the stream.  No
+ * counterpart in the reference. */
+p2_status p2_measure_fp64_rate(p2_ctx* ctx, double* tflops, double* ms);
+
 /* ---- synthetic inputs (benchmarks and tests) --------------------------- */
 /* Fill a propagator with entries Re, Im ~ N(0,1) scaled by exp(-a*|t - t0|),
  * drawn from a counter-based SplitMix64 + Box-Muller stream keyed by

@@ -46,13 +46,15 @@ def oracle():
 
 
 def reference():
-    """The reference's NtoN / Delta functions, or None when not built here."""
+    """The reference's baryon functions and meson kernels, or None when not built here."""
     global _ref
     if _ref is None and os.path.exists(REF_LIB):
         lib = C.CDLL(REF_LIB)
         lib.ref_nucleon.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         lib.ref_delta.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         lib.ref_light.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        lib.ref_meson_ft.argtypes = [C.c_int, C.POINTER(C.c_int), C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                     C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.c_void_p]
         _ref = lib
     return _ref
 
@@ -141,6 +143,28 @@ def ref_light(u1, d1, which):
     u1 = np.ascontiguousarray(u1, dtype=np.complex128)
     d1 = np.ascontiguousarray(d1, dtype=np.complex128)
     lib.ref_light(u1.ctypes.data, d1.ctypes.data, int(which), out.ctypes.data)
+    return out
+
+
+def ref_meson_ft(kind, L, u, d, j, src, moms):
+    """The reference's meson kernels with their in-kernel projection on local
+    slice j (kind 0: contract_mesons_device, 20 components; 1:
+    contract_mesons_all_device, 34; 2: contract_mesons_new_device, 10).
+    u, d: complex128 [144][V3*nt].  Returns [nmom][ncomp] complex."""
+    lib = reference()
+    L = _ip(L[:3])
+    V3 = int(L[0] * L[1] * L[2])
+    u = np.ascontiguousarray(u, dtype=np.complex128).reshape(144, -1)
+    d = np.ascontiguousarray(d, dtype=np.complex128).reshape(144, -1)
+    nt = u.shape[1] // V3
+    moms = _ip(moms).reshape(-1, 3)
+    ncomp = {0: 20, 1: 34, 2: 10}[kind]
+    out = np.zeros((len(moms), ncomp), dtype=np.complex128)
+    rc = lib.ref_meson_ft(int(kind), L.ctypes.data_as(C.POINTER(C.c_int)), nt, u.ctypes.data, d.ctypes.data, int(j),
+                          _ip(src[:3]).ctypes.data_as(C.POINTER(C.c_int)), moms.ctypes.data_as(C.POINTER(C.c_int)),
+                          len(moms), out.ctypes.data)
+    if rc != ncomp:
+        raise RuntimeError(f"ref_meson_ft failed ({rc})")
     return out
 
 

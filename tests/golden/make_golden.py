@@ -100,7 +100,9 @@ def reference_udsc_digests(kern: str):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PLEGMA_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT (or set PLEGMA_REFERENCE)")
     digests = reference_digests(ref)
     path = os.path.join(HERE, "ref_table_digests.json")
     with open(path, "w") as f:

@@ -1,0 +1,173 @@
+"""Per-time-slice error of the split-FP16 form at the benchmark sizes, where
+its FP32 accumulation and per-component FP16 scaling actually run:
+
+  * 48^3 x 96, nucleon C g5 + 16x16 mesons, 123 momenta (the metric
+    configuration, the exact workload of bench.py);
+  * 32^3 x 64, 16 sources with windows of 8-20 slices stored per window,
+    nucleon + Delta (both isospins) + 16x16 mesons, K = 480, one batched call;
+  * 64^3 x 128, FP32 propagators (decay 0.4), K = 480, 257 momenta, on
+    windows of slices held around the source and at the far side of the
+    lattice.
+
+err(t) = max_{p,k} |C_gpu - C_oracle| / sum_x |c_k(x,t)| <= 1e-6 against the
+FP64 oracle on the slices beside the source, at the source and at the
+largest |t - t0| (where the baryons are ~1e-31 of the source slice's value).
+The oracle runs only on the checked slices (copied to the host one at a
+time), so each test takes seconds of host time per slice."""
+import numpy as np
+import pytest
+import torch
+
+from plegma_b200 import lib as p2
+
+import p2test  # noqa: F401  (puts the oracle on the path)
+import oracle_py as orc  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+TOL_SPLIT = 1e-6
+TOL_PLAIN = 1e-12
+
+
+def _source(L, seed):
+    rng = np.random.default_rng(seed)
+    return tuple(int(rng.integers(0, L[d])) for d in range(4))
+
+
+def _slice(buf, V3, j):
+    """Slice j of a device propagator [144][nt * V3] as a host array [144][V3]."""
+    return buf.view(144, -1, V3)[:, j, :].cpu().numpy()
+
+
+def _slice_error(L, res_blocks, u, d, src, moms, what, tau, t_global, fp32=False):
+    """err(tau) of one slice: the oracle on the slice's host copy."""
+    out, asum, _ = orc.twopt(L, u, d, src, moms, what, [tau], t_first=t_global, fp32=fp32)
+    k0, err = 0, 0.0
+    for bit, g, ds, c, _ in p2.block_info(what, 1, len(moms))[0]:
+        n = g * ds * c
+        ref = out[0, :, k0:k0 + n].reshape(len(moms), g, ds, c).transpose(1, 2, 0, 3)
+        rabs = asum[0, k0:k0 + n].reshape(g, ds, c)
+        gpu = res_blocks[bit][:, :, tau]  # [g][ds][nmom][c]
+        diff = np.abs(gpu - ref).max(axis=2)
+        err = max(err, float((diff / np.maximum(rabs, 1e-300)).max()))
+        k0 += n
+    return err
+
+
+def _far_tau(T, t0):
+    """Source-relative time of the slice farthest from t0 (|t - t0| not periodic)."""
+    t = 0 if t0 >= T - 1 - t0 else T - 1
+    return (t - t0) % T
+
+
+def test_split_error_metric_configuration_48():
+    L = (48, 48, 48, 96)
+    V3 = L[0] * L[1] * L[2]
+    seed = 1003
+    src = _source(L, seed)
+    what = p2.NUCLEON_CG5 | p2.MESON_G16
+    moms = p2.mom_list(9)
+    ctx = p2.Context(L)
+    u = torch.empty(144 * V3 * L[3], dtype=torch.complex128, device="cuda")
+    d = torch.empty_like(u)
+    ctx.synth(u.data_ptr(), True, p2.P2_FP64, seed, 0, src[3], 0.5)
+    ctx.synth(d.data_ptr(), True, p2.P2_FP64, seed, 1, src[3], 0.5)
+    props = [ctx.prop(u.data_ptr()), ctx.prop(d.data_ptr())]
+    _, total = p2.block_info(what, L[3], len(moms))
+    taus = sorted({0, 1, L[3] - 1, L[3] // 2, _far_tau(L[3], src[3])})
+    errs = {}
+    for mode in (p2.P2_SPLIT_FP16, p2.P2_PLAIN_FP64):
+        out = torch.zeros(total, dtype=torch.complex128, device="cuda")
+        ctx.contract_project(props, [ctx.request(src, L[3], what, out.data_ptr(), mode=mode, moms=moms)])
+        ctx.sync()
+        res = p2.result_blocks(what, L[3], len(moms), out.cpu().numpy())
+        e = []
+        for tau in taus:
+            t = (src[3] + tau) % L[3]
+            e.append(_slice_error(L, res, _slice(u, V3, t), _slice(d, V3, t), src, moms, what, tau, t))
+        errs[mode] = np.array(e)
+        del out
+    ctx.close()
+    assert errs[p2.P2_SPLIT_FP16].max() < TOL_SPLIT, (taus, errs)
+    assert errs[p2.P2_PLAIN_FP64].max() < TOL_PLAIN, (taus, errs)
+
+
+def test_split_error_batched_configuration_32():
+    """16 sources, windows 8-20 stored per window (the batched benchmark's
+    storage), one p2_contract_project call; checked on three sources."""
+    L = (32, 32, 32, 64)
+    V3 = L[0] * L[1] * L[2]
+    seed = 1004
+    rng = np.random.default_rng(seed)
+    what = p2.NUCLEON_CG5 | p2.DELTA_ISO12 | p2.DELTA_ISO32 | p2.MESON_G16
+    moms = p2.mom_list(9)
+    ctx = p2.Context(L)
+    srcs, bufs, props, reqs, outs = [], [], [], [], []
+    for i in range(16):
+        src = tuple(int(rng.integers(0, L[dd])) for dd in range(4))
+        W = int(rng.integers(8, 21))
+        for f in range(2):
+            b = torch.empty(144 * V3 * W, dtype=torch.complex128, device="cuda")
+            ctx.synth(b.data_ptr(), True, p2.P2_FP64, seed + i, f, src[3], 0.5, src[3], W)
+            bufs.append(b)
+            props.append(ctx.prop(b.data_ptr(), t_first=src[3], nt=W))
+        _, total = p2.block_info(what, W, len(moms))
+        o = torch.zeros(total, dtype=torch.complex128, device="cuda")
+        outs.append(o)
+        reqs.append(ctx.request(src, W, what, o.data_ptr(), mode=p2.P2_SPLIT_FP16, moms=moms, prop_u=2 * i,
+                                prop_d=2 * i + 1))
+        srcs.append((src, W))
+    ctx.contract_project(props, reqs)
+    ctx.sync()
+    errs = []
+    for i in (0, 7, 15):
+        src, W = srcs[i]
+        res = p2.result_blocks(what, W, len(moms), outs[i].cpu().numpy())
+        for tau in sorted({0, 1, W - 1}):
+            t = (src[3] + tau) % L[3]
+            e = _slice_error(L, res, _slice(bufs[2 * i], V3, tau), _slice(bufs[2 * i + 1], V3, tau), src, moms, what,
+                             tau, t)
+            errs.append((i, tau, e))
+    ctx.close()
+    assert max(e for _, _, e in errs) < TOL_SPLIT, errs
+
+
+def test_split_error_large_configuration_64():
+    """64^3 x 128 with FP32 propagators and 257 momenta (262,144 sites per
+    slice): one source whose views hold the two slices at the source and the
+    two farthest from it (a request over the full window computes the slices
+    its views hold)."""
+    L = (64, 64, 64, 128)
+    V3 = L[0] * L[1] * L[2]
+    seed = 1005
+    src = _source(L, seed)
+    what = p2.NUCLEON_CG5 | p2.DELTA_ISO12 | p2.DELTA_ISO32 | p2.MESON_G16
+    moms = p2.mom_list(16)
+    assert len(moms) == 257
+    ctx = p2.Context(L)
+    tfar = _far_tau(L[3], src[3])
+    errs = []
+    for tau0 in (0, min(tfar, L[3] - 2)):
+        t_first = (src[3] + tau0) % L[3]
+        bufs = []
+        for f in range(2):
+            b = torch.empty(144 * V3 * 2, dtype=torch.complex64, device="cuda")
+            ctx.synth(b.data_ptr(), True, p2.P2_FP32, seed, f, src[3], 0.4, t_first, 2)
+            bufs.append(b)
+        props = [ctx.prop(b.data_ptr(), p2.P2_FP32, t_first=t_first, nt=2) for b in bufs]
+        _, total = p2.block_info(what, L[3], len(moms))
+        out = torch.zeros(total, dtype=torch.complex128, device="cuda")
+        req = ctx.request(src, L[3], what, out.data_ptr(), mode=p2.P2_SPLIT_FP16, moms=moms)
+        assert ctx.local_taus(props, req) == [tau0, tau0 + 1]
+        ctx.contract_project(props, [req])
+        ctx.sync()
+        res = p2.result_blocks(what, L[3], len(moms), out.cpu().numpy())
+        for j in range(2):
+            tau = tau0 + j
+            t = (src[3] + tau) % L[3]
+            e = _slice_error(L, res, _slice(bufs[0], V3, j), _slice(bufs[1], V3, j), src, moms, what, tau, t,
+                             fp32=True)
+            errs.append((tau, e))
+        del out, bufs
+    ctx.close()
+    assert max(e for _, e in errs) < TOL_SPLIT, errs

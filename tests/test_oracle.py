@@ -182,3 +182,82 @@ def test_oracle_second_nucleon_interpolator_matches_reference_build(rng, which, 
     for _ in range(3):
         u, d = rand_site(rng), rand_site(rng)
         assert rel(orc.site(u, d, bit), orc.ref_light(u, d, which)) < 1e-13
+
+
+# ---- mesons and the projection against the reference's own kernels ----------
+# The reference's contract_mesons_device (10 diagonal structures of S1 S1^+
+# and S2 S2^+), contract_mesons_all_device (34 Gamma pairs) and
+# contract_mesons_new_device (10 structures of S1 S2^+), each followed by its
+# in-kernel fourier_transform_3D (source-relative phase, sign -1), compiled
+# from the reference sources as host code and summed over sites as its host
+# driver does.  The lattice is odd and anisotropic and the source is off the
+# origin, so a sign or orientation error in the phase or a transposed Gamma
+# index shows.
+
+def _meson_case(seed, L=(3, 4, 5, 3)):
+    rng = np.random.default_rng(seed)
+    V3 = L[0] * L[1] * L[2]
+    u = rng.standard_normal((144, V3 * L[3])) + 1j * rng.standard_normal((144, V3 * L[3]))
+    d = rng.standard_normal((144, V3 * L[3])) + 1j * rng.standard_normal((144, V3 * L[3]))
+    return L, u, d
+
+
+REF_MESON_KINDS = [(0, DG10), (1, A34), (2, N10)]
+
+
+@pytest.mark.parametrize("kind,bit", REF_MESON_KINDS)
+def test_oracle_mesons_projected_match_reference_kernels(kind, bit):
+    if orc.reference() is None:
+        pytest.skip("reference contraction library not built here")
+    L, u, d = _meson_case(77 + kind)
+    src = (2, 1, 3, 1)
+    moms = np.array(spin.create_mom(3))
+    for j in range(L[3]):
+        tau = (j - src[3]) % L[3]
+        mine, _, _ = orc.twopt(L, u, d, src, moms, bit, [tau])
+        ref = orc.ref_meson_ft(kind, L, u, d, j, src, moms)
+        assert rel(mine[0], ref) < 1e-13, (kind, j)
+
+
+def test_oracle_g16_covers_reference_pairs_projected():
+    """The all-pairs block restricted to the reference's 34 pairs and its 10
+    diagonal structures equals the reference kernels' projected output."""
+    if orc.reference() is None:
+        pytest.skip("reference contraction library not built here")
+    L, u, d = _meson_case(91)
+    src = (1, 3, 0, 2)
+    moms = np.array(spin.create_mom(2))
+    j = 1
+    tau = (j - src[3]) % L[3]
+    g16, _, _ = orc.twopt(L, u, d, src, moms, G16, [tau])
+    g16 = g16[0].reshape(len(moms), 16, 16)
+    a34 = orc.ref_meson_ft(1, L, u, d, j, src, moms)
+    mine = np.concatenate([g16[:, 0, 0:1], g16[:, 5, 5:6], g16[:, 1:5, 1:5].reshape(-1, 16),
+                           g16[:, 6:10, 6:10].reshape(-1, 16)], axis=1)
+    assert rel(mine, a34) < 1e-13
+    n10 = orc.ref_meson_ft(2, L, u, d, j, src, moms)
+    m10 = [0, 5, 1, 2, 3, 4, 6, 7, 8, 9]
+    assert rel(np.stack([g16[:, g, g] for g in m10], axis=1), n10) < 1e-13
+
+
+def test_reference_projection_sign_and_source_phase():
+    """The reference kernel's projection of a field that is nonzero on one
+    site x only is exp(-i p.(x - x0)) times the site value: the sign and the
+    source-relative origin, read off the reference itself."""
+    if orc.reference() is None:
+        pytest.skip("reference contraction library not built here")
+    L, u, d = _meson_case(5)
+    V3 = L[0] * L[1] * L[2]
+    x = (2, 3, 1)
+    sid = x[0] + L[0] * (x[1] + L[1] * x[2])
+    mask = np.zeros(V3 * L[3])
+    mask[sid + V3 * 2] = 1.0
+    u1, d1 = u * mask, d * mask
+    src = (1, 2, 4, 0)
+    moms = np.array(spin.create_mom(2))
+    ref = orc.ref_meson_ft(2, L, u1, d1, 2, src, moms)
+    site_val = orc.ref_meson_ft(2, L, u1, d1, 2, src, [[0, 0, 0]])[0]
+    ph = np.exp(-2j * np.pi * sum(moms[:, i] * (x[i] - src[i]) / L[i] for i in range(3)))
+    assert rel(ref, ph[:, None] * site_val[None, :]) < 1e-13
+    mine, _, _ = orc.twopt(L, u1, d1, src, moms, N10, [2])
+    assert rel(mine[0], ref) < 1e-13

@@ -40,6 +40,38 @@ def test_no_alloc_matches_allocating_projection_twice():
     ctx.close()
 
 
+def test_no_alloc_on_a_spatial_sub_lattice():
+    """A rank holding the second half of x (p2_geom coords (1, 0, 0, 0)): the
+    phase tables must use global coordinates, as p2_ft_apply's do."""
+    ctx = p2.Context((8, 6, 4, 4), procs=(2, 1, 1, 1), coords=(1, 0, 0, 0))
+    rng = np.random.default_rng(78)
+    dof, nt, moms = 5, 4, p2.mom_list(2)
+    f = rng.standard_normal((dof, ctx.V3 * nt)) + 1j * rng.standard_normal((dof, ctx.V3 * nt))
+    fd = torch.from_numpy(f.reshape(-1)).cuda()
+    for _ in range(2):
+        ref, got = _ref_and_noalloc(ctx, fd, dof, nt, moms, -1)
+        assert np.abs(got - ref).max() / np.abs(ref).max() < TOL
+    ctx.close()
+
+
+def test_no_alloc_at_the_scratch_limit():
+    """Partial sums that fill the scratch to within a few kB (one site split
+    fits): accepted, and equal to p2_ft_apply."""
+    ctx = p2.Context((8, 8, 8, 1))
+    moms = p2.mom_list(9)
+    nmom = len(moms)
+    tabs = ((3 * nmom * 4 + 255) // 256 + (3 * nmom * 8 * 16 + 255) // 256) * 256
+    dof = ((32 << 20) - tabs) // (nmom * 16)
+    assert dof * nmom * 16 + tabs <= (32 << 20) < (dof + 1) * nmom * 16 + tabs
+    rng = np.random.default_rng(79)
+    f = (rng.standard_normal((dof, ctx.V3)) + 1j * rng.standard_normal((dof, ctx.V3))).astype(np.complex128)
+    fd = torch.from_numpy(f.reshape(-1)).cuda()
+    ref, got = _ref_and_noalloc(ctx, fd, dof, 1, moms, -1)
+    assert np.all(np.isfinite(got))
+    assert np.abs(got - ref).max() / np.abs(ref).max() < TOL
+    ctx.close()
+
+
 def test_no_alloc_rejects_requests_beyond_the_scratch():
     ctx = p2.Context((4, 4, 4, 8))
     big_dof = (32 << 20) // (8 * 123 * 16) + 1  # nt * nmom * dof * 16 bytes > 32 MiB
