@@ -463,6 +463,8 @@ def main():
                 fl = FP64_FLOP_PER_SITE[kname]
             else:
                 continue
+            if kms[1] <= 0:
+                continue
             ach = fl * sites * args.steps / (kms[1] * 1e-3) / 1e12
             roof64[kname] = {"achieved": ach, "frac": ach / fp64_tflops, "flop_per_site": fl,
                              "flop_kind": "algorithmic" if kname.startswith("project") else "executed (ncu)"}

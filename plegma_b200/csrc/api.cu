@@ -930,7 +930,7 @@ p2_status p2_ft_apply_split(p2_ctx* c, const double* field, int dof, int nt, con
   if (sign != 1 && sign != -1) return c->fail(P2_ERR_INVALID_ARG, "p2_ft_apply_split: sign must be +1 or -1");
   if (out_location != P2_DEVICE && out_location != P2_HOST) return c->fail(P2_ERR_INVALID_ARG, "bad out_location");
   if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
-  if (c->project_split_smem_max < p2::project_split_smem_bytes(144))
+  if (c->project_split_smem_max < p2::project_split_smem_bytes(p2::project_split_max_nt()))
     return c->fail(P2_ERR_UNSUPPORTED, "device shared memory per block too small for the tensor-core projection");
   // exp(+i p.x) = exp(-i (-p).x): the projection's rows carry exp(-i p.x)
   Plan pl;

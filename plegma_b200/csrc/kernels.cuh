@@ -121,7 +121,7 @@ struct SplitGemmArgs {
   const int* cmax;   // [ntau][K] max(|Re|,|Im|) as float bits
   const void* A;     // phase tiles (origin x = 0, shared by all sources)
   int ntau, K, V3, nkstep, nmtile;
-  int NT, ntile;     // components per N-tile (multiple of 16, <= 144), N-tiles
+  int NT, ntile;     // components per N-tile (multiple of 8, <= project_split_max_nt()), N-tiles
   int ks_per_split, nsplit;
   float* part;       // [ntau][nsplit][nmtile][128][ntile * 2 * NT]
   int* err;          // set to 1 if a bounded wait gave up
@@ -163,6 +163,7 @@ cudaError_t launch_build_phases(const PhaseBuildArgs& a, cudaStream_t s);
 cudaError_t launch_project_split(const SplitGemmArgs& a, cudaStream_t s);
 cudaError_t launch_split_reduce(const SplitReduceArgs& a, cudaStream_t s);
 int project_split_smem_bytes(int NT);
+int project_split_max_nt();  // widest N-tile (components) of the tensor-core projection
 
 cudaError_t launch_contract_plain(const ContractArgs& a, int grid, cudaStream_t s);
 // FP32 site contraction; fp32_in selects complex-float propagators.

@@ -176,13 +176,14 @@ p2_status split_prepare_tables(p2_ctx* c, const Plan& pl, unsigned what, int& nm
 p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int nkstep, const SliceDesc* dsl,
                         const int* exps, const int* kexp, const std::vector<ScatterBlock>& blocks, double* out,
                         long long oT, long long oK, const int* kphase) {
-  // projection GEMM candidates (N-tile width NT <= 144 components = 288
-  // TMEM columns, number of N-tiles, site splits, k-steps per split): the
-  // fewest N-tiles at ~2 waves first, then up to two more N-tiles at 1, 2
-  // and 4 waves
+  // projection GEMM candidates (N-tile width NT <= project_split_max_nt()
+  // components, a multiple of 8; number of N-tiles, site splits, k-steps per
+  // split): the fewest N-tiles at ~2 waves first, then up to two more N-tiles
+  // at 1, 2 and 4 waves
   std::vector<std::vector<int>> cands;
-  for (int ntile = (K + 143) / 144, extra = 0; extra < 3; ntile++, extra++) {
-    const int NT = ((K + ntile - 1) / ntile + 15) / 16 * 16;
+  const int maxnt = p2::project_split_max_nt();
+  for (int ntile = (K + maxnt - 1) / maxnt, extra = 0; extra < 3; ntile++, extra++) {
+    const int NT = ((K + ntile - 1) / ntile + 7) / 8 * 8;
     if ((ntile - 1) * NT >= K) continue;  // an empty N-tile
     for (int waves : {2, 1, 4}) {
       const int per = ntile * nmtile * n;
@@ -267,7 +268,7 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
     P2_TRY(c, c->errflag.ensure(16), "error flag alloc");
     P2_TRY(c, cudaMemsetAsync(c->errflag.p, 0, 16, c->stream), "error flag clear");
   }
-  if (c->project_split_smem_max < p2::project_split_smem_bytes(144))
+  if (c->project_split_smem_max < p2::project_split_smem_bytes(p2::project_split_max_nt()))
     return c->fail(P2_ERR_UNSUPPORTED, "device shared memory per block too small for the tensor-core projection");
   const p2_request& r0 = reqs[idx[0]];
   const unsigned what = r0.contractions;

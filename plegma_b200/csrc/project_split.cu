@@ -19,6 +19,16 @@
 // over site splits and the un-scaling are FP64 (k_split_reduce), in a fixed
 // order.
 //
+// Accumulation precision.  Each tensor-core accumulation step D += A B
+// (K = 16) loses about 2^-27 of |D| with a consistent sign (measured on B200:
+// the error of a mean-dominated sum grows linearly with the number of MMAs
+// accumulated into one TMEM tile, 3e-5 of the sum after ~2600 of them), so
+// a k-step range must not accumulate in one TMEM tile.  The products go into
+// one of two TMEM tiles D1a / D1b for kPromote k-steps (48 MMAs, <= ~3e-7),
+// then the converter warps add that tile into an FP32 sum kept in a third
+// TMEM region (CUDA-core adds, round to nearest) while the MMAs fill the
+// other tile.  3 x 2NT TMEM columns: NT <= 80.
+//
 // CTA: 15 converter warps and one copy/MMA warp, one N-tile of NT
 // components (2NT TMEM columns), a range of 64-site k-steps.  Per k-step the
 // converters load c (coalesced along x, 16 bytes per thread and component),
@@ -46,6 +56,8 @@ constexpr int kConvWarps = 15;         // converter warps
 constexpr int kThreads = 512;          // + the copy / MMA warp (16 warps; all 16 run the epilogue)
 constexpr int kKS = 64;                   // sites per k-step
 constexpr int kATile = 128 * kKS * 2;     // bytes of one 128 x 64 FP16 tile
+constexpr int kPromote = 4;               // k-steps accumulated in one TMEM tile before it is added to the sum
+constexpr int kMaxNT = 80;                // 3 x 2NT TMEM columns <= 512
 
 __host__ __device__ constexpr int b_tile_bytes(int NT) { return 2 * NT * kKS * 2; }
 // Stage counts: B (converted operand) stages let the converters run ahead of
@@ -61,8 +73,9 @@ __host__ __device__ constexpr int stage_bytes(int NT, int nb, int na) {
 __host__ __device__ constexpr int b_stages(int NT) { return stage_bytes(NT, 3, 3) <= kSmemMax ? 3 : 2; }
 __host__ __device__ constexpr int a_stages(int NT) { return stage_bytes(NT, b_stages(NT), 3) <= kSmemMax ? 3 : 2; }
 __host__ __device__ constexpr int smem_bytes(int NT) { return stage_bytes(NT, b_stages(NT), a_stages(NT)); }
+// two ping-pong accumulator tiles and the FP32 sum, 2NT columns each
 __host__ __device__ constexpr int tmem_cols(int NT) {
-  return 2 * NT <= 32 ? 32 : 2 * NT <= 64 ? 64 : 2 * NT <= 128 ? 128 : 2 * NT <= 256 ? 256 : 512;
+  return 6 * NT <= 32 ? 32 : 6 * NT <= 64 ? 64 : 6 * NT <= 128 ? 128 : 6 * NT <= 256 ? 256 : 512;
 }
 
 __global__ void k_build_phases(const PhaseBuildArgs a) {
@@ -94,16 +107,46 @@ __global__ void k_build_phases(const PhaseBuildArgs a) {
   }
 }
 
+// Adds accumulator tile D1 (TMEM columns d1col..d1col + NR) into the FP32 sum
+// (columns scol..), or copies it when `first`, for the 32 TMEM lanes of this
+// warp's quarter: 4-column units j, j + nq, j + 2 nq, ... (warp-uniform).
+template <int NR>
+__device__ __forceinline__ void drain_tile(uint32_t tbase, int j, int nq, uint32_t d1col, uint32_t scol, bool first) {
+  constexpr int NU = NR / 4;
+  for (int u0 = j; u0 < NU; u0 += 2 * nq) {
+    uint32_t r[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) r[q] = 0u;
+    const int u1 = u0 + nq;
+    tc::tmem_ld4(tbase + d1col + 4 * u0, r);
+    if (!first) tc::tmem_ld4(tbase + scol + 4 * u0, r + 4);
+    if (u1 < NU) {
+      tc::tmem_ld4(tbase + d1col + 4 * u1, r + 8);
+      if (!first) tc::tmem_ld4(tbase + scol + 4 * u1, r + 12);
+    }
+    tc::tmem_wait_ld16(r);
+    uint32_t o0[4], o1[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      o0[q] = __float_as_uint(__uint_as_float(r[q]) + __uint_as_float(r[4 + q]));
+      o1[q] = __float_as_uint(__uint_as_float(r[8 + q]) + __uint_as_float(r[12 + q]));
+    }
+    tc::tmem_st4(tbase + scol + 4 * u0, o0);
+    if (u1 < NU) tc::tmem_st4(tbase + scol + 4 * u1, o1);
+  }
+  tc::tmem_wait_st();
+}
+
 template <int NT>
 __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmArgs a) {
   constexpr int NR = 2 * NT;                 // B rows (Re, Im per component)
   constexpr int BT = b_tile_bytes(NT);
   constexpr int NA = a_stages(NT);
   constexpr int NB = b_stages(NT);
-  constexpr int NH = NR > 256 ? 2 : 1;       // MMAs per product (N <= 256 each)
-  constexpr int NM = NR / NH;
-  constexpr uint32_t IDESC = tc::idesc_f16_f32(128, NM);
+  static_assert(NT % 8 == 0 && NT <= kMaxNT, "N-tile width");
+  constexpr uint32_t IDESC = tc::idesc_f16_f32(128, NR);
   constexpr int TCOLS = tmem_cols(NT);
+  constexpr int NP = NB > kPromote ? NB : kPromote;  // k-steps per accumulator tile (>= NB: see the drain schedule)
   constexpr int JN = (NT + kConvWarps - 1) / kConvWarps;  // components per converter thread
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // the dynamic window is only guaranteed 16-byte aligned: round up to 1024
@@ -112,7 +155,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
   uint64_t* fullA = (uint64_t*)(sA + NA * 2 * kATile);
   uint64_t* done = fullA + 3;
   uint64_t* fullB = done + 3;
-  uint32_t* tslot = (uint32_t*)(fullB + 3);
+  uint64_t* d1full = fullB + 3;  // accumulator tile b holds its group's complete sum (MMA commit)
+  uint64_t* d1free = d1full + 2;  // accumulator tile b has been added to the sum (converter warps)
+  uint32_t* tslot = (uint32_t*)(d1free + 2);
   int* flag = (int*)(tslot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -131,6 +176,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
     for (int j = 0; j < NB; j++) {
       tc::mbar_init(&done[j], 1);
       tc::mbar_init(&fullB[j], kConvWarps);
+    }
+    for (int j = 0; j < 2; j++) {
+      tc::mbar_init(&d1full[j], 1);
+      tc::mbar_init(&d1free[j], kConvWarps);
     }
     tc::fence_mbar_init();
     *flag = 0;
@@ -166,6 +215,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
           issue_a(next);
         }
         const int s = i % NB;
+        const int grp = i / NP, b = grp & 1;
+        // the first k-step of a group reuses accumulator tile b: the converters
+        // must have added group grp - 2 into the sum
+        if (i % NP == 0 && grp >= 2 && !tc::mbar_wait(&d1free[b], ((grp >> 1) - 1) & 1)) {
+          failed = true;
+          break;
+        }
         if (!tc::mbar_wait(&fullA[i % NA], (i / NA) & 1) || !tc::mbar_wait(&fullB[s], (i / NB) & 1)) {
           failed = true;
           break;
@@ -173,20 +229,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
         tc::tc_fence_after();
         const uint32_t a_hi = tc::smem_u32(sA + (i % NA) * 2 * kATile), a_lo = a_hi + kATile;
         const uint32_t b_hi = tc::smem_u32(smem + s * 2 * BT), b_lo = b_hi + BT;
+        const uint32_t d1 = tmem + (uint32_t)(b * NR);
 #pragma unroll
         for (int kk = 0; kk < kKS / 16; kk++) {
 #pragma unroll
           for (int prod = 0; prod < 3; prod++) {
             const uint32_t aa = (prod == 2 ? a_lo : a_hi) + kk * 32;
             const uint32_t bb = (prod == 1 ? b_lo : b_hi) + kk * 32;
-#pragma unroll
-            for (int h = 0; h < NH; h++) {
-              const uint32_t acc = (i > 0 || kk > 0 || prod > 0) ? 1u : 0u;
-              tc::mma_f16(tmem + h * NM, tc::desc_sw128(aa), tc::desc_sw128(bb + h * (NM / 8) * 1024), IDESC, acc);
-            }
+            const uint32_t acc = (i % NP > 0 || kk > 0 || prod > 0) ? 1u : 0u;
+            tc::mma_f16(d1, tc::desc_sw128(aa), tc::desc_sw128(bb), IDESC, acc);
           }
         }
         tc::mma_commit(&done[s]);
+        if (i % NP == NP - 1 || i == nk - 1) tc::mma_commit(&d1full[b]);
         committed = i;
       }
       // the accumulators are complete (or, after a failure, no MMA or phase
@@ -286,13 +341,42 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
       if (lane == 0) tc::mbar_arrive(&fullB[s]);
       return false;
     };
+    // accumulator tile of group g (k-steps g NP .. g NP + NP - 1) into the
+    // sum: converter warp w serves TMEM lane quarter w % 4 (warp 15, the MMA
+    // warp, leaves quarter 3 to three converter warps)
+    const int quarter = warp & 3, qj = warp >> 2, nq = quarter == 3 ? 3 : 4;
+    const uint32_t tbase = tmem + ((uint32_t)(32 * quarter) << 16);
+    int drained = 0;  // groups added to the sum so far
+    auto drain = [&](int g) -> bool {
+      const int b = g & 1;
+      if (!tc::mbar_wait(&d1full[b], (g >> 1) & 1)) return true;
+      tc::tc_fence_after();
+      drain_tile<NR>(tbase, qj, nq, (uint32_t)(b * NR), (uint32_t)(2 * NR), g == 0);
+      tc::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&d1free[b]);
+      drained = g + 1;
+      return false;
+    };
     if (nk > 0) load_b(ks0, b0);
+    // the drain of group g comes before the converters wait for the MMAs of
+    // k-step (g + 1) NP (converter step (g + 1) NP + NB), which need tile g+1's
+    // predecessor drained; NP >= NB keeps the MMAs of group g + 2 from waiting
+    // on it
+    auto drain_due = [&](int i) -> bool {
+      const int r = i - NB;
+      return r >= NP && r % NP == 0 && drain(r / NP - 1);
+    };
     for (int i = 0; i < nk; i += 2) {
-      if (*(volatile int*)flag || step(i, b0, b1) || (i + 1 < nk && step(i + 1, b1, b0))) {
+      if (*(volatile int*)flag || drain_due(i) || step(i, b0, b1) ||
+          (i + 1 < nk && (drain_due(i + 1) || step(i + 1, b1, b0)))) {
         failed = true;
         break;
       }
     }
+    const int ngroups = (nk + NP - 1) / NP;
+    while (!failed && drained < ngroups)
+      if (drain(drained)) failed = true;
   }
   failed = __syncthreads_or(failed || *(volatile int*)flag);
   if (failed) {
@@ -307,7 +391,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
 #pragma unroll 1
     for (int c = (warp >> 2) * 16; c < NR; c += 64) {
       float v[16];
-      tc::tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c, v);
+      tc::tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(2 * NR + c), v);
       float4* d4 = (float4*)(dst + c);
 #pragma unroll
       for (int q = 0; q < 4; q++) d4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
@@ -381,19 +465,9 @@ cudaError_t launch_nt(const SplitGemmArgs& a, cudaStream_t s) {
 
 }  // namespace
 
-int project_split_smem_bytes(int NT) {
-  switch (NT) {
-    case 16: return smem_bytes(16);
-    case 32: return smem_bytes(32);
-    case 48: return smem_bytes(48);
-    case 64: return smem_bytes(64);
-    case 80: return smem_bytes(80);
-    case 96: return smem_bytes(96);
-    case 112: return smem_bytes(112);
-    case 128: return smem_bytes(128);
-    default: return smem_bytes(144);
-  }
-}
+int project_split_max_nt() { return kMaxNT; }
+
+int project_split_smem_bytes(int NT) { return smem_bytes(NT < 8 ? 8 : NT > kMaxNT ? kMaxNT : (NT + 7) / 8 * 8); }
 
 cudaError_t launch_build_phases(const PhaseBuildArgs& a, cudaStream_t s) {
   const long long n = (long long)a.nmtile * a.nkstep * 128 * kKS;
@@ -403,16 +477,18 @@ cudaError_t launch_build_phases(const PhaseBuildArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_project_split(const SplitGemmArgs& a, cudaStream_t s) {
+  static_assert(kMaxNT == 80, "instantiations below");
   switch (a.NT) {
+    case 8: return launch_nt<8>(a, s);
     case 16: return launch_nt<16>(a, s);
+    case 24: return launch_nt<24>(a, s);
     case 32: return launch_nt<32>(a, s);
+    case 40: return launch_nt<40>(a, s);
     case 48: return launch_nt<48>(a, s);
+    case 56: return launch_nt<56>(a, s);
     case 64: return launch_nt<64>(a, s);
+    case 72: return launch_nt<72>(a, s);
     case 80: return launch_nt<80>(a, s);
-    case 96: return launch_nt<96>(a, s);
-    case 112: return launch_nt<112>(a, s);
-    case 128: return launch_nt<128>(a, s);
-    case 144: return launch_nt<144>(a, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -603,7 +603,7 @@ p2_status p2_contract_udsc(p2_ctx* c, const p2_prop* props, int nprops, const p2
   }
   int nmtile = 0, nkstep = 0;
   if (split) {
-    if (c->project_split_smem_max < project_split_smem_bytes(144))
+    if (c->project_split_smem_max < project_split_smem_bytes(project_split_max_nt()))
       return c->fail(P2_ERR_UNSUPPORTED, "device shared memory per block too small for the tensor-core projection");
     if (!c->errflag.p) {
       P2_TRY(c, c->errflag.ensure(16), "error flag alloc");

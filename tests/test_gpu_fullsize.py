@@ -88,6 +88,7 @@ def test_split_error_metric_configuration_48():
         errs[mode] = np.array(e)
         del out
     ctx.close()
+    print("48^3 x 96 err(t) at taus", taus, {m: e.tolist() for m, e in errs.items()})
     assert errs[p2.P2_SPLIT_FP16].max() < TOL_SPLIT, (taus, errs)
     assert errs[p2.P2_PLAIN_FP64].max() < TOL_PLAIN, (taus, errs)
 
@@ -129,6 +130,7 @@ def test_split_error_batched_configuration_32():
                              tau, t)
             errs.append((i, tau, e))
     ctx.close()
+    print("32^3 x 64 batched err(t)", errs)
     assert max(e for _, _, e in errs) < TOL_SPLIT, errs
 
 
@@ -170,4 +172,57 @@ def test_split_error_large_configuration_64():
             errs.append((tau, e))
         del out, bufs
     ctx.close()
+    print("64^3 x 128 err(t)", errs)
     assert max(e for _, e in errs) < TOL_SPLIT, errs
+
+
+def test_split_error_mean_dominated_sums():
+    """Correlators whose site values all share a sign (the pion Tr[S S^+] >= 0
+    of u = d, and a generic field of mean 1) are the worst case for the
+    tensor-core accumulation, whose rounding loses ~2^-27 of the running sum
+    per step with a consistent sign: a whole slice summed in one TMEM tile
+    was 3e-5 off at 48^3.  The accumulator tiles are added into an FP32 sum
+    every few k-steps, so the error stays well inside the bound at any
+    volume and split count."""
+    L = (48, 48, 48, 16)
+    V3 = L[0] * L[1] * L[2]
+    ctx = p2.Context(L)
+    # generic transform of a mean-1 field, all 16 slices in one launch (long site ranges per CTA)
+    rng = np.random.default_rng(11)
+    moms = p2.mom_list(2)
+    dof, nt = 8, L[3]
+    f = 1.0 + 0.1 * (rng.standard_normal((dof, nt, V3)) + 1j * rng.standard_normal((dof, nt, V3)))
+    fd = torch.from_numpy(f.reshape(-1)).cuda()
+    out = np.zeros(nt * dof * len(moms), dtype=np.complex128)
+    ctx.ft_apply(fd.data_ptr(), dof, nt, moms, -1, out.ctypes.data, p2.P2_HOST, mode=p2.P2_SPLIT_FP16)
+    out = out.reshape(nt, dof, len(moms))
+    x = np.arange(V3)
+    ph = 2 * np.pi * (np.outer(moms[:, 0], x % L[0]) / L[0] + np.outer(moms[:, 1], (x // L[0]) % L[1]) / L[1] +
+                      np.outer(moms[:, 2], x // (L[0] * L[1])) / L[2])
+    E = np.exp(-1j * ph)
+    ferr = 0.0
+    for j in (0, nt - 1):
+        ref = f[:, j, :] @ E.T
+        ferr = max(ferr, float((np.abs(out[j] - ref).max(axis=1) / np.abs(f[:, j, :]).sum(axis=1)).max()))
+    del fd
+    # the pion of u = d in the contraction (component G16[0][0] is |S|^2 at every site)
+    src = (5, 7, 9, 3)
+    (u,) = [torch.empty(144 * V3 * L[3], dtype=torch.complex128, device="cuda")]
+    ctx.synth(u.data_ptr(), True, p2.P2_FP64, 1107, 0, src[3], 0.5)
+    what = p2.NUCLEON_CG5 | p2.MESON_G16
+    mq = p2.mom_list(9)
+    _, total = p2.block_info(what, L[3], len(mq))
+    o = torch.zeros(total, dtype=torch.complex128, device="cuda")
+    props = [ctx.prop(u.data_ptr()), ctx.prop(u.data_ptr())]
+    ctx.contract_project(props, [ctx.request(src, L[3], what, o.data_ptr(), mode=p2.P2_SPLIT_FP16, moms=mq)])
+    ctx.sync()
+    res = p2.result_blocks(what, L[3], len(mq), o.cpu().numpy())
+    perr = []
+    for tau in (0, 1, 8):
+        t = (src[3] + tau) % L[3]
+        us = _slice(u, V3, t)
+        perr.append(_slice_error(L, res, us, us, src, mq, what, tau, t))
+    ctx.close()
+    print("mean-dominated: field err", ferr, "pion (u = d) err(t)", perr)
+    assert ferr < TOL_SPLIT, ferr
+    assert max(perr) < TOL_SPLIT, perr
