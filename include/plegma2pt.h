@@ -345,6 +345,17 @@ p2_status p2_profile_enable(p2_ctx* ctx, int on);
 /* Fills up to max entries, returns the number of kernels seen; reset != 0 clears. */
 int p2_profile_read(p2_ctx* ctx, p2_kernel_time* out, int max, int reset);
 
+/* Test hook for the device-side failure path: the next tensor-core
+ * projection launched on this context (split form, p2_ft_apply_split)
+ * withholds its converters' operand-ready signals and gives every mbarrier
+ * wait a short limit, so its waits run out; the kernel records the timeout,
+ * waits for its own bulk copies, frees its TMEM and returns, and the next
+ * p2_sync (or the synchronising call itself) reports P2_ERR_DEVICE_TIMEOUT.
+ * The context stays usable.  Cleared by that launch.  Nothing faults or hangs:
+ * every wait is bounded.  No counterpart in the reference (it aborts through
+ * PLEGMA_error, include/global/PLEGMA_prints.hpp:49-81). */
+p2_status p2_debug_wait_timeout(p2_ctx* ctx);
+
 /* FP64 FMA rate of the context's device, the roofline denominator of the
  * plain form's FP64 kernels: an FMA loop (8 independent chains per thread,
  * 8 CTAs of 256 threads per SM) timed with CUDA events on the context's

@@ -102,6 +102,7 @@ struct p2_ctx {
   std::vector<int> split_moms_key;  // momentum list the phase tiles and rows were built for
   unsigned split_what_key = 0;      // contraction set of the component exponents
   int project_split_smem_max = 0;  // opt-in shared memory per block of the device
+  int wait_test = 0;               // p2_debug_wait_timeout armed for the next tensor-core projection
   size_t ws_budget = 0;
   // plain form: phase tables and momentum list, rebuilt when the momentum list changes
   p2host::DevBuf ptab;

@@ -125,6 +125,8 @@ struct SplitGemmArgs {
   int ks_per_split, nsplit;
   float* part;       // [ntau][nsplit][nmtile][128][ntile * 2 * NT]
   int* err;          // set to 1 if a bounded wait gave up
+  long long wait_limit;  // polls of every mbarrier wait before it gives up
+  int withhold;      // test hook: the converters never signal their B stages, so the waits run out
 };
 
 struct SplitReduceArgs {

@@ -208,6 +208,7 @@ p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int
   g.nmtile = nmtile;
   g.part = (float*)c->fpart.p;
   g.err = (int*)c->errflag.p;
+  g.wait_limit = 1LL << 24;
   auto set = [&](p2::SplitGemmArgs& q, const std::vector<int>& v) {
     q.NT = v[0];
     q.ntile = v[1];
@@ -227,6 +228,11 @@ p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int
                      pick),
          "projection tuning");
   set(g, pick);
+  if (c->wait_test) {  // p2_debug_wait_timeout: this launch's waits run out (after tuning, which launches normally)
+    g.withhold = 1;
+    g.wait_limit = 1LL << 14;
+    c->wait_test = 0;
+  }
   const int NT = g.NT, nsplit = g.nsplit;
   const int ncols = g.ntile * 2 * NT;
   {
@@ -350,3 +356,10 @@ void precision_release(p2_ctx* c) {
 }
 
 }  // namespace p2
+
+extern "C" p2_status p2_debug_wait_timeout(p2_ctx* c) {
+  if (!c) return P2_ERR_INVALID_ARG;
+  if (c->host_only) return c->fail(P2_ERR_UNSUPPORTED, "host-only context");
+  c->wait_test = 1;
+  return P2_OK;
+}

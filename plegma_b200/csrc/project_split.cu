@@ -188,6 +188,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = *tslot;
+  const long long lim = a.wait_limit;
   const unsigned char* Ab = (const unsigned char*)a.A + (long long)mt * a.nkstep * 2 * kATile;
   bool failed = false;
 
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
         // whose MMAs must be complete
         const int next = i + NA - 2;
         if (next < nk && next > issued) {
-          if (next >= NA && !tc::mbar_wait(&done[(next - NA) % NB], ((next - NA) / NB) & 1)) {
+          if (next >= NA && !tc::mbar_wait(&done[(next - NA) % NB], ((next - NA) / NB) & 1, lim)) {
             failed = true;
             break;
           }
@@ -218,11 +219,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
         const int grp = i / NP, b = grp & 1;
         // the first k-step of a group reuses accumulator tile b: the converters
         // must have added group grp - 2 into the sum
-        if (i % NP == 0 && grp >= 2 && !tc::mbar_wait(&d1free[b], ((grp >> 1) - 1) & 1)) {
+        if (i % NP == 0 && grp >= 2 && !tc::mbar_wait(&d1free[b], ((grp >> 1) - 1) & 1, lim)) {
           failed = true;
           break;
         }
-        if (!tc::mbar_wait(&fullA[i % NA], (i / NA) & 1) || !tc::mbar_wait(&fullB[s], (i / NB) & 1)) {
+        if (!tc::mbar_wait(&fullA[i % NA], (i / NA) & 1, lim) || !tc::mbar_wait(&fullB[s], (i / NB) & 1, lim)) {
           failed = true;
           break;
         }
@@ -246,7 +247,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
       }
       // the accumulators are complete (or, after a failure, no MMA or phase
       // copy is still in flight) before the block moves on
-      if (committed >= 0 && !tc::mbar_wait(&done[committed % NB], (committed / NB) & 1)) failed = true;
+      if (committed >= 0 && !tc::mbar_wait(&done[committed % NB], (committed / NB) & 1, lim)) failed = true;
       if (failed) {
         *flag = 1;
         for (int j = max(0, issued - NA + 1); j <= issued; j++)
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
     auto step = [&](int i, const float4 (&cur)[JN], float4 (&nxt)[JN]) -> bool {
       const int s = i % NB;
       if (i + 1 < nk) load_b(ks0 + i + 1, nxt);
-      if (i >= NB && !tc::mbar_wait(&done[s], ((i / NB) - 1) & 1)) return true;
+      if (i >= NB && !tc::mbar_wait(&done[s], ((i / NB) - 1) & 1, lim)) return true;
       unsigned char* Bh = smem + s * 2 * BT;
       unsigned char* Bl = Bh + BT;
 #pragma unroll
@@ -338,7 +339,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
       }
       tc::fence_proxy_async_smem();
       __syncwarp();
-      if (lane == 0) tc::mbar_arrive(&fullB[s]);
+      if (lane == 0 && !a.withhold) tc::mbar_arrive(&fullB[s]);
       return false;
     };
     // accumulator tile of group g (k-steps g NP .. g NP + NP - 1) into the
@@ -349,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
     int drained = 0;  // groups added to the sum so far
     auto drain = [&](int g) -> bool {
       const int b = g & 1;
-      if (!tc::mbar_wait(&d1full[b], (g >> 1) & 1)) return true;
+      if (!tc::mbar_wait(&d1full[b], (g >> 1) & 1, lim)) return true;
       tc::tc_fence_after();
       drain_tile<NR>(tbase, qj, nq, (uint32_t)(b * NR), (uint32_t)(2 * NR), g == 0);
       tc::tc_fence_before();

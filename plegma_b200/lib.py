@@ -93,7 +93,7 @@ EXPORTS = ["p2_ctx_create", "p2_ctx_destroy", "p2_last_error", "p2_sync", "p2_se
            "p2_synth_propagator", "p2_profile_enable", "p2_profile_read", "p2_alloc", "p2_free", "p2_copy",
            "p2_ft_apply_noalloc", "p2_set_workspace", "p2_graph_create", "p2_graph_launch", "p2_graph_sync",
            "p2_graph_destroy", "p2_tune_enable", "p2_tune_count", "p2_udsc_datasets", "p2_contract_udsc", "p2_local_taus", "p2_prop_transform",
-           "p2_prop_absorb", "p2_ft_apply_split", "p2_measure_fp64_rate"]
+           "p2_prop_absorb", "p2_ft_apply_split", "p2_measure_fp64_rate", "p2_debug_wait_timeout"]
 
 _lib = None
 
@@ -145,6 +145,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.p2_profile_enable.argtypes = [C.c_void_p, C.c_int]
     lib.p2_profile_read.argtypes = [C.c_void_p, C.POINTER(P2KernelTime), C.c_int, C.c_int]
     lib.p2_measure_fp64_rate.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.p2_debug_wait_timeout.argtypes = [C.c_void_p]
     _lib = lib
     return lib
 
@@ -344,6 +345,10 @@ class Context:
         buf = (P2KernelTime * 64)()
         n = self.lib.p2_profile_read(self.h, buf, 64, int(reset))
         return {buf[i].name.decode(): (buf[i].launches, buf[i].ms) for i in range(min(n, 64))}
+
+    def debug_wait_timeout(self):
+        """p2_debug_wait_timeout: the next tensor-core projection's waits run out (test hook)."""
+        self.check(self.lib.p2_debug_wait_timeout(self.h))
 
     def fp64_rate(self):
         """p2_measure_fp64_rate: (TFLOP/s, ms) of the FP64 FMA-loop kernel."""

@@ -52,3 +52,24 @@ def test_workspace_out_of_memory_recovers(mode):
     got, _ = run(ctx, bufs, (3, 1, 2, 2), 8, what, q2max=2, mode=mode)
     assert np.array_equal(got, ref)
     ctx.close()
+
+
+def test_device_wait_timeout_is_reported_and_the_context_recovers():
+    """The tensor-core projection's mbarrier waits are bounded.  With the test
+    hook armed, its converters never signal their operand stages, every wait
+    runs out after a short limit, the kernel drains its own bulk copies, frees
+    its TMEM and returns; the call reports P2_ERR_DEVICE_TIMEOUT, and the next
+    call on the same context gives the same bits as before.  No fault and no
+    hang: the failure is a flag that nothing sets."""
+    ctx = p2.Context((8, 8, 8, 4))
+    src = (1, 2, 3, 1)
+    bufs = device_props(ctx, [(21, 0), (21, 1)], t0=src[3])
+    what = p2.NUCLEON_CG5 | p2.MESON_G16
+    ref, _ = run(ctx, bufs, src, 4, what, q2max=2, mode=p2.P2_SPLIT_FP16)
+    ctx.debug_wait_timeout()
+    with pytest.raises(p2.P2Error) as e:
+        run(ctx, bufs, src, 4, what, q2max=2, mode=p2.P2_SPLIT_FP16)
+    assert e.value.status == p2.P2_ERR_DEVICE_TIMEOUT, e.value
+    got, _ = run(ctx, bufs, src, 4, what, q2max=2, mode=p2.P2_SPLIT_FP16)
+    assert np.array_equal(got, ref)
+    ctx.close()
