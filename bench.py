@@ -210,87 +210,111 @@ TRAFFIC_PER_SITE = {("contract_f32", "split"): 6863, ("contract_plain_fp64", "pl
 FP64_FLOP_PER_SITE = {"contract_plain_fp64": None}
 
 BATCHED = {
-    # name: (lattice, sources, window range, |n|^2 max, propagator precision, decay, seed)
-    "batched_32x64": ((32, 32, 32, 64), 16, (8, 20), 9, "fp64", 0.5, 1004),
-    "batched_64x128": ((64, 64, 64, 128), 4, (32, 32), 16, "fp32", 0.4, 1005),
+    # name: (lattice, sources, window range, |n|^2 max, propagator precision, decay, seed, sources resident at once)
+    "batched_32x64": ((32, 32, 32, 64), 16, (8, 20), 9, "fp64", 0.5, 1004, 16),
+    # every source over all 128 slices: one FP32 source pair is 77 GB, so the
+    # sources are streamed through HBM one at a time (each timed while resident)
+    "batched_64x128": ((64, 64, 64, 128), 4, (128, 128), 16, "fp32", 0.4, 1005, 1),
 }
+BATCH_WORKSPACE = 32 << 30  # position-buffer chunk budget of the batched runs (fewer, larger chunks per graph)
 
 
 def run_batched(name, stream, steps, warmup, forms=("split",)):
-    """Many sources with uneven windows in one recorded CUDA graph per step:
-    nucleon C g5 + Delta C g_k (both isospins) + 16x16 mesons (K = 480).
-    Propagators are stored for each source's window only (t_first = t0,
-    nt = window), so 16 sources x 2 flavours fit in HBM."""
+    """Many sources with uneven windows, each group of resident sources
+    replayed as one recorded CUDA graph per step: nucleon C g5 + Delta C g_k
+    (both isospins) + 16x16 mesons (K = 480).  Propagators are stored for each
+    source's window only (t_first = t0, nt = window).  When the sources do not
+    fit in HBM together they are streamed: each group is generated (untimed),
+    its graph timed over `steps` replays, and a step's time is the sum over
+    the groups."""
     import torch
     from plegma_b200 import lib as p2
-    Lb, nsrc, (wmin, wmax), q2, prec, decay, seed = BATCHED[name]
+    Lb, nsrc, (wmin, wmax), q2, prec, decay, seed, resident = BATCHED[name]
     what = p2.NUCLEON_CG5 | p2.DELTA_ISO12 | p2.DELTA_ISO32 | p2.MESON_G16
     K = p2.components(what)
     moms = p2.mom_list(q2)
     ctx = p2.Context(Lb)
     ctx.set_stream(stream.cuda_stream)
-    ctx.tune(True)
+    free, _ = torch.cuda.mem_get_info()
     V3 = Lb[0] * Lb[1] * Lb[2]
     rng = np.random.default_rng(seed)
     P = p2.P2_FP32 if prec == "fp32" else p2.P2_FP64
     dt = torch.complex64 if prec == "fp32" else torch.complex128
-    srcs, bufs, props = [], [], []
+    esz = 8 if prec == "fp32" else 16
+    srcs = []
     for i in range(nsrc):
         src = tuple(int(rng.integers(0, Lb[dd])) for dd in range(4))
-        W = int(rng.integers(wmin, wmax + 1))
-        for f in range(2):
-            b = torch.empty(144 * V3 * W, dtype=dt, device="cuda")
-            ctx.synth(b.data_ptr(), True, P, seed + i, f, src[3], decay, src[3], W)
-            bufs.append(b)
-            props.append(ctx.prop(b.data_ptr(), P, p2.P2_DEVICE, src[3], W))
-        srcs.append((src, W))
+        srcs.append((src, int(rng.integers(wmin, wmax + 1))))
+    props_bytes = max(2 * 144 * V3 * W * esz for _, W in srcs) * resident
+    ctx.set_workspace(int(min(BATCH_WORKSPACE, max(free - props_bytes - (8 << 30), 1 << 30))))
+    ctx.tune(True)
     sites = sum(W for _, W in srcs) * V3
     res = {"workload": f"{Lb[0]}^3x{Lb[3]}, {nsrc} sources, windows {wmin}-{wmax} (sum {sites // V3} slices), "
                        f"nucleon Cg5 + Delta Cg_k (iso 1/2, 3/2) + 16x16 mesons, K={K}, |n|^2<={q2} "
-                       f"({len(moms)} momenta), {prec} propagators stored per window",
-           "sites_per_step": sites, "launch": "one CUDA graph per step (p2_graph_launch)", "forms": {}}
+                       f"({len(moms)} momenta), {prec} propagators stored per window" +
+                       (f", {resident} source(s) resident at a time" if resident < nsrc else ""),
+           "sites_per_step": sites,
+           "launch": "one CUDA graph per step (p2_graph_launch)" if resident >= nsrc else
+                     f"one CUDA graph per resident group of {resident} source(s), {nsrc // resident} groups per step",
+           "forms": {}}
     for form in forms:
         mode = p2.P2_SPLIT_FP16 if form == "split" else p2.P2_PLAIN_FP64
-        outs, reqs = [], []
-        for i, (src, W) in enumerate(srcs):
-            _, total = p2.block_info(what, W, len(moms))
-            o = torch.zeros(total, dtype=torch.complex128, device="cuda")
-            outs.append(o)
-            reqs.append(ctx.request(src, W, what, o.data_ptr(), mode=mode, moms=moms, prop_u=2 * i,
-                                    prop_d=2 * i + 1))
-        # per-kernel device time from one eager call (graph replays are not split by kernel)
-        ctx.profile(True)
-        ctx.profile_read(reset=True)
-        ctx.contract_project(props, reqs)
-        ctx.sync()
-        prof = ctx.profile_read(reset=True)
-        ctx.profile(False)
-        g = ctx.graph(props, reqs)
-        for _ in range(warmup):
-            g.launch()
-        g.sync()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        with ClockSampler(torch.cuda.current_device()) as clk:
-            ev0.record(stream)
-            for _ in range(steps):
+        ms_total, prof_tot, clocks, launches = 0.0, {}, [], 0
+        for g0 in range(0, nsrc, resident):
+            group = srcs[g0:g0 + resident]
+            bufs, props, outs, reqs = [], [], [], []
+            for i, (src, W) in enumerate(group):
+                for f in range(2):
+                    b = torch.empty(144 * V3 * W, dtype=dt, device="cuda")
+                    ctx.synth(b.data_ptr(), True, P, seed + g0 + i, f, src[3], decay, src[3], W)
+                    bufs.append(b)
+                    props.append(ctx.prop(b.data_ptr(), P, p2.P2_DEVICE, src[3], W))
+                _, total = p2.block_info(what, W, len(moms))
+                o = torch.zeros(total, dtype=torch.complex128, device="cuda")
+                outs.append(o)
+                reqs.append(ctx.request(src, W, what, o.data_ptr(), mode=mode, moms=moms, prop_u=2 * i,
+                                        prop_d=2 * i + 1))
+            # per-kernel device time from one eager call (graph replays are not split by kernel)
+            ctx.profile(True)
+            ctx.profile_read(reset=True)
+            ctx.contract_project(props, reqs)
+            ctx.sync()
+            prof = ctx.profile_read(reset=True)
+            ctx.profile(False)
+            for k, v in prof.items():
+                a = prof_tot.setdefault(k, [0, 0.0])
+                a[0] += v[0]
+                a[1] += v[1]
+            g = ctx.graph(props, reqs)
+            for _ in range(warmup):
                 g.launch()
-            ev1.record(stream)
-            torch.cuda.synchronize()
-        g.sync()
-        ms = ev0.elapsed_time(ev1) / steps
-        tot = sum(v[1] for v in prof.values()) or 1.0
-        res["forms"][form] = {"ms_per_step": ms, "sites_per_s": sites / (ms * 1e-3), "steps": steps,
+            g.sync()
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            with ClockSampler(torch.cuda.current_device()) as clk:
+                ev0.record(stream)
+                for _ in range(steps):
+                    g.launch()
+                ev1.record(stream)
+                torch.cuda.synchronize()
+            g.sync()
+            ms_total += ev0.elapsed_time(ev1) / steps
+            clocks.append(clk.summary())
+            launches += sum(v[0] for v in prof.values())
+            g.close()
+            del outs, bufs
+            torch.cuda.empty_cache()
+        tot = sum(v[1] for v in prof_tot.values()) or 1.0
+        sm = [c["sm_mhz"] for c in clocks if c.get("sm_mhz")]
+        res["forms"][form] = {"ms_per_step": ms_total, "sites_per_s": sites / (ms_total * 1e-3), "steps": steps,
                               "kernels": {k: {"launches": v[0], "ms": v[1], "share": v[1] / tot}
-                                          for k, v in prof.items()},
-                              "gpu_launches_per_step": sum(v[0] for v in prof.values()),
-                              "clocks": clk.summary()}
-        g.close()
-        del outs
+                                          for k, v in prof_tot.items() if v[0]},
+                              "gpu_launches_per_step": launches,
+                              "clocks": {"sm_mhz": statistics.median(sm) if sm else None,
+                                         "reasons": sorted({r for c in clocks for r in c.get("reasons", [])})}}
     res["tuned_shapes"] = ctx.tune_count()
     res["seed"] = seed
     ctx.close()
-    del bufs
     torch.cuda.empty_cache()
     return res
 

@@ -25,8 +25,10 @@
 //  - half-warp h contracts site h of the tile (site_contract.cuh);
 //  - split form: the tile is converted once into padded FP32 rows (component-
 //    major staging, one buffer), and the 16 x 16 meson outputs go back through
-//    the sites' rows to a tile-wide flush that writes 128-byte component rows
-//    (and, when nothing else needs the lanes' sink stage, forms it).
+//    the sites' rows to a tile-wide flush that writes 128-byte component rows;
+//    when nothing else needs the lanes' Gamma stages (g16_raw) the outputs are
+//    the colour-traced products M themselves and the Gamma sums run after the
+//    projection.
 #include "kernels.cuh"
 #include "launch_util.h"
 #include "site_contract.cuh"
@@ -91,9 +93,9 @@ __device__ __forceinline__ int* smax_slot(Cx<float>* sf, int k) {
 
 // Split form, 16 x 16 mesons: a half-warp reads only its own site's FP32 row,
 // so once its contraction is done it stages the site's 256 outputs in that
-// row (C[g1][g2] of lane g1, or with the flush's sink stage the value of lane
-// l before it, in the slot of g1 = l), output j = 16 g2 + g1 at complex
-// 10 (j >> 3) + (j & 7): the four data
+// row (C[g1][g2] of lane g1, or with g16_raw the products M_{a d}[b][z] of lane
+// l = 4 a + d in the slot of g1 = l, g2 = 4 b + z), output j = 16 g2 + g1 at
+// complex 10 (j >> 3) + (j & 7): the four data
 // units of every block (the colour-8 and spare slots keep their contents, the
 // spare slots holding the per-component maxima).  The flush after the tile
 // writes them to HBM, 128 contiguous bytes per component; direct stores from
@@ -162,19 +164,28 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
     w.put_slot(a.k.nuc + 16 + l, pn[1], 1);
   }
   const int g1 = lt.meson_g1();  // the sink Gamma of this lane's meson outputs
-  if (a.what & (8u | 16u | 32u)) {
+  if (w.g16 && g16_raw(a.what)) {
+    // the colour-traced products M_{al de}[b][z] of lane (al, de): no Gamma
+    // stage here, k_meson_gamma forms the Gamma sums after the projection
+    Cx<R> M[4][4];
+    meson_M(row, kU, kD, l >> 2, l & 3, M);
+    __syncwarp(mask);  // every lane of the half-warp has finished reading the row
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+#pragma unroll
+      for (int z = 0; z < 4; z++) w.g16[g16_slot(l, 4 * b + z)] = M[b][z];
+  } else if (a.what & (8u | 16u | 32u)) {
     Cx<R> c[16];
     // staged 16 x 16 outputs leave their unit phases r_g1 r_g2 to the
     // projection's reduction (g16_phase_deferred); the other blocks get them here
     const bool phased = w.g16 == nullptr;
-    const bool sink = !(w.g16 && g16_flush_wht(a.what));  // else the flush forms the sink stage
-    meson_site(row, kU, kD, lt, l, mask, sink, phased, c);
+    meson_site(row, kU, kD, lt, l, mask, true, phased, c);
     auto val = [&](int g2) { return phased ? c[g2] : meson_phase(lt, g2, c[g2]); };
     if (a.what & 8u) {
       if (w.g16) {
         __syncwarp(mask);  // every lane of the half-warp has finished reading the row
 #pragma unroll
-        for (int g2 = 0; g2 < 16; g2++) w.g16[g16_slot(sink ? g1 : l, g2)] = c[g2];
+        for (int g2 = 0; g2 < 16; g2++) w.g16[g16_slot(g1, g2)] = c[g2];
       } else {  // direct stores (plain form, or split form with the 10 diagonal structures: maxima in shared memory)
 #pragma unroll
         for (int g2 = 0; g2 < 16; g2++) w.put(a.k.g16 + g1 * 16 + g2, c[g2]);
@@ -278,7 +289,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
   // 16 x 16 meson outputs staged in the sites' own FP32 rows (not with the
   // 10 diagonal structures, whose second pass reads the rows again)
   const bool stage = !DELTA && g16_phase_deferred(a.what);
-  const bool fwht = stage && g16_flush_wht(a.what);  // the flush forms the sink Gamma stage
   const int tid = threadIdx.x;
   const int hw = tid >> 4, l = tid & 15;
   const unsigned mask = halfwarp_mask();
@@ -292,9 +302,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
 
   int cur = -1;  // slice whose maxima the spare slots hold
   // running maxima in registers: nucleon outputs of lane l (slots 0, 1) and
-  // the staged meson outputs this thread writes out (slots 2 + g2, or
-  // 2 + 4 u + j with the flush's sink stage); the Delta instantiation tracks
-  // its maxima in shared memory only
+  // the staged meson outputs this thread writes out (slots 2 + g2); the
+  // Delta instantiation tracks its maxima in shared memory only
   constexpr int kSlots = DELTA ? 1 : 18;
   float rmax[kSlots];
 #pragma unroll
@@ -309,8 +318,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
         rmax[i] = 0.f;
         if (!(tid & 16) && (a.what & 1u)) atomicMax(smax_slot(sf, a.k.nuc + 16 * i + l), __float_as_int(m));
       }
-      // mesons: the 16 threads of half-warp hw hold components g16 + 16 g1 + g2
-      // (g1 = hw; with the flush's sink stage g1 = flush[hw >> 2][u], g2 = 4 (hw & 3) + j)
+      // mesons: the 16 threads of half-warp hw hold components g16 + 16 hw + g2
 #pragma unroll
       for (int i = 2; i < kSlots; i++) {
         float m = rmax[i];
@@ -319,8 +327,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
         m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 4));
         m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 8));
         rmax[i] = 0.f;
-        const int k = fwht ? a.k.g16 + 16 * c_meson_flush[hw >> 2][(i - 2) >> 2][0] + 4 * (hw & 3) + ((i - 2) & 3)
-                           : a.k.g16 + 16 * hw + (i - 2);
+        const int k = a.k.g16 + 16 * hw + (i - 2);
         if (l == 0 && stage) atomicMax(smax_slot(sf, k), __float_as_int(m));
       }
     }
@@ -393,35 +400,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
         // thread (site s = tid & 15, g1 = tid >> 4): components g16 + 16 g1 + g2,
         // each a 128-byte row segment over the tile's 16 sites
         const int s = tid & 15;
-        if (x0 + s < a.V3 && fwht) {
-          // thread (site s, class m = hw >> 2, g2 = 4 (hw & 3) + j): the canonical
-          // 4-point transform over the lanes m ^ 5 t0 ^ 10 t1 of the class; output
-          // u is component g1 = flush[m][u] (sign and phases in the reduction)
-          const int m = hw >> 2;
-          const Cx<float>* srow = sf + s * kRow32;
-          int base[4], g1u[4];
-#pragma unroll
-          for (int t = 0; t < 4; t++) {
-            const int ln = m ^ (5 * (t & 1)) ^ (10 * (t >> 1));
-            base[t] = 10 * (ln >> 3) + (ln & 7);  // g16_slot(ln, g2) - 20 g2
-            g1u[t] = c_meson_flush[m][t][0];
-          }
-          Cx<float>* o = (Cx<float>*)a.out + ((long long)tl * a.K + a.k.g16 + 4 * (hw & 3)) * a.V3 + x0 + s;
-#pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const int g2 = 4 * (hw & 3) + j;
-            Cx<float> x[4];
-#pragma unroll
-            for (int t = 0; t < 4; t++) x[t] = srow[base[t] + 20 * g2];
-            const Cx<float> a0 = x[0] + x[1], a1 = x[0] - x[1], a2 = x[2] + x[3], a3 = x[2] - x[3];
-            const Cx<float> y[4] = {a0 + a2, a1 + a3, a0 - a2, a1 - a3};
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-              o[(long long)(16 * g1u[u] + j) * a.V3] = y[u];
-              rmax[2 + 4 * u + j] = fmaxf(rmax[2 + 4 * u + j], fmaxf(fabsf(y[u].x), fabsf(y[u].y)));
-            }
-          }
-        } else if (x0 + s < a.V3) {
+        if (x0 + s < a.V3) {
           Cx<float>* o = (Cx<float>*)a.out + ((long long)tl * a.K + a.k.g16 + 16 * hw) * a.V3 + x0 + s;
 #pragma unroll
           for (int g2 = 0; g2 < 16; g2++) {

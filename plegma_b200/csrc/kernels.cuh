@@ -14,10 +14,13 @@ constexpr int kMaxBlocks = 10;  // contraction blocks of a request (one per P2_*
 // whenever the 16 x 16 block is requested without the 10 diagonal structures.
 __host__ __device__ constexpr bool g16_phase_deferred(unsigned what) { return (what & 8u) && !(what & 64u); }
 // ... and, when neither the 34 pairs nor the 10 diagonal structures of the
-// same lanes are requested, the sink Gamma stage as well: the lanes stage
-// their values before the butterflies and the tile flush forms the 4-point
-// transforms (signs sigma of the flush table folded into the phases).
-__host__ __device__ constexpr bool g16_flush_wht(unsigned what) {
+// same lanes are requested, no Gamma stage at all: the Gamma sums are linear
+// and commute with the momentum projection, so the split contraction writes
+// the 256 colour-traced products M_{a d}[b][z] = sum_colour u[a][b] conj(d[d][z])
+// as the block's components (component 16 (4 a + d) + 4 b + z) and
+// k_meson_gamma forms C[g1][g2] = sum G1[d][pi1(d)] G2[b][pi2(b)]
+// M_{pi1(d) d}[b][pi2(b)] from their projections, per slice and momentum.
+__host__ __device__ constexpr bool g16_raw(unsigned what) {
   return g16_phase_deferred(what) && !(what & (16u | 32u));
 }
 
@@ -164,6 +167,17 @@ cudaError_t launch_field_to_f32(const FieldF32Args& a, int nsm, cudaStream_t s);
 cudaError_t launch_build_phases(const PhaseBuildArgs& a, cudaStream_t s);
 cudaError_t launch_project_split(const SplitGemmArgs& a, cudaStream_t s);
 cudaError_t launch_split_reduce(const SplitReduceArgs& a, cudaStream_t s);
+
+// The 16 x 16 meson Gamma sums applied in place to the projected colour
+// products of g16_raw requests: for every slice and momentum, the block's 256
+// values M are replaced by C.  Result location as SplitReduceArgs (block
+// layout: blk is the 16 x 16 block).
+struct MesonGammaArgs {
+  const SliceDesc* sl;
+  int ntau, nmom;
+  ScatterBlock blk;
+};
+cudaError_t launch_meson_gamma(const MesonGammaArgs& a, cudaStream_t s);
 int project_split_smem_bytes(int NT);
 int project_split_max_nt();  // widest N-tile (components) of the tensor-core projection
 

@@ -96,14 +96,6 @@ constexpr int gamma_phase_q(int g) {
   return kGammaRe[g][0] == 1 ? 0 : kGammaIm[g][0] == 1 ? 1 : kGammaRe[g][0] == -1 ? 2 : 3;
 }
 constexpr int meson_phase_q(int g1, int g2) { return (gamma_phase_q(g1) + gamma_phase_q(g2)) & 3; }
-// Sign sigma of g1's output in the flush form of the sink Gamma stage.
-constexpr int meson_flush_sign(int g1) {
-  for (int m = 0; m < 4; m++)
-    for (int u = 0; u < 4; u++)
-      if (kMesonFlush[m][u][0] == g1) return kMesonFlush[m][u][1];
-  return 0;
-}
-
 // Packed float pairs for the paired FP32 FMA (fma.rn.f32x2): one instruction
 // updates both halves of a register pair.
 typedef unsigned long long f32x2;

@@ -151,16 +151,16 @@ p2_status split_prepare_tables(p2_ctx* c, const Plan& pl, unsigned what, int& nm
   }
   if (what && c->split_what_key != what) {
     // [K][2] scale powers, then [K] unit phases i^q of the 16 x 16 mesons
-    // that the contraction leaves out (g16_phase_deferred)
+    // that the contraction leaves out (g16_phase_deferred; with g16_raw the
+    // components are colour products and the Gamma sums, phases included,
+    // come after the reduction)
     std::vector<int> ke = component_exponents(what);
     const int K = (int)ke.size() / 2;
     ke.resize(3 * (size_t)K, 0);
-    if (g16_phase_deferred(what)) {
+    if (g16_phase_deferred(what) && !g16_raw(what)) {
       const int k0 = offsets_of(what).g16;
       for (int g1 = 0; g1 < 16; g1++)
-        for (int g2 = 0; g2 < 16; g2++)
-          ke[2 * K + k0 + 16 * g1 + g2] =
-              (meson_phase_q(g1, g2) + (g16_flush_wht(what) && meson_flush_sign(g1) < 0 ? 2 : 0)) & 3;
+        for (int g2 = 0; g2 < 16; g2++) ke[2 * K + k0 + 16 * g1 + g2] = meson_phase_q(g1, g2);
     }
     if ((st = upload_async(c, c->kexp, ke.data(), ke.size() * sizeof(int), "component exponents")) != P2_OK) return st;
     c->split_what_key = what;
@@ -344,6 +344,22 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
     if ((st = split_project(c, pl, K, n, nmtile, nkstep, dsl, (const int*)c->expb.p, kexp, pl.blocks, nullptr, 0,
                             0, g16_phase_deferred(what) ? kexp + 2 * K : nullptr)) != P2_OK)
       return st;
+    if (g16_raw(what)) {
+      // the Gamma sums of the 16 x 16 block on its projected colour products
+      p2::MesonGammaArgs mg{};
+      mg.sl = dsl;
+      mg.ntau = n;
+      mg.nmom = pl.nmom;
+      bool found = false;
+      for (const auto& b : pl.blocks)
+        if (b.comps == 256) {
+          mg.blk = b;
+          found = true;
+        }
+      if (!found) return c->fail(P2_ERR_INVALID_ARG, "16 x 16 meson block missing from the plan");
+      ProfScope ps(c, "meson_gamma");
+      P2_TRY(c, p2::launch_meson_gamma(mg, c->stream), "meson Gamma sums");
+    }
   }
   return P2_OK;
 }

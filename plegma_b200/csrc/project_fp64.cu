@@ -8,7 +8,8 @@
 // phase tables (p.x = sum_d n_d x_d), built on the host in double precision.
 //
 // CTA tile 64 momenta x (16*TK) components, 256 threads, each thread a
-// 4 x TK register tile; sites are consumed 16 at a time from shared memory.
+// 4 x TK register tile; sites are consumed 16 at a time from shared memory,
+// the next 16 sites' global loads in flight meanwhile.
 // The site range of a slice is split over `nsplit` CTAs whose partial sums
 // go to `part`; k_scatter adds them in a fixed order (bitwise reproducible)
 // and writes the result layout.
@@ -24,11 +25,19 @@ constexpr int kXS = 16;  // sites per step
 constexpr int kTP = 4;   // momenta per thread
 constexpr int kPT = 16 * kTP;
 
+// Shared-memory tiles of one 16-site step: phases sE[site][momentum] and
+// site values sC[component][site ^ (component & 15)] (component-major like
+// the global buffer, the site index XOR-swizzled so that the transposing
+// store and the per-component reads of a quarter-warp both touch 8
+// different 16-byte bank groups).  The next step's global loads are issued
+// into registers before the current step's products (software pipeline).
 template <int TK>
 __global__ void __launch_bounds__(kThreads, 1) k_project_fp64(const ProjArgs a) {
   constexpr int KT = 16 * TK;
+  constexpr int NE = (kXS * kPT) / kThreads;  // phase entries per thread per step
+  constexpr int NC = (kXS * KT) / kThreads;   // site values per thread per step
   __shared__ Cx<double> sE[kXS][kPT];
-  __shared__ Cx<double> sC[kXS][KT];
+  __shared__ Cx<double> sC[KT][kXS];
   const int tid = threadIdx.x;
   const int tp = tid >> 4, tk = tid & 15;
   const int ktiles = (a.K + KT - 1) / KT;
@@ -48,41 +57,61 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_fp64(const ProjArgs a) 
 #pragma unroll
     for (int j = 0; j < TK; j++) acc[i][j] = czero<double>();
 
-  for (int xs0 = xb; xs0 < xe; xs0 += kXS) {
-    // phases for 16 sites x 64 momenta
+  // this thread's loads of a step: phase entries (xs = e / kPT, pp = e % kPT)
+  // as three per-dimension factors, site values (xs = e % kXS, kk = e / kXS);
+  // the widest tile (TK = 8) has no registers to spare: it loads each step
+  // at the step's start instead
+  constexpr bool kPrefetch = TK <= 6;
+  Cx<double> fx[NE], fy[NE], fz[NE], cv_next[NC];
+  auto load_phases = [&](int xs0) {
 #pragma unroll
-    for (int r = 0; r < (kXS * kPT) / kThreads; r++) {
+    for (int r = 0; r < NE; r++) {
       const int e = tid + r * kThreads;
       const int xs = e / kPT, pp = e % kPT;
       const int p = p0 + pp, x = xs0 + xs;
-      Cx<double> v = czero<double>();
+      fx[r] = fy[r] = fz[r] = czero<double>();
       if (p < a.nmom && x < xe) {
         const int xx = x % a.Lx, yy = (x / a.Lx) % a.Ly, zz = x / LxLy;
-        const Cx<double> ex = tab[(0 * a.nmom + p) * a.Lmax + xx];
-        const Cx<double> ey = tab[(1 * a.nmom + p) * a.Lmax + yy];
-        const Cx<double> ez = tab[(2 * a.nmom + p) * a.Lmax + zz];
-        v = cmul(cmul(ex, ey), ez);
+        fx[r] = tab[(0 * a.nmom + p) * a.Lmax + xx];
+        fy[r] = tab[(1 * a.nmom + p) * a.Lmax + yy];
+        fz[r] = tab[(2 * a.nmom + p) * a.Lmax + zz];
       }
-      sE[xs][pp] = v;
     }
-    // site values for 16 sites x KT components (coalesced along x)
+  };
+  auto load_step = [&](int xs0) {
+    load_phases(xs0);
 #pragma unroll
-    for (int r = 0; r < (kXS * KT) / kThreads; r++) {
+    for (int r = 0; r < NC; r++) {
       const int e = tid + r * kThreads;
       const int xs = e % kXS, kk = e / kXS;
       const int k = k0 + kk, x = xs0 + xs;
-      Cx<double> v = czero<double>();
-      if (k < a.K && x < xe) v = c[(long long)k * a.sK + x];
-      sC[xs][kk] = v;
+      cv_next[r] = czero<double>();
+      if (k < a.K && x < xe) cv_next[r] = c[(long long)k * a.sK + x];
+    }
+  };
+  if (kPrefetch && xb < xe) load_step(xb);
+  for (int xs0 = xb; xs0 < xe; xs0 += kXS) {
+    if (!kPrefetch) load_step(xs0);
+#pragma unroll
+    for (int r = 0; r < NE; r++) {
+      const int e = tid + r * kThreads;
+      sE[e / kPT][e % kPT] = cmul(cmul(fx[r], fy[r]), fz[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < NC; r++) {
+      const int e = tid + r * kThreads;
+      const int xs = e % kXS, kk = e / kXS;
+      sC[kk][xs ^ (kk & 15)] = cv_next[r];
     }
     __syncthreads();
+    if (kPrefetch && xs0 + kXS < xe) load_step(xs0 + kXS);  // in flight during the products
 #pragma unroll 4
     for (int xs = 0; xs < kXS; xs++) {
       Cx<double> ev[kTP], cv[TK];
 #pragma unroll
       for (int i = 0; i < kTP; i++) ev[i] = sE[xs][tp + 16 * i];
 #pragma unroll
-      for (int j = 0; j < TK; j++) cv[j] = sC[xs][tk + 16 * j];
+      for (int j = 0; j < TK; j++) cv[j] = sC[tk + 16 * j][xs ^ tk];  // (tk + 16 j) & 15 == tk
 #pragma unroll
       for (int i = 0; i < kTP; i++)
 #pragma unroll

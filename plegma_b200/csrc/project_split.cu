@@ -56,7 +56,10 @@ constexpr int kConvWarps = 15;         // converter warps
 constexpr int kThreads = 512;          // + the copy / MMA warp (16 warps; all 16 run the epilogue)
 constexpr int kKS = 64;                   // sites per k-step
 constexpr int kATile = 128 * kKS * 2;     // bytes of one 128 x 64 FP16 tile
-constexpr int kPromote = 4;               // k-steps accumulated in one TMEM tile before it is added to the sum
+#ifndef P2_PROMOTE_KSTEPS
+#define P2_PROMOTE_KSTEPS 4
+#endif
+constexpr int kPromote = P2_PROMOTE_KSTEPS;  // k-steps accumulated in one TMEM tile before it is added to the sum
 constexpr int kMaxNT = 80;                // 3 x 2NT TMEM columns <= 512
 
 __host__ __device__ constexpr int b_tile_bytes(int NT) { return 2 * NT * kKS * 2; }
@@ -196,10 +199,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
     // ---- copy / MMA warp: lane 0 ----
     if (lane == 0 && nk > 0) {
       int issued = -1, committed = -1;
+      // the phase tiles are re-read by every N-tile, slice and site split:
+      // they stay in L2 ahead of the position buffer streamed past them
+      const uint64_t keep_policy = tc::policy_evict_last();
       auto issue_a = [&](int i) {  // phase tiles of k-step i into A stage i % NA
         const int sa = i % NA;
         tc::mbar_expect_tx(&fullA[sa], 2 * kATile);
-        tc::bulk_g2s(sA + sa * 2 * kATile, Ab + (long long)(ks0 + i) * 2 * kATile, 2 * kATile, &fullA[sa]);
+        tc::bulk_g2s_hint(sA + sa * 2 * kATile, Ab + (long long)(ks0 + i) * 2 * kATile, 2 * kATile, &fullA[sa],
+                          keep_policy);
         issued = i;
       };
       issue_a(0);
@@ -291,6 +298,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
       if (kg + kConvWarps * j < NT && k0 + kg + kConvWarps * j < a.K) jok |= 1u << j;
     const Cx<float>* cthr = cb + (long long)(k0 + kg) * a.V3 + 2 * sp;
     const long long cstride = (long long)kConvWarps * a.V3;
+    const uint64_t stream_policy = tc::policy_evict_first();  // the position buffer is read once
     auto load_b = [&](int ks, float4 (&r)[JN]) {
       const long long x = (long long)ks * kKS + 2 * sp;
       const Cx<float>* cks = cthr + (long long)ks * kKS;
@@ -300,7 +308,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
         if (((jok >> j) & 1u) && x < a.V3) {
           const Cx<float>* src = cks + j * cstride;
           if (even) {
-            r[j] = *reinterpret_cast<const float4*>(src);
+            r[j] = tc::ld_stream_f4(src, stream_policy);
           } else {
             r[j].x = src[0].x;
             r[j].y = src[0].y;
@@ -454,6 +462,38 @@ __global__ void k_split_reduce(const SplitReduceArgs a) {
   }
 }
 
+// C[g1][g2] = sum_{d, b} G1[d][pi1(d)] G2[b][pi2(b)] M_{pi1(d) d}[b][pi2(b)]
+// (PLEGMA_mesonsAll.cuh:58-76 with the spin sums moved after the projection:
+// the Gamma sums are linear).  One block per (momentum, slice): the 256
+// projected colour products of the 16 x 16 block are read into shared memory
+// and replaced in place by the 256 C[g1][g2], component 16 g1 + g2.
+__constant__ int c_gperm[16][4] = P2_INIT_GammaPerm;
+__constant__ int c_gre[16][4] = P2_INIT_GammaRe;
+__constant__ int c_gim[16][4] = P2_INIT_GammaIm;
+
+__global__ void __launch_bounds__(256) k_meson_gamma(const MesonGammaArgs a) {
+  __shared__ Cx<double> sm[256];
+  const int p = blockIdx.x, tl = blockIdx.y, j = threadIdx.x;
+  const SliceDesc& sd = a.sl[tl];
+  Cx<double>* v = (Cx<double>*)sd.out + a.blk.base * sd.totalT * a.nmom + ((long long)sd.tau * a.nmom + p) * 256;
+  sm[j] = v[j];
+  __syncthreads();
+  const int g1 = j >> 4, g2 = j & 15;
+  Cx<double> acc = czero<double>();
+#pragma unroll
+  for (int d = 0; d < 4; d++) {
+    const int al = c_gperm[g1][d];
+    const Cx<double> v1 = cx<double>((double)c_gre[g1][d], (double)c_gim[g1][d]);
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int z = c_gperm[g2][b];
+      const Cx<double> v2 = cx<double>((double)c_gre[g2][b], (double)c_gim[g2][b]);
+      cmac(acc, cmul(v1, v2), sm[16 * (4 * al + d) + 4 * b + z]);
+    }
+  }
+  v[j] = acc;
+}
+
 template <int NT>
 cudaError_t launch_nt(const SplitGemmArgs& a, cudaStream_t s) {
   const int smem = smem_bytes(NT);
@@ -577,6 +617,12 @@ cudaError_t launch_field_to_f32(const FieldF32Args& a, int nsm, cudaStream_t s) 
   k_field_exponent<<<grid, 256, 0, s>>>(a, xchunk);
   k_field_exps_zero<<<tb, 256, 0, s>>>(a.exps, a.ntau);
   k_field_to_f32<<<grid, 256, 0, s>>>(a, xchunk);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_meson_gamma(const MesonGammaArgs& a, cudaStream_t s) {
+  if (a.ntau < 1 || a.nmom < 1) return cudaSuccess;
+  k_meson_gamma<<<dim3(a.nmom, a.ntau), 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

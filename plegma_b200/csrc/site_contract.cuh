@@ -66,7 +66,6 @@ struct LaneTables {
 __constant__ int c_nuc_lane[16][8] = P2_INIT_NucLane;
 __constant__ int c_delta_lane[3][16][8] = P2_INIT_DeltaLane;
 __constant__ int c_meson_lane[16][3] = P2_INIT_MesonLane;
-__constant__ int c_meson_flush[4][4][2] = P2_INIT_MesonFlush;
 __constant__ int c_light_lane[3][16][8] = P2_INIT_LightLane;
 __constant__ int c_light_g5[16][3] = P2_INIT_LightG5;
 
@@ -643,8 +642,7 @@ __device__ __forceinline__ Cx<R> meson_phase(const LaneTables& lt, int g2, Cx<R>
 // Generic meson block of the lines A and B (block offsets): the lane gets
 // C[g1][g2] for g2 = 0..15 in out[], g1 = lt.meson_g1() (a permutation of the
 // lanes), times conj(r_g1 r_g2) when phased is false; with sink false the
-// lane keeps its values before the sink stage (the tile flush forms it,
-// spin.meson_flush_table).  Lane (al, de) first
+// lane keeps its values before the sink stage.  Lane (al, de) first
 // forms, per source class m2, the Walsh-Hadamard transform over b of
 // M[b][b ^ m2] (N[g2] / r_g2 at index s_g2); the sink Gamma then runs as a
 // Walsh-Hadamard transform over the 4 lanes of the lane's class (two

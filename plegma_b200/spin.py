@@ -349,39 +349,6 @@ def meson_lane_table():
     return lanes
 
 
-def meson_flush_table():
-    """Sink-Gamma stage of the staged 16 x 16 mesons done in the tile flush:
-    the lanes store their values before the butterflies and a flush thread
-    forms the canonical 4-point transform y_u = sum_t (-1)^{popcount(u & t)}
-    x_t over the lanes m ^ 5 t_0 ^ 10 t_1 of class m.  The butterflies of
-    lane t leave sigma y_u on it (sigma = +-1), so y_u is C[g1][g2] /
-    (sigma r_g1 r_g2) for that lane's g1.  Returns [m][u] = (g1, sigma)."""
-    lanes = meson_lane_table()
-    out = []
-    for m in range(4):
-        L = [m ^ (5 * (t & 1)) ^ (10 * (t >> 1)) for t in range(4)]
-        H = np.zeros((4, 4))
-        for tp in range(4):
-            x = np.zeros(16)
-            x[L[tp]] = 1.0
-            s0 = np.array([-1 if (l & 1) else 1 for l in range(16)])
-            s1 = np.array([-1 if (l & 2) else 1 for l in range(16)])
-            x = s0 * x + x[[l ^ 5 for l in range(16)]]
-            x = s1 * x + x[[l ^ 10 for l in range(16)]]
-            for t in range(4):
-                H[t, tp] = x[L[t]]
-        row = []
-        for u in range(4):
-            yu = np.array([(-1) ** bin(u & t).count("1") for t in range(4)])
-            hit = [(t, sg) for t in range(4) for sg in (1, -1) if np.array_equal(H[t], sg * yu)]
-            assert len(hit) == 1, (m, u)
-            t, sg = hit[0]
-            row.append([lanes[L[t]][0], sg])
-        out.append(row)
-    assert sorted(g for r in out for g, _ in r) == list(range(16))
-    return out
-
-
 def header_text() -> str:
     perms, res, ims = gamma16_tables()
     nuc = nucleon_table()
@@ -402,7 +369,6 @@ def header_text() -> str:
            _c_array("kDeltaSink", "int", [diquark_lane_tables(t)[0] for t in dl]),
            _c_array("kDeltaLane", "int", [diquark_lane_tables(t)[1] for t in dl]),
            _c_array("kMesonLane", "int", meson_lane_table()),
-           _c_array("kMesonFlush", "int", meson_flush_table()),
            _c_array("kNtrIdx", "int", [r[:6] for r in light_nucleon_tables()["NtoR"]]),
            _c_array("kNtrVal", "int", [r[6] for r in light_nucleon_tables()["NtoR"]]),
            _c_array("kRtnIdx", "int", [r[:6] for r in light_nucleon_tables()["RtoN"]]),

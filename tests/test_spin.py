@@ -119,20 +119,6 @@ def test_meson_walsh_stage_matches_direct_sum():
             assert complex(lanes[l][1], lanes[l][2]) == walsh[g1][2]
             emu[g1, g2] = x[l] * (1j) ** ((spin_phase_q(walsh, g1) + spin_phase_q(walsh, g2)) % 4)
     assert np.allclose(emu, direct, atol=1e-12)
-    # the same stage done in the tile flush (spin.meson_flush_table): canonical
-    # transform over the class's lanes, output u to g1 with the sign sigma
-    flush = spin.meson_flush_table()
-    emu2 = np.zeros((16, 16), dtype=complex)
-    for g2 in range(16):
-        m2, s2, _ = walsh[g2]
-        x = np.array([sum(chi(s2, b) * M[l >> 2, l & 3, b, b ^ m2] for b in range(4)) for l in range(16)])
-        for m in range(4):
-            xt = [x[m ^ (5 * (t & 1)) ^ (10 * (t >> 1))] for t in range(4)]
-            for u in range(4):
-                g1, sg = flush[m][u]
-                y = sum(chi(u, t) * xt[t] for t in range(4))
-                emu2[g1, g2] = sg * y * (1j) ** ((spin_phase_q(walsh, g1) + spin_phase_q(walsh, g2)) % 4)
-    assert np.allclose(emu2, direct, atol=1e-12)
 
 
 def spin_phase_q(walsh, g):
