@@ -207,7 +207,7 @@ def run_reference(args, rank, world):
 TRAFFIC_PER_SITE = {("contract_f32", "split"): 6863, ("contract_plain_fp64", "plain"): 9129}
 # executed FP64 flop per site of the plain site contraction (2 per DFMA, 1 per
 # DADD / DMUL, from the ncu instruction counters of the 32^3 x 16 case)
-FP64_FLOP_PER_SITE = {"contract_plain_fp64": None}
+FP64_FLOP_PER_SITE = {"contract_plain_fp64": 55968}
 
 BATCHED = {
     # name: (lattice, sources, window range, |n|^2 max, propagator precision, decay, seed, sources resident at once)
@@ -335,6 +335,9 @@ def main():
                          "(lets a profiler run skip the tuning launches)")
     ap.add_argument("--lattice", default=None,
                     help="Lx,Ly,Lz,Lt override for small profiling cases (not the benchmark workload)")
+    ap.add_argument("--what", default="metric", choices=["metric", "delta"],
+                    help="contraction set of a profiling case: the metric's (nucleon + 16x16 mesons) or the batched "
+                         "configurations' (with both Delta isospins, K = 480)")
     args = ap.parse_args()
     global L
     if args.lattice:
@@ -371,6 +374,10 @@ def main():
     V3 = L[0] * L[1] * L[2]
     sites = V3 * L[3]
     what = p2.NUCLEON_CG5 | p2.MESON_G16
+    if args.what == "delta":
+        if not args.lattice:
+            ap.error("--what delta is a profiling case: give --lattice")
+        what |= p2.DELTA_ISO12 | p2.DELTA_ISO32
     K = p2.components(what)
     moms = p2.mom_list(Q2MAX)
     nmom = len(moms)

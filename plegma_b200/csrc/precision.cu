@@ -297,9 +297,14 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
   p2_status st = split_prepare_tables(c, pl, what, nmtile, nkstep);
   if (st != P2_OK) return st;
 
-  // chunk of slices: FP32 position buffer within the workspace budget
+  // chunk of slices: FP32 position buffer within the workspace budget; a
+  // chunk may hold slices of many requests (a batch of sources), so up to
+  // all of the batch's slices go into one chunk
   const size_t per_slice = (size_t)K * c->V3 * 8;
-  int tc = (int)std::max<size_t>(1, std::min<size_t>(c->ws_budget / std::max<size_t>(per_slice, 1), c->T));
+  size_t nslices = 0;
+  for (int q = 0; q < nidx; q++) nslices += (size_t)std::max(reqs[idx[q]].totalT, 0);
+  int tc = (int)std::max<size_t>(1, std::min<size_t>(c->ws_budget / std::max<size_t>(per_slice, 1),
+                                                   std::max<size_t>(nslices, 1)));
   if (all_host64) tc = std::min(tc, 4);  // short chunks: the host conversion pipeline fills and drains faster
   const Work w = make_work(c, props, reqs, idx, nidx, tc);
   if (w.sl.empty()) return P2_OK;
