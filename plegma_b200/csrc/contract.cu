@@ -347,37 +347,59 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
       cur = tl;
     }
     // scale by 2^-E per flavour and convert to FP32 once per tile: thread
-    // (site s, transform groups q = c0 + 16 j of 72: 36 per flavour) reads the
+    // (site s, groups g = c0 + 16 j of 40: 20 per flavour) reads the
     // component-major staging, applies the slice's load-time transform to the
-    // group's four blocks and writes the site's padded row (exact
-    // power-of-two scales; products are formed in double so that no
-    // intermediate leaves the representable range)
+    // group's four blocks b, b + 2, b + 8, b + 10 and writes the site's padded
+    // row (exact power-of-two scales; products are formed in double so that
+    // no intermediate leaves the representable range).  Groups 0..15 of a
+    // flavour are (b, colour pair 2k, 2k + 1): one 16-byte store per block,
+    // so the 8 sites of a quarter-warp write 8 different bank groups (rows are
+    // 161 units apart); groups 16..19 are (b, colour 8).
     {
       const double su = ldexp(1.0, -a.exps[2 * tl]), sd = ldexp(1.0, -a.exps[2 * tl + 1]);
       const int xfu = a.sl[tl].xf[0], xfd = a.sl[tl].xf[1];
       const int s = tid & (kSitesPerTile - 1), c0 = tid >> 4;
       Cx<float>* row = sf + s * kRow32;
 #pragma unroll
-      for (int j = 0; j < 5; j++) {
-        const int q = c0 + 16 * j;
-        if (q < 72) {
-          const int f = q >= 36;
-          int b, cc;
-          prop_group_base(q - 36 * f, b, cc);
-          // the group's four components at fixed offsets from one staging and one row index
-          const Cx<Tin>* src = st + (144 * f + 9 * b + cc) * kSitesPerTile + s;
-          Cx<float>* dst = row + 2 * row32_unit(16 * f + b, cc >> 1) + (cc & 1);
-          Cx<double> v[4];
-#pragma unroll
-          for (int i = 0; i < 4; i++) {
-            const Cx<Tin> x = src[9 * group_blk(i) * kSitesPerTile];
-            v[i] = cx<double>((double)x.x, (double)x.y);
-          }
-          prop_group_transform(v[0], v[1], v[2], v[3], f ? xfd : xfu);
+      for (int j = 0; j < 3; j++) {
+        const int g = c0 + 16 * j;
+        if (g < 40) {
+          const int f = g >= 20, gf = g - 20 * f;
+          const int bq = gf & 3, b = (bq >> 1) * 4 + (bq & 1);  // first block of the transform group: 0, 1, 4, 5
+          const int xf = f ? xfd : xfu;
           const double sc = f ? sd : su;
+          const Cx<Tin>* src = st + (144 * f + 9 * b) * kSitesPerTile + s;
+          if (gf < 16) {
+            const int k = gf >> 2;  // colours 2k, 2k + 1
+            Cx<double> v[2][4];
 #pragma unroll
-          for (int i = 0; i < 4; i++)
-            dst[2 * row32_unit(group_blk(i), 0)] = cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
+            for (int c = 0; c < 2; c++)
+#pragma unroll
+              for (int i = 0; i < 4; i++) {
+                const Cx<Tin> x = src[(9 * group_blk(i) + 2 * k + c) * kSitesPerTile];
+                v[c][i] = cx<double>((double)x.x, (double)x.y);
+              }
+#pragma unroll
+            for (int c = 0; c < 2; c++) prop_group_transform(v[c][0], v[c][1], v[c][2], v[c][3], xf);
+            Cx<float>* dst = row + 2 * row32_unit(16 * f + b, k);
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+              *reinterpret_cast<float4*>(dst + 2 * row32_unit(group_blk(i), 0)) =
+                  make_float4((float)(v[0][i].x * sc), (float)(v[0][i].y * sc), (float)(v[1][i].x * sc),
+                              (float)(v[1][i].y * sc));
+          } else {
+            Cx<double> v[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              const Cx<Tin> x = src[(9 * group_blk(i) + 8) * kSitesPerTile];
+              v[i] = cx<double>((double)x.x, (double)x.y);
+            }
+            prop_group_transform(v[0], v[1], v[2], v[3], xf);
+            Cx<float>* dst = row + 2 * row32_unit(16 * f + b, 4);
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+              dst[2 * row32_unit(group_blk(i), 0)] = cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
+          }
         }
       }
     }
