@@ -459,6 +459,7 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request* reqs, con
     a.K = pl.K;
     a.k = offsets_of(what);
     a.out = c->cbuf.p;
+    a.g16_raw = p2::g16_raw(what) ? 1 : 0;  // the projection is followed by k_meson_gamma
     {
       ProfScope ps(c, "contract_plain_fp64");
       P2_TRY(c, p2::launch_contract_plain(a, c->nsm, c->stream), "contract kernel");
@@ -532,6 +533,22 @@ p2_status run_plain(p2_ctx* c, const p2_prop* props, const p2_request* reqs, con
     {
       ProfScope ps(c, "reduce_scatter");
       P2_TRY(c, p2::launch_scatter(sa, c->stream), "reduction kernel");
+    }
+    if (p2::g16_raw(what)) {
+      // the Gamma sums of the 16 x 16 block on its projected colour products
+      p2::MesonGammaArgs mg{};
+      mg.sl = sg.desc((int)ci);
+      mg.ntau = n;
+      mg.nmom = pl.nmom;
+      bool found = false;
+      for (const auto& b : pl.blocks)
+        if (b.comps == 256) {
+          mg.blk = b;
+          found = true;
+        }
+      if (!found) return c->fail(P2_ERR_INVALID_ARG, "16 x 16 meson block missing from the plan");
+      ProfScope ps(c, "meson_gamma");
+      P2_TRY(c, p2::launch_meson_gamma(mg, c->stream), "meson Gamma sums");
     }
   }
   return P2_OK;

@@ -164,16 +164,23 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
     w.put_slot(a.k.nuc + 16 + l, pn[1], 1);
   }
   const int g1 = lt.meson_g1();  // the sink Gamma of this lane's meson outputs
-  if (w.g16 && g16_raw(a.what)) {
+  if (a.g16_raw) {
     // the colour-traced products M_{al de}[b][z] of lane (al, de): no Gamma
     // stage here, k_meson_gamma forms the Gamma sums after the projection
     Cx<R> M[4][4];
     meson_M(row, kU, kD, l >> 2, l & 3, M);
-    __syncwarp(mask);  // every lane of the half-warp has finished reading the row
+    if (w.g16) {
+      __syncwarp(mask);  // every lane of the half-warp has finished reading the row
 #pragma unroll
-    for (int b = 0; b < 4; b++)
+      for (int b = 0; b < 4; b++)
 #pragma unroll
-      for (int z = 0; z < 4; z++) w.g16[g16_slot(l, 4 * b + z)] = M[b][z];
+        for (int z = 0; z < 4; z++) w.g16[g16_slot(l, 4 * b + z)] = M[b][z];
+    } else {
+#pragma unroll
+      for (int b = 0; b < 4; b++)
+#pragma unroll
+        for (int z = 0; z < 4; z++) w.put(a.k.g16 + 16 * l + 4 * b + z, M[b][z]);
+    }
   } else if (a.what & (8u | 16u | 32u)) {
     Cx<R> c[16];
     // staged 16 x 16 outputs leave their unit phases r_g1 r_g2 to the

@@ -62,6 +62,9 @@ struct ContractArgs {
   // (input x 2^-E, exps[2 s + f]), and max(|Re|,|Im|) per (slice, component) as float bits
   const int* exps;
   int* cmax;  // [ntau][K]
+  // 1: the 16 x 16 block's components are the colour products M of g16_raw
+  // (its result goes through the projection and then k_meson_gamma)
+  int g16_raw;
 };
 
 // Per-slice magnitude exponents of the u and d views, from a strided sample.

@@ -339,6 +339,7 @@ p2_status precision_run_batch(p2_ctx* c, const p2_prop* props, const p2_request*
     a.out = c->cbuf.p;
     a.exps = (const int*)c->expb.p;
     a.cmax = (int*)c->cmaxb.p;
+    a.g16_raw = g16_raw(what) ? 1 : 0;
     {
       ProfScope ps(c, "contract_f32");
       P2_TRY(c, p2::launch_contract_f32(a, chunk_fp32, 2 * c->nsm, c->stream), "contract kernel");

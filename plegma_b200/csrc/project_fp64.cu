@@ -31,8 +31,11 @@ constexpr int kPT = 16 * kTP;
 // store and the per-component reads of a quarter-warp both touch 8
 // different 16-byte bank groups).  The next step's global loads are issued
 // into registers before the current step's products (software pipeline).
+// Tiles of up to 4 x 4 complex per thread fit in 128 registers: two CTAs per
+// SM (16 warps) hide the loads without a register prefetch; the 4 x 6 tile
+// runs one CTA per SM with the prefetch, the 4 x 8 tile with neither.
 template <int TK>
-__global__ void __launch_bounds__(kThreads, 1) k_project_fp64(const ProjArgs a) {
+__global__ void __launch_bounds__(kThreads, TK <= 4 ? 2 : 1) k_project_fp64(const ProjArgs a) {
   constexpr int KT = 16 * TK;
   constexpr int NE = (kXS * kPT) / kThreads;  // phase entries per thread per step
   constexpr int NC = (kXS * KT) / kThreads;   // site values per thread per step
@@ -59,9 +62,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_fp64(const ProjArgs a) 
 
   // this thread's loads of a step: phase entries (xs = e / kPT, pp = e % kPT)
   // as three per-dimension factors, site values (xs = e % kXS, kk = e / kXS);
-  // the widest tile (TK = 8) has no registers to spare: it loads each step
-  // at the step's start instead
-  constexpr bool kPrefetch = TK <= 6;
+  // the 4 x 6 tile prefetches; the others load each step at its start
+  constexpr bool kPrefetch = TK == 6;
   Cx<double> fx[NE], fy[NE], fz[NE], cv_next[NC];
   auto load_phases = [&](int xs0) {
 #pragma unroll
@@ -91,17 +93,42 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_fp64(const ProjArgs a) 
   };
   if (kPrefetch && xb < xe) load_step(xb);
   for (int xs0 = xb; xs0 < xe; xs0 += kXS) {
-    if (!kPrefetch) load_step(xs0);
+    if (kPrefetch) {
 #pragma unroll
-    for (int r = 0; r < NE; r++) {
-      const int e = tid + r * kThreads;
-      sE[e / kPT][e % kPT] = cmul(cmul(fx[r], fy[r]), fz[r]);
-    }
+      for (int r = 0; r < NE; r++) {
+        const int e = tid + r * kThreads;
+        sE[e / kPT][e % kPT] = cmul(cmul(fx[r], fy[r]), fz[r]);
+      }
 #pragma unroll
-    for (int r = 0; r < NC; r++) {
-      const int e = tid + r * kThreads;
-      const int xs = e % kXS, kk = e / kXS;
-      sC[kk][xs ^ (kk & 15)] = cv_next[r];
+      for (int r = 0; r < NC; r++) {
+        const int e = tid + r * kThreads;
+        const int xs = e % kXS, kk = e / kXS;
+        sC[kk][xs ^ (kk & 15)] = cv_next[r];
+      }
+    } else {
+      // each entry straight from the global tables into shared memory (no register arrays live)
+#pragma unroll
+      for (int r = 0; r < NE; r++) {
+        const int e = tid + r * kThreads;
+        const int xs = e / kPT, pp = e % kPT;
+        const int p = p0 + pp, x = xs0 + xs;
+        Cx<double> v = czero<double>();
+        if (p < a.nmom && x < xe) {
+          const int xx = x % a.Lx, yy = (x / a.Lx) % a.Ly, zz = x / LxLy;
+          v = cmul(cmul(tab[(0 * a.nmom + p) * a.Lmax + xx], tab[(1 * a.nmom + p) * a.Lmax + yy]),
+                   tab[(2 * a.nmom + p) * a.Lmax + zz]);
+        }
+        sE[xs][pp] = v;
+      }
+#pragma unroll
+      for (int r = 0; r < NC; r++) {
+        const int e = tid + r * kThreads;
+        const int xs = e % kXS, kk = e / kXS;
+        const int k = k0 + kk, x = xs0 + xs;
+        Cx<double> v = czero<double>();
+        if (k < a.K && x < xe) v = c[(long long)k * a.sK + x];
+        sC[kk][xs ^ (kk & 15)] = v;
+      }
     }
     __syncthreads();
     if (kPrefetch && xs0 + kXS < xe) load_step(xs0 + kXS);  // in flight during the products
