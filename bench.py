@@ -207,7 +207,7 @@ def run_reference(args, rank, world):
 TRAFFIC_PER_SITE = {("contract_f32", "split"): 6863, ("contract_plain_fp64", "plain"): 9129}
 # executed FP64 flop per site of the plain site contraction (2 per DFMA, 1 per
 # DADD / DMUL, from the ncu instruction counters of the 32^3 x 16 case)
-FP64_FLOP_PER_SITE = {"contract_plain_fp64": 55968}
+FP64_FLOP_PER_SITE = {"contract_plain_fp64": 50336}
 
 BATCHED = {
     # name: (lattice, sources, window range, |n|^2 max, propagator precision, decay, seed, sources resident at once)

@@ -143,18 +143,17 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
                        [&](int j, int ds, Cx<R> v) { w.put(base[j] + 16 * ds + l, v); });
   }
   if (DELTA && (a.what & (2u | 4u))) {
-    // group g of each isospin block, datasets (u-rich, d-rich)
-    // the iso-1/2 partial sums are parked in the iso-1/2 output slots when
-    // those are requested, else in the iso-3/2 slots that are written later
-    const int park = (a.what & 2u) ? a.k.diso12 : a.k.diso32;
+    // group g of each isospin block, datasets (u-rich, d-rich); the iso-1/2
+    // partial sums of G^{ud} wait in a per-thread array (local memory, L1)
+    // until the G^{uu} / G^{dd} terms complete them
+    Cx<R> parked[3][2];
     delta_site(
         row, lt, l, mask,
         [&](int g, int j, Cx<R> v) {
           if (j < 2 && (a.what & 2u)) w.put(a.k.diso12 + (g * 2 + j) * 16 + l, v);
           if (j >= 2 && (a.what & 4u)) w.put(a.k.diso32 + (g * 2 + j - 2) * 16 + l, v);
         },
-        [&](int g, int j, Cx<R> v) { w.out[(long long)(park + (g * 2 + j) * 16 + l) * w.V3] = v; },
-        [&](int g, int j) { return w.out[(long long)(park + (g * 2 + j) * 16 + l) * w.V3]; });
+        [&](int g, int j, Cx<R> v) { parked[g][j] = v; }, [&](int g, int j) { return parked[g][j]; });
   }
   if (DELTA) return;
   if (a.what & 1u) {

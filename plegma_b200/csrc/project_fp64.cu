@@ -139,10 +139,23 @@ __global__ void __launch_bounds__(kThreads, TK <= 4 ? 2 : 1) k_project_fp64(cons
       for (int i = 0; i < kTP; i++) ev[i] = sE[xs][tp + 16 * i];
 #pragma unroll
       for (int j = 0; j < TK; j++) cv[j] = sC[tk + 16 * j][xs ^ tk];  // (tk + 16 j) & 15 == tk
+      // the two FMAs of each real and imaginary part in separate passes, so
+      // that consecutive DFMAs update different accumulators (4 TK of them
+      // between an accumulator's dependent pair)
 #pragma unroll
       for (int i = 0; i < kTP; i++)
 #pragma unroll
-        for (int j = 0; j < TK; j++) cmac(acc[i][j], ev[i], cv[j]);
+        for (int j = 0; j < TK; j++) {
+          acc[i][j].x = fma(ev[i].x, cv[j].x, acc[i][j].x);
+          acc[i][j].y = fma(ev[i].x, cv[j].y, acc[i][j].y);
+        }
+#pragma unroll
+      for (int i = 0; i < kTP; i++)
+#pragma unroll
+        for (int j = 0; j < TK; j++) {
+          acc[i][j].x = fma(-ev[i].y, cv[j].y, acc[i][j].x);
+          acc[i][j].y = fma(ev[i].y, cv[j].x, acc[i][j].y);
+        }
     }
     __syncthreads();
   }
