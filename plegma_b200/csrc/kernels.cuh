@@ -131,7 +131,7 @@ struct SplitGemmArgs {
   int ks_per_split, nsplit;
   float* part;       // [ntau][nsplit][nmtile][128][ntile * 2 * NT]
   int* err;          // set to 1 if a bounded wait gave up
-  long long wait_limit;  // polls of every mbarrier wait before it gives up
+  long long wait_limit;  // nanoseconds (global timer) an mbarrier wait may take before it gives up; 0: 2 s
   int withhold;      // test hook: the converters never signal their B stages, so the waits run out
 };
 

@@ -208,7 +208,7 @@ p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int
   g.nmtile = nmtile;
   g.part = (float*)c->fpart.p;
   g.err = (int*)c->errflag.p;
-  g.wait_limit = 1LL << 24;
+  g.wait_limit = 0;  // the kernel's default time limit
   auto set = [&](p2::SplitGemmArgs& q, const std::vector<int>& v) {
     q.NT = v[0];
     q.ntile = v[1];
@@ -230,7 +230,7 @@ p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int
   set(g, pick);
   if (c->wait_test) {  // p2_debug_wait_timeout: this launch's waits run out (after tuning, which launches normally)
     g.withhold = 1;
-    g.wait_limit = 1LL << 14;
+    g.wait_limit = 20000000;  // 20 ms
     c->wait_test = 0;
   }
   const int NT = g.NT, nsplit = g.nsplit;

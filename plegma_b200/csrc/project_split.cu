@@ -73,8 +73,20 @@ constexpr int kBarBytes = 128;  // mbarriers, TMEM address, error flag
 __host__ __device__ constexpr int stage_bytes(int NT, int nb, int na) {
   return nb * 2 * b_tile_bytes(NT) + na * 2 * kATile + kBarBytes + 1024;
 }
-__host__ __device__ constexpr int b_stages(int NT) { return stage_bytes(NT, 3, 3) <= kSmemMax ? 3 : 2; }
-__host__ __device__ constexpr int a_stages(int NT) { return stage_bytes(NT, b_stages(NT), 3) <= kSmemMax ? 3 : 2; }
+#ifndef P2_PROJ_NB
+#define P2_PROJ_NB 3
+#endif
+#ifndef P2_PROJ_NA
+#define P2_PROJ_NA 3
+#endif
+constexpr int kMaxNA = 4, kMaxNB = 3;
+__host__ __device__ constexpr int b_stages(int NT) {
+  return stage_bytes(NT, P2_PROJ_NB, P2_PROJ_NA) <= kSmemMax ? P2_PROJ_NB : stage_bytes(NT, 3, 3) <= kSmemMax ? 3 : 2;
+}
+__host__ __device__ constexpr int a_stages(int NT) {
+  return stage_bytes(NT, P2_PROJ_NB, P2_PROJ_NA) <= kSmemMax ? P2_PROJ_NA
+         : stage_bytes(NT, b_stages(NT), 3) <= kSmemMax ? 3 : 2;
+}
 __host__ __device__ constexpr int smem_bytes(int NT) { return stage_bytes(NT, b_stages(NT), a_stages(NT)); }
 // two ping-pong accumulator tiles and the FP32 sum, 2NT columns each
 __host__ __device__ constexpr int tmem_cols(int NT) {
@@ -147,6 +159,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
   constexpr int NA = a_stages(NT);
   constexpr int NB = b_stages(NT);
   static_assert(NT % 8 == 0 && NT <= kMaxNT, "N-tile width");
+  static_assert(NA <= kMaxNA && NB <= kMaxNB && (kMaxNA + 2 * kMaxNB + 4) * 8 + 12 <= kBarBytes, "mbarrier area");
   constexpr uint32_t IDESC = tc::idesc_f16_f32(128, NR);
   constexpr int TCOLS = tmem_cols(NT);
   constexpr int NP = NB > kPromote ? NB : kPromote;  // k-steps per accumulator tile (>= NB: see the drain schedule)
@@ -156,12 +169,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* sA = smem + NB * 2 * BT;  // NA phase stages of 2 kATile (hi, lo) after the NB B stages
   uint64_t* fullA = (uint64_t*)(sA + NA * 2 * kATile);
-  uint64_t* done = fullA + 3;
-  uint64_t* fullB = done + 3;
+  uint64_t* done = fullA + kMaxNA;
+  uint64_t* fullB = done + kMaxNB;
   uint64_t* d1full = fullB + 3;  // accumulator tile b holds its group's complete sum (MMA commit)
   uint64_t* d1free = d1full + 2;  // accumulator tile b has been added to the sum (converter warps)
   uint32_t* tslot = (uint32_t*)(d1free + 2);
   int* flag = (int*)(tslot + 1);
+  int* skipf = flag + 1;  // another CTA of the launch has already failed: do no work
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nti = blockIdx.x % a.ntile, mt = blockIdx.x / a.ntile;
@@ -186,16 +200,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
     }
     tc::fence_mbar_init();
     *flag = 0;
+    *skipf = *(volatile int*)a.err;
   }
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = *tslot;
-  const long long lim = a.wait_limit;
+  const long long lim = a.wait_limit > 0 ? a.wait_limit : tc::kWaitLimitNs;
+  const bool skip = *skipf != 0;
   const unsigned char* Ab = (const unsigned char*)a.A + (long long)mt * a.nkstep * 2 * kATile;
-  bool failed = false;
+  bool failed = skip;
 
-  if (warp == kConvWarps) {
+  if (skip) {
+    // the launch's result is discarded: straight to the epilogue's error path
+  } else if (warp == kConvWarps) {
     // ---- copy / MMA warp: lane 0 ----
     if (lane == 0 && nk > 0) {
       int issued = -1, committed = -1;
@@ -211,17 +229,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
       };
       issue_a(0);
       for (int i = 0; i < nk && !failed; i++) {
-        // the phase copy of k-step `next` (one k-step ahead with three A
-        // stages, this k-step with two) reuses the stage of k-step next - NA,
-        // whose MMAs must be complete
-        const int next = i + NA - 2;
-        if (next < nk && next > issued) {
-          if (next >= NA && !tc::mbar_wait(&done[(next - NA) % NB], ((next - NA) / NB) & 1, lim)) {
+        // the phase copies up to k-step i + NA - 2 (NA - 2 k-steps ahead; this
+        // k-step with two stages); the copy of k-step j reuses the stage of
+        // k-step j - NA <= i - 2, whose MMAs must be complete
+        const int next = min(i + NA - 2, nk - 1);
+        while (issued < next) {
+          const int j = issued + 1;
+          if (j >= NA && !tc::mbar_wait(&done[(j - NA) % NB], ((j - NA) / NB) & 1, lim)) {
             failed = true;
             break;
           }
-          issue_a(next);
+          issue_a(j);
         }
+        if (failed) break;
         const int s = i % NB;
         const int grp = i / NP, b = grp & 1;
         // the first k-step of a group reuses accumulator tile b: the converters
@@ -258,7 +278,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
       if (failed) {
         *flag = 1;
         for (int j = max(0, issued - NA + 1); j <= issued; j++)
-          tc::mbar_wait(&fullA[j % NA], (j / NA) & 1, 1LL << 22);
+          tc::mbar_wait(&fullA[j % NA], (j / NA) & 1, 100000000LL);  // in-flight copies: 0.1 s
       }
     }
     __syncwarp();

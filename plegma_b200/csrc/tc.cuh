@@ -28,12 +28,30 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "r"(smem_u32(bar)), "r"(parity));
   return ok != 0;
 }
-// Wait with an iteration limit; returns false (and the caller records an
-// error) if the phase did not complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = (1LL << 24)) {
-  for (long long i = 0; i < limit; i++)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
+// Nanoseconds of the GPU's global timer.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+
+// Default limit of a bounded wait: every wait of the pipelines here normally
+// completes within microseconds.
+constexpr long long kWaitLimitNs = 2000000000LL;
+
+// Wait with a time limit (nanoseconds of the global timer, checked every 64
+// polls: a try_wait may suspend the thread for a while, so a poll count would
+// not bound the time); returns false (and the caller records an error) if the
+// phase did not complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit_ns = kWaitLimitNs) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+#pragma unroll 1
+    for (int i = 0; i < 64; i++)
+      if (mbar_try_wait(bar, parity)) return true;
+    if ((long long)(global_ns() - t0) > limit_ns) return false;
+  }
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
