@@ -208,6 +208,11 @@ TRAFFIC_PER_SITE = {("contract_f32", "split"): 6863, ("contract_plain_fp64", "pl
 # executed FP64 flop per site of the plain site contraction (2 per DFMA, 1 per
 # DADD / DMUL, from the ncu instruction counters of the 32^3 x 16 case)
 FP64_FLOP_PER_SITE = {"contract_plain_fp64": 50336}
+# LSU data-pipe wavefronts per site of the split site contraction (ncu
+# l1tex__data_pipe_lsu_wavefronts.sum / sites, 32^3 x 16 case): its binding
+# on-chip limit, one wavefront (128 bytes between shared memory and the
+# registers) per SM and clock
+LSU_WAVEFRONTS_PER_SITE = {"contract_f32": 481.6}
 
 BATCHED = {
     # name: (lattice, sources, window range, |n|^2 max, propagator precision, decay, seed, sources resident at once)
@@ -468,6 +473,19 @@ def main():
                 "traffic_note": "DRAM read+write bytes per site from the ncu capture of the 32^3x16 case, "
                                 "times the sites of one launch" if tps else None,
                 "algorithmic_bytes_per_launch": bytes_per_site * per_launch, "sites_per_launch": per_launch}
+    # the split contraction against its on-chip bound: the LSU data pipe's one
+    # wavefront per SM and clock, at the median SM clock sampled in the timed region
+    roof_lsu = None
+    if ck and LSU_WAVEFRONTS_PER_SITE.get(ck[0]) and r["clocks"].get("sm_mhz"):
+        n, kms = prof[ck[0]]
+        nsm = torch.cuda.get_device_properties(0).multi_processor_count
+        wf = LSU_WAVEFRONTS_PER_SITE[ck[0]]
+        floor_ms = wf * sites / (nsm * r["clocks"]["sm_mhz"] * 1e6) * 1e3
+        ms_k = kms / args.steps
+        roof_lsu = {"kernel": ck[0], "bound": "lsu data pipe (1 wavefront / SM / clock)",
+                    "wavefronts_per_site": wf, "wavefronts_source": "ncu, 32^3x16 case",
+                    "sm_mhz": r["clocks"]["sm_mhz"], "sms": nsm, "floor_ms_per_step": floor_ms,
+                    "ms_per_step": ms_k, "frac": floor_ms / ms_k if ms_k > 0 else None}
     # the projection against the tensor (split) or FP64 (plain) roofline, algorithmic flop = 8 nmom K per site
     roof_proj = None
     pk = [k for k in prof if k.startswith("project")]
@@ -593,7 +611,7 @@ def main():
                 "err_note": "max over the checked slices of max_{p,k} |C - C_oracle| / sum_x |c_k(x,t)|, "
                             "FP64 oracle, this run's own output",
                 "fp64_peak": fp64, "roofline_fp64": roof64,
-                "roofline": roof, "roofline_projection": roof_proj, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roof, "roofline_lsu": roof_lsu, "roofline_projection": roof_proj, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": r["clocks"], "batched": batched}
         print(json.dumps(line), flush=True)
     if dist:
