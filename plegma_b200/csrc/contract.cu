@@ -84,8 +84,9 @@ __device__ __forceinline__ int diag10_slot(int g) {
 }
 
 // Split form: the per-component maxima of the current slice live in the spare
-// slot of each FP32 tile block (row s, block j holds components 2 (32 s + j)
-// and 2 (32 s + j) + 1), which no load of the contraction reads.
+// slot of each FP32 tile block position (row s, position j holds components
+// 2 (32 s + j) and 2 (32 s + j) + 1), which no load of the contraction reads,
+// whichever block the position holds.
 __device__ __forceinline__ int* smax_slot(Cx<float>* sf, int k) {
   const int p = k >> 1, s = p >> 5, j = p & 31;
   return reinterpret_cast<int*>(sf + s * kRow32 + 2 * row32_unit(j, 4) + 1) + (k & 1);
@@ -94,16 +95,21 @@ __device__ __forceinline__ int* smax_slot(Cx<float>* sf, int k) {
 // Split form, 16 x 16 mesons: a half-warp reads only its own site's FP32 row,
 // so once its contraction is done it stages the site's 256 outputs in that
 // row (C[g1][g2] of lane g1, or with g16_raw the products M_{a d}[b][z] of lane
-// l = 4 a + d in the slot of g1 = l, g2 = 4 b + z), output j = 16 g2 + g1 at
-// complex 10 (j >> 3) + (j & 7): the four data
-// units of every block (the colour-8 and spare slots keep their contents, the
-// spare slots holding the per-component maxima).  The flush after the tile
-// writes them to HBM, 128 contiguous bytes per component; direct stores from
-// the lanes would touch 16 component rows per instruction.  The staging
-// buffer stays free for the whole next tile's copies.
+// l = 4 a + d in the slot of g1 = l, g2 = 4 b + z), in the eight data
+// complex (units 0-3) of the row's 32 block positions (the colour-8 and spare
+// slots keep their contents, the spare slots holding the per-component
+// maxima).  The 16 outputs of one g2 go to positions b1 (g1 < 8) and b1 + 4
+// (g1 >= 8), b1 = 8 (g2 >> 2) + (g2 & 3): their eight 16-byte units lie in
+// eight different bank groups (4 positions = 20 units = 4 mod 8), and those
+// of the warp's other site, whose row starts 161 units further, in the same
+// eight shifted by one, so a warp-wide store takes the minimum two
+// wavefronts.  The flush after the tile writes them to HBM, 128 contiguous
+// bytes per component; direct stores from the lanes would touch 16 component
+// rows per instruction.  The staging buffer stays free for the whole next
+// tile's copies.
 __device__ __forceinline__ int g16_slot(int g1, int g2) {
-  const int j = 16 * g2 + g1;
-  return 10 * (j >> 3) + (j & 7);
+  const int pos = 8 * (g2 >> 2) + (g2 & 3) + 4 * (g1 >> 3);
+  return 10 * pos + (g1 & 7);
 }
 
 template <typename R>
@@ -295,6 +301,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
   // 16 x 16 meson outputs staged in the sites' own FP32 rows (not with the
   // 10 diagonal structures, whose second pass reads the rows again)
   const bool stage = !DELTA && g16_phase_deferred(a.what);
+  // block layout of the FP32 rows: conflict-free lane-varying loads for the
+  // nucleon and mesons; the Delta keeps the plain order (its registers are fuller)
+  constexpr bool kPerm = !DELTA;
   const int tid = threadIdx.x;
   const int hw = tid >> 4, l = tid & 15;
   const unsigned mask = halfwarp_mask();
@@ -387,10 +396,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
               }
 #pragma unroll
             for (int c = 0; c < 2; c++) prop_group_transform(v[c][0], v[c][1], v[c][2], v[c][3], xf);
-            Cx<float>* dst = row + 2 * row32_unit(16 * f + b, k);
 #pragma unroll
             for (int i = 0; i < 4; i++)
-              *reinterpret_cast<float4*>(dst + 2 * row32_unit(group_blk(i), 0)) =
+              *reinterpret_cast<float4*>(row + 2 * row32_unit<kPerm>(16 * f + b + group_blk(i), k)) =
                   make_float4((float)(v[0][i].x * sc), (float)(v[0][i].y * sc), (float)(v[1][i].x * sc),
                               (float)(v[1][i].y * sc));
           } else {
@@ -401,10 +409,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
               v[i] = cx<double>((double)x.x, (double)x.y);
             }
             prop_group_transform(v[0], v[1], v[2], v[3], xf);
-            Cx<float>* dst = row + 2 * row32_unit(16 * f + b, 4);
 #pragma unroll
             for (int i = 0; i < 4; i++)
-              dst[2 * row32_unit(group_blk(i), 0)] = cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
+              row[2 * row32_unit<kPerm>(16 * f + b + group_blk(i), 4)] =
+                  cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
           }
         }
       }
@@ -417,7 +425,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
     }
     const int x0 = tc.x0();
     if (x0 + hw < a.V3) {
-      const RowF32 row{sf + hw * kRow32};
+      const RowF32T<kPerm> row{sf + hw * kRow32};
       const Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x0 + hw, a.V3, DELTA ? nullptr : rmax, sf,
                             stage ? sf + hw * kRow32 : nullptr};
       contract_site<DELTA>(a, row, lt, l, mask, w);

@@ -95,23 +95,46 @@ struct RowF64 {
 // transposing writes of 16 sites then start in 8 different bank groups,
 // and the two sites of a warp read disjoint bank groups.
 constexpr int kRow32 = 322;  // complex per site row (32 blocks x 10 + 2)
-__device__ __forceinline__ int row32_unit(int blk, int k) { return blk * 5 + k; }
+// Position of spin block blk = 16 f + 4 mu + nu in the row.  PERM = false:
+// position blk.  PERM = true: the blocks of a flavour are placed so that the
+// four blocks of any fixed mu (nu = 0..3), of any fixed nu (mu = 0..3) and
+// the eight of mu in {0, 1} or {2, 3} sit at positions distinct mod 8, i.e.
+// in different bank groups (a position is 5 units and 5 is invertible mod
+// 8): position (nu + 4 (mu & 1) + (mu >> 1)) mod 8 + 8 (mu >> 1).  The loads
+// whose block varies over the lanes (the mesons' A[al][b] and B[de][z], the
+// diquarks' X[nu][x'] and Y[lam][y'], the slot and type-a terms) then fetch
+// their 4 or 8 distinct units without bank conflicts (ncu, nucleon + mesons
+// at 32^3 x 16: shared-load bank conflicts 44.9 M -> 17.8 M per launch), at
+// the price of per-lane position registers, so the Delta instantiation,
+// whose registers are fuller, keeps PERM = false.
+template <bool PERM>
+__host__ __device__ __forceinline__ constexpr int row32_pos(int blk) {
+  return PERM ? (blk & ~15) | ((((blk & 3) + 4 * ((blk >> 2) & 1) + ((blk >> 3) & 1)) & 7) + 8 * ((blk >> 3) & 1))
+              : blk;
+}
+template <bool PERM = false>
+__device__ __forceinline__ int row32_unit(int blk, int k) {
+  return row32_pos<PERM>(blk) * 5 + k;
+}
 
-struct RowF32 {
+template <bool PERM>
+struct RowF32T {
   typedef float R;
+  static constexpr bool kPerm = PERM;
   const Cx<float>* p;
   __device__ __forceinline__ void pair(int blk, int k, Cx<float>& v0, Cx<float>& v1) const {
-    const float4 q = *reinterpret_cast<const float4*>(p + 2 * row32_unit(blk, k));
+    const float4 q = *reinterpret_cast<const float4*>(p + 2 * row32_unit<PERM>(blk, k));
     v0 = cx<float>(q.x, q.y);
     v1 = cx<float>(q.z, q.w);
   }
-  __device__ __forceinline__ Cx<float> last(int blk) const { return p[2 * row32_unit(blk, 4)]; }
+  __device__ __forceinline__ Cx<float> last(int blk) const { return p[2 * row32_unit<PERM>(blk, 4)]; }
   __device__ __forceinline__ void load9(int blk, Cx<float> v[9]) const {
 #pragma unroll
     for (int k = 0; k < 4; k++) pair(blk, k, v[2 * k], v[2 * k + 1]);
     v[8] = last(blk);
   }
 };
+using RowF32 = RowF32T<false>;
 
 constexpr int kU = 0, kD = 16;  // block offsets of the u and d propagators in a row
 
@@ -195,9 +218,8 @@ __device__ __forceinline__ void diquark_acc_ct(const Row& row, int X, int Y, int
 // output, (ax bx, ax by) and (ay bx, ay by): b enters as its natural (Re, Im)
 // pair (and its negation for the subtracted terms), a as broadcasts shared
 // by its four terms.
-template <int nu, int lam, int sg>
-__device__ __forceinline__ void dq_acc_f32(const RowF32& row, int X, int Y, int xp, int yp, f32x2 px[9],
-                                           f32x2 py[9]) {
+template <int nu, int lam, int sg, typename Row>
+__device__ __forceinline__ void dq_acc_f32(const Row& row, int X, int Y, int xp, int yp, f32x2 px[9], f32x2 py[9]) {
   Cx<float> a[9], b[9];
   row.load9(X + nu * 4 + xp, a);
   row.load9(Y + lam * 4 + yp, b);
@@ -226,8 +248,8 @@ __device__ __forceinline__ void dq_acc_f32(const RowF32& row, int X, int Y, int 
   }
 }
 
-template <int S, int iA>
-__device__ __forceinline__ void diquark_acc_ct_f32(const RowF32& row, int X, int Y, int xp, int yp, f32x2 px[9],
+template <int S, int iA, typename Row>
+__device__ __forceinline__ void diquark_acc_ct_f32(const Row& row, int X, int Y, int xp, int yp, f32x2 px[9],
                                                    f32x2 py[9]) {
   dq_acc_f32<sink_entry(S, iA, 0), sink_entry(S, iA, 1), sink_entry(S, iA, 2)>(row, X, Y, xp, yp, px, py);
 }
@@ -587,8 +609,8 @@ __device__ __forceinline__ void meson_M(const Row& row, int A, int B, int al, in
 // FP32 tile: the same sum with paired FMAs on (Re, Im) pairs,
 //   M += (u.x, u.y) * (d.x, d.x) + (u.y, -u.x) * (d.y, d.y),
 // two instructions per complex product instead of four.
-template <>
-__device__ __forceinline__ void meson_M<RowF32>(const RowF32& row, int A, int B, int al, int de, Cx<float> Mo[4][4]) {
+template <bool PERM>
+__device__ __forceinline__ void meson_M(const RowF32T<PERM>& row, int A, int B, int al, int de, Cx<float> Mo[4][4]) {
   f32x2 M[4][4];
 #pragma unroll
   for (int i = 0; i < 4; i++)

@@ -338,7 +338,6 @@ __global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc_f32(const UdscAr
           int b, cc;
           prop_group_base(q - 36 * f, b, cc);
           const Cx<Tin>* src = st + (144 * f + 9 * b + cc) * kSitesU + s;
-          Cx<float>* dst = row + 2 * row32_unit(16 * f + b, cc >> 1) + (cc & 1);
           Cx<double> v[4];
 #pragma unroll
           for (int i = 0; i < 4; i++) {
@@ -348,7 +347,8 @@ __global__ void __launch_bounds__(kThreadsU, 1) k_contract_udsc_f32(const UdscAr
           prop_group_transform(v[0], v[1], v[2], v[3], sd.xf[f]);
 #pragma unroll
           for (int i = 0; i < 4; i++)
-            dst[2 * row32_unit(group_blk(i), 0)] = cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
+            row[2 * row32_unit(16 * f + b + group_blk(i), cc >> 1) + (cc & 1)] =
+                cx<float>((float)(v[i].x * sc), (float)(v[i].y * sc));
         }
       }
     }
