@@ -111,6 +111,9 @@ __device__ __forceinline__ int g16_slot(int g1, int g2) {
   const int pos = 8 * (g2 >> 2) + (g2 & 3) + 4 * (g1 >> 3);
   return 10 * pos + (g1 & 7);
 }
+// The nucleon's 32 outputs of a site staged beside them: component c in the
+// colour-8 complex of block position c (complex 10 c + 8).
+__device__ __forceinline__ int nuc_slot(int c) { return 10 * c + 8; }
 
 template <typename R>
 struct Writer {
@@ -130,6 +133,10 @@ struct Writer {
   // (slot) and reaches shared memory once per time slice.
   __device__ __forceinline__ void put_slot(int k, Cx<R> v, int slot) const {
     out[(long long)k * V3] = v;
+    note_slot(v, slot);
+  }
+  // the maximum only (the value leaves through the staged flush)
+  __device__ __forceinline__ void note_slot(Cx<R> v, int slot) const {
     if (rmax) rmax[slot] = fmaxf(rmax[slot], fmaxf(fabsf((float)v.x), fabsf((float)v.y)));
   }
 };
@@ -162,12 +169,28 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
         [&](int g, int j, Cx<R> v) { parked[g][j] = v; }, [&](int g, int j) { return parked[g][j]; });
   }
   if (DELTA) return;
-  if (a.what & 1u) {
-    Cx<R> pn[2];
+  // nucleon outputs: with staged 16 x 16 mesons they wait in registers until
+  // the mesons have read the row, then go to its colour-8 slots and out
+  // through the flush with the mesons (128-byte component rows instead of 16
+  // scattered 16-byte segments per warp-wide store)
+  const bool nuc = (a.what & 1u) != 0;
+  Cx<R> pn[2];
+  if (nuc) {
     nucleon_site(row, lt, l, mask, pn);
-    w.put_slot(a.k.nuc + l, pn[0], 0);
-    w.put_slot(a.k.nuc + 16 + l, pn[1], 1);
+    if (w.g16) {
+      w.note_slot(pn[0], 0);
+      w.note_slot(pn[1], 1);
+    } else {
+      w.put_slot(a.k.nuc + l, pn[0], 0);
+      w.put_slot(a.k.nuc + 16 + l, pn[1], 1);
+    }
   }
+  auto stage_nucleon = [&]() {
+    if (nuc) {
+      w.g16[nuc_slot(l)] = pn[0];
+      w.g16[nuc_slot(16 + l)] = pn[1];
+    }
+  };
   const int g1 = lt.meson_g1();  // the sink Gamma of this lane's meson outputs
   if (a.g16_raw) {
     // the colour-traced products M_{al de}[b][z] of lane (al, de): no Gamma
@@ -180,6 +203,7 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
       for (int b = 0; b < 4; b++)
 #pragma unroll
         for (int z = 0; z < 4; z++) w.g16[g16_slot(l, 4 * b + z)] = M[b][z];
+      stage_nucleon();
     } else {
 #pragma unroll
       for (int b = 0; b < 4; b++)
@@ -198,6 +222,7 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
         __syncwarp(mask);  // every lane of the half-warp has finished reading the row
 #pragma unroll
         for (int g2 = 0; g2 < 16; g2++) w.g16[g16_slot(g1, g2)] = c[g2];
+        stage_nucleon();
       } else {  // direct stores (plain form, or split form with the 10 diagonal structures: maxima in shared memory)
 #pragma unroll
         for (int g2 = 0; g2 < 16; g2++) w.put(a.k.g16 + g1 * 16 + g2, c[g2]);
@@ -443,6 +468,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
             const Cx<float> v = sf[s * kRow32 + g16_slot(hw, g2)];
             o[(long long)g2 * a.V3] = v;
             rmax[2 + g2] = fmaxf(rmax[2 + g2], fmaxf(fabsf(v.x), fabsf(v.y)));
+          }
+          // nucleon components 2 g1, 2 g1 + 1 (maxima already taken by their lanes)
+          if (a.what & 1u) {
+            Cx<float>* on = (Cx<float>*)a.out + ((long long)tl * a.K + a.k.nuc + 2 * hw) * a.V3 + x0 + s;
+            on[0] = sf[s * kRow32 + nuc_slot(2 * hw)];
+            on[a.V3] = sf[s * kRow32 + nuc_slot(2 * hw + 1)];
           }
         }
       }
