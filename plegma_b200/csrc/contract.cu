@@ -45,8 +45,11 @@ constexpr int kStage = kSitesPerTile * kRow;
 // CM = false: site-major [site][kRow] (the plain kernel reads it directly);
 // CM = true: component-major [flavour * 144 + component][16 sites], written
 // without bank conflicts and transposed by the split kernel's conversion.
+// Only the staging rows 144 f + component in [lo, hi) are copied (component-
+// major staging; the site-major one always copies all).
 template <typename Tin, bool CM = false>
-__device__ __forceinline__ void issue_tile(const ContractArgs& a, Cx<Tin>* st, int tl, int x0, bool valid) {
+__device__ __forceinline__ void issue_tile(const ContractArgs& a, Cx<Tin>* st, int tl, int x0, bool valid, int lo = 0,
+                                           int hi = 288) {
   if (valid) {
     const int s = threadIdx.x & (kSitesPerTile - 1);
     const int x = x0 + s;
@@ -64,10 +67,12 @@ __device__ __forceinline__ void issue_tile(const ContractArgs& a, Cx<Tin>* st, i
       for (int r = 0; r < 9; r++) {
         const int comp = (threadIdx.x >> 4) + 16 * r;
         Cx<Tin>* dst = CM ? st + (144 * f + comp) * kSitesPerTile + s : st + s * kRow + 144 * f + comp;
-        if (sizeof(Tin) == 8)
-          cp_async16(dst, src, ok ? 16 : 0);
-        else
-          cp_async8(dst, src, ok ? 8 : 0);
+        if (!CM || (144 * f + comp >= lo && 144 * f + comp < hi)) {
+          if (sizeof(Tin) == 8)
+            cp_async16(dst, src, ok ? 16 : 0);
+          else
+            cp_async8(dst, src, ok ? 8 : 0);
+        }
         src += step;
       }
     }
@@ -115,13 +120,17 @@ __device__ __forceinline__ int g16_slot(int g1, int g2) {
 // colour-8 complex of block position c (complex 10 c + 8).
 __device__ __forceinline__ int nuc_slot(int c) { return 10 * c + 8; }
 
-template <typename R>
+// STG: the Delta outputs go to the tile's output staging (a compile-time
+// choice: a run-time branch in the output path costs the Delta code ~3 %).
+template <typename R, bool STG = false>
 struct Writer {
   Cx<R>* out;
   long long V3;
   float* rmax;          // split form: this lane's running maxima of its nucleon outputs (slots 0, 1)
   Cx<float>* smax_base;  // split form: tile whose spare slots hold the per-component maxima, or null
-  Cx<R>* g16;           // split form: this site's FP32 row, reused as its 16 x 16 meson staging; or null
+  Cx<R>* g16;           // split form: this site's FP32 row, reused as its 16 x 16 meson staging (Delta
+                        // instantiation: the tile's output staging); or null
+  int h;                // the site's index in the tile (Delta output staging)
   __device__ __forceinline__ void put(int k, Cx<R> v) const {
     out[(long long)k * V3] = v;
     if (smax_base) {
@@ -135,6 +144,16 @@ struct Writer {
     out[(long long)k * V3] = v;
     note_slot(v, slot);
   }
+  // Delta instantiation: output row r of the tile's staging ([row][16 sites],
+  // the site index XOR-swizzled by the row so that the 16 lanes of a store,
+  // rows r0 + l, hit 16 different bank pairs), or component k straight to HBM
+  // with its maximum
+  __device__ __forceinline__ void dput(int r, int k, Cx<R> v) const {
+    if constexpr (STG)
+      g16[r * 16 + (h ^ (r & 15))] = v;
+    else
+      put(k, v);
+  }
   // the maximum only (the value leaves through the staged flush)
   __device__ __forceinline__ void note_slot(Cx<R> v, int slot) const {
     if (rmax) rmax[slot] = fmaxf(rmax[slot], fmaxf(fabsf((float)v.x), fabsf((float)v.y)));
@@ -146,9 +165,9 @@ struct Writer {
 // the two instantiations over the same tiles (the Delta part is ~5x the rest
 // in arithmetic, so the second pass over the propagators is hidden under its
 // compute).
-template <bool DELTA, typename Row>
+template <bool DELTA, typename Row, typename W>
 __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& row, const LaneTables& lt, int l,
-                                              unsigned mask, const Writer<typename Row::R>& w) {
+                                              unsigned mask, const W& w) {
   typedef typename Row::R R;
   if (DELTA && (a.what & (128u | 256u | 512u))) {
     const int base[3] = {a.k.ntor, a.k.rton, a.k.rtor};
@@ -163,8 +182,9 @@ __device__ __forceinline__ void contract_site(const ContractArgs& a, const Row& 
     delta_site(
         row, lt, l, mask,
         [&](int g, int j, Cx<R> v) {
-          if (j < 2 && (a.what & 2u)) w.put(a.k.diso12 + (g * 2 + j) * 16 + l, v);
-          if (j >= 2 && (a.what & 4u)) w.put(a.k.diso32 + (g * 2 + j - 2) * 16 + l, v);
+          // staging rows: iso-1/2 0..95, iso-3/2 96..191
+          if (j < 2 && (a.what & 2u)) w.dput((g * 2 + j) * 16 + l, a.k.diso12 + (g * 2 + j) * 16 + l, v);
+          if (j >= 2 && (a.what & 4u)) w.dput(96 + (g * 2 + j - 2) * 16 + l, a.k.diso32 + (g * 2 + j - 2) * 16 + l, v);
         },
         [&](int g, int j, Cx<R> v) { parked[g][j] = v; }, [&](int g, int j) { return parked[g][j]; });
   }
@@ -300,7 +320,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
     const int x = cur.x0() + hw;
     if (x < a.V3) {
       const RowF64 row{st + hw * kRow};
-      const Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr, nullptr, nullptr};
+      const Writer<double> w{(Cx<double>*)a.out + (long long)tl * a.K * a.V3 + x, a.V3, nullptr, nullptr, nullptr, 0};
       contract_site<DELTA>(a, row, lt, l, mask, w);
     }
     __syncthreads();
@@ -318,7 +338,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_contract_plain(const ContractAr
 // fit on an SM.
 constexpr int kStage32 = kSitesPerTile * kRow32;
 
-template <typename Tin, bool DELTA>
+template <typename Tin, bool DELTA, bool DSTG = false>
 __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<Tin>* st = (Cx<Tin>*)smem_raw;
@@ -329,6 +349,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
   // block layout of the FP32 rows: conflict-free lane-varying loads for the
   // nucleon and mesons; the Delta keeps the plain order (its registers are fuller)
   constexpr bool kPerm = !DELTA;
+  // Delta instantiation with only the Delta blocks: its 192 outputs per site
+  // (rows 0..95 iso-1/2, 96..191 iso-3/2) are staged in the last 24 KB of the
+  // staging buffer, whose rows of the next tile are copied only after the
+  // tile's output flush has read them; the flush writes 128-byte component
+  // rows and takes the per-component maxima over the tile's sites (direct
+  // stores from the lanes would touch 16 component rows per store, with a
+  // shared-memory atomic per output)
+  // (launched only for requests whose Delta pass holds the Delta blocks alone;
+  // kept a run-time value: as a compile-time one ptxas spills 780 bytes here)
+  const bool dstg = DELTA && DSTG && (a.what & (2u | 4u)) != 0;
+  constexpr int kLate0 = 288 - 192 * kSitesPerTile * (int)sizeof(Cx<float>) / (kSitesPerTile * (int)sizeof(Cx<Tin>));
+  Cx<float>* dstage = (Cx<float>*)(st + kLate0 * kSitesPerTile);
   const int tid = threadIdx.x;
   const int hw = tid >> 4, l = tid & 15;
   const unsigned mask = halfwarp_mask();
@@ -443,17 +475,43 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
       }
     }
     __syncthreads();
-    // the staged tile has been converted: refill the staging buffer while contracting
-    {
-      const TileCursor nx = tc.next();
-      issue_tile<Tin, true>(a, st, nx.tl, nx.x0(), nx.tl < a.ntau);
-    }
+    // the staged tile has been converted: refill the staging buffer while
+    // contracting (with Delta output staging, all but its tail)
+    const TileCursor nx = tc.next();
+    issue_tile<Tin, true>(a, st, nx.tl, nx.x0(), nx.tl < a.ntau, 0, dstg ? kLate0 : 288);
     const int x0 = tc.x0();
     if (x0 + hw < a.V3) {
       const RowF32T<kPerm> row{sf + hw * kRow32};
-      const Writer<float> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x0 + hw, a.V3, DELTA ? nullptr : rmax, sf,
-                            stage ? sf + hw * kRow32 : nullptr};
+      const Writer<float, DELTA && DSTG> w{(Cx<float>*)a.out + (long long)tl * a.K * a.V3 + x0 + hw, a.V3, DELTA ? nullptr : rmax, sf,
+                            stage ? sf + hw * kRow32 : dstg ? dstage : nullptr, hw};
       contract_site<DELTA>(a, row, lt, l, mask, w);
+    }
+    if constexpr (DELTA) {
+      if (dstg) {
+        __syncthreads();  // every site's outputs are staged
+        // half-warp q, lane s: staging rows q + 16 i of site s
+        const int s = tid & 15, q = tid >> 4;
+        const bool okx = x0 + s < a.V3;
+#pragma unroll 1
+        for (int i = 0; i < 12; i++) {
+          const int r = q + 16 * i;
+          if (!(r < 96 ? (a.what & 2u) : (a.what & 4u))) continue;  // uniform over the half-warp
+          const int k = r < 96 ? a.k.diso12 + r : a.k.diso32 + r - 96;
+          const Cx<float> v = dstage[r * 16 + (s ^ q)];
+          float m = 0.f;
+          if (okx) {
+            ((Cx<float>*)a.out)[((long long)tl * a.K + k) * a.V3 + x0 + s] = v;
+            m = fmaxf(fabsf(v.x), fabsf(v.y));
+          }
+          m = fmaxf(m, __shfl_xor_sync(mask, m, 1));
+          m = fmaxf(m, __shfl_xor_sync(mask, m, 2));
+          m = fmaxf(m, __shfl_xor_sync(mask, m, 4));
+          m = fmaxf(m, __shfl_xor_sync(mask, m, 8));
+          if (s == 0) atomicMax(smax_slot(sf, k), __float_as_int(m));
+        }
+        __syncthreads();  // the staging tail is read: the next tile's last rows may land there
+        issue_tile<Tin, true>(a, st, nx.tl, nx.x0(), nx.tl < a.ntau, kLate0, 288);
+      }
     }
     if constexpr (!DELTA) {
       if (stage) {
@@ -558,13 +616,13 @@ cudaError_t launch_plain_t(const ContractArgs& a, int grid, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <typename Tin, bool DELTA>
+template <typename Tin, bool DELTA, bool DSTG = false>
 cudaError_t launch_f32_t(const ContractArgs& a, int grid, cudaStream_t s) {
   const int smem = kSitesPerTile * 288 * (int)sizeof(Cx<Tin>) + kStage32 * (int)sizeof(Cx<float>);
   if (a.K > 2 * 32 * kSitesPerTile) return cudaErrorInvalidValue;  // more components than spare slots
-  cudaError_t e = ensure_smem((const void*)k_contract_f32<Tin, DELTA>, smem);
+  cudaError_t e = ensure_smem((const void*)k_contract_f32<Tin, DELTA, DSTG>, smem);
   if (e != cudaSuccess) return e;
-  k_contract_f32<Tin, DELTA><<<grid, kThreads, smem, s>>>(a);
+  k_contract_f32<Tin, DELTA, DSTG><<<grid, kThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -582,8 +640,14 @@ cudaError_t launch_contract_f32(const ContractArgs& a, int fp32_in, int grid, cu
   cudaError_t e = cudaSuccess;
   if (a.what & ~kDeltaBits)
     e = fp32_in ? launch_f32_t<float, false>(a, grid, s) : launch_f32_t<double, false>(a, grid, s);
-  if (e == cudaSuccess && (a.what & kDeltaBits))
-    e = fp32_in ? launch_f32_t<float, true>(a, grid, s) : launch_f32_t<double, true>(a, grid, s);
+  if (e == cudaSuccess && (a.what & kDeltaBits)) {
+    // the Delta pass with the Delta blocks alone stages its outputs
+    const bool stg = !(a.what & (128u | 256u | 512u));
+    if (stg)
+      e = fp32_in ? launch_f32_t<float, true, true>(a, grid, s) : launch_f32_t<double, true, true>(a, grid, s);
+    else
+      e = fp32_in ? launch_f32_t<float, true>(a, grid, s) : launch_f32_t<double, true>(a, grid, s);
+  }
   return e;
 }
 
