@@ -204,7 +204,7 @@ def run_reference(args, rank, world):
 # DRAM bytes (read + write) per site of the dominant kernel, measured with ncu
 # on the 32^3 x 16 case of the same kernel; traffic grows with the sites a
 # launch processes, so it scales to the benchmark's launches
-TRAFFIC_PER_SITE = {("contract_f32", "split"): 6869, ("contract_plain_fp64", "plain"): 9129}
+TRAFFIC_PER_SITE = {("contract_f32", "split"): 6864, ("contract_plain_fp64", "plain"): 9129}
 # executed FP64 flop per site of the plain site contraction (2 per DFMA, 1 per
 # DADD / DMUL, from the ncu instruction counters of the 32^3 x 16 case)
 FP64_FLOP_PER_SITE = {"contract_plain_fp64": 50336}
@@ -212,7 +212,7 @@ FP64_FLOP_PER_SITE = {"contract_plain_fp64": 50336}
 # l1tex__data_pipe_lsu_wavefronts.sum / sites, 32^3 x 16 case): its binding
 # on-chip limit, one wavefront (128 bytes between shared memory and the
 # registers) per SM and clock
-LSU_WAVEFRONTS_PER_SITE = {"contract_f32": 416.1}
+LSU_WAVEFRONTS_PER_SITE = {"contract_f32": 394.8}
 
 BATCHED = {
     # name: (lattice, sources, window range, |n|^2 max, propagator precision, decay, seed, sources resident at once)

@@ -544,12 +544,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
     for (int k = tid; k < a.K; k += kThreads) atomicMax(a.cmax + (long long)cur * a.K + k, *smax_slot(sf, k));
 }
 
+// Threads of the sampling kernel: the samples are scattered, so its time is
+// the number of rounds of loads in flight per thread (21504 samples, 8 per
+// thread and round).
+constexpr int kSampleThreads = 512;
+
 // Per-slice exponent E with max(|Re|,|Im|) < 2^E over a strided sample of
 // sites and components (every 7th component, every 97th site), so that the
 // scaled entries are O(1) in FP32.  Only the binary exponents are compared,
 // so FP64 entries far below FP32's range are handled exactly.
 __global__ void k_sample_exponents(const SampleArgs a) {
-  __shared__ int red[256];
+  __shared__ int red[kSampleThreads];
   const int tl = blockIdx.x, f = blockIdx.y;
   const SliceDesc& sd = a.sl[tl];
   const void* p = f ? sd.d : sd.u;
@@ -652,7 +657,7 @@ cudaError_t launch_contract_f32(const ContractArgs& a, int fp32_in, int grid, cu
 }
 
 cudaError_t launch_sample_exponents(const SampleArgs& a, cudaStream_t s) {
-  k_sample_exponents<<<dim3(a.ntau, 2), 256, 0, s>>>(a);
+  k_sample_exponents<<<dim3(a.ntau, 2), kSampleThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 
