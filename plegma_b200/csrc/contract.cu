@@ -365,6 +365,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
   const int hw = tid >> 4, l = tid & 15;
   const unsigned mask = halfwarp_mask();
   const LaneTables lt = load_lane_tables(l);
+  // the tile flush's thread -> (site, g1) map: lanes 0-7 / 8-15 / 16-23 / 24-31
+  // of warp w take sites 0-7 / 0-7 / 8-15 / 8-15 of g1 = 2 w / 2 w + 1 / 2 w / 2 w + 1
+  const int flush_s = (tid & 7) + ((tid >> 1) & 8), flush_g1 = 2 * (tid >> 5) + ((tid >> 3) & 1);
 
   const int tiles_per_tau = (a.V3 + kSitesPerTile - 1) / kSitesPerTile;
   TileCursor tc(blockIdx.x, gridDim.x, tiles_per_tau);
@@ -390,17 +393,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
         rmax[i] = 0.f;
         if (!(tid & 16) && (a.what & 1u)) atomicMax(smax_slot(sf, a.k.nuc + 16 * i + l), __float_as_int(m));
       }
-      // mesons: the 16 threads of half-warp hw hold components g16 + 16 hw + g2
+      // mesons: the 16 flush threads of g1 (lanes with the same bit 3 of a
+      // warp) hold components g16 + 16 g1 + g2
 #pragma unroll
       for (int i = 2; i < kSlots; i++) {
         float m = rmax[i];
         m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
         m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
         m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 4));
-        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 8));
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 16));
         rmax[i] = 0.f;
-        const int k = a.k.g16 + 16 * hw + (i - 2);
-        if (l == 0 && stage) atomicMax(smax_slot(sf, k), __float_as_int(m));
+        const int k = a.k.g16 + 16 * flush_g1 + (i - 2);
+        if ((tid & 23) == 0 && stage) atomicMax(smax_slot(sf, k), __float_as_int(m));
       }
     }
   };
@@ -516,22 +520,25 @@ __global__ void __launch_bounds__(kThreads, 2) k_contract_f32(const ContractArgs
     if constexpr (!DELTA) {
       if (stage) {
         __syncthreads();
-        // thread (site s = tid & 15, g1 = tid >> 4): components g16 + 16 g1 + g2,
-        // each a 128-byte row segment over the tile's 16 sites
-        const int s = tid & 15;
+        // thread (site s, g1 = flush_g1): components g16 + 16 g1 + g2, each a
+        // 128-byte row segment over the tile's 16 sites written by the 16
+        // threads of that g1; a half-warp reads 8 sites x the 2 adjacent
+        // outputs of one 16-byte unit per site (rows 161 units apart: 8
+        // different bank groups, one wavefront)
+        const int s = flush_s;
         if (x0 + s < a.V3) {
-          Cx<float>* o = (Cx<float>*)a.out + ((long long)tl * a.K + a.k.g16 + 16 * hw) * a.V3 + x0 + s;
+          Cx<float>* o = (Cx<float>*)a.out + ((long long)tl * a.K + a.k.g16 + 16 * flush_g1) * a.V3 + x0 + s;
 #pragma unroll
           for (int g2 = 0; g2 < 16; g2++) {
-            const Cx<float> v = sf[s * kRow32 + g16_slot(hw, g2)];
+            const Cx<float> v = sf[s * kRow32 + g16_slot(flush_g1, g2)];
             o[(long long)g2 * a.V3] = v;
             rmax[2 + g2] = fmaxf(rmax[2 + g2], fmaxf(fabsf(v.x), fabsf(v.y)));
           }
           // nucleon components 2 g1, 2 g1 + 1 (maxima already taken by their lanes)
           if (a.what & 1u) {
-            Cx<float>* on = (Cx<float>*)a.out + ((long long)tl * a.K + a.k.nuc + 2 * hw) * a.V3 + x0 + s;
-            on[0] = sf[s * kRow32 + nuc_slot(2 * hw)];
-            on[a.V3] = sf[s * kRow32 + nuc_slot(2 * hw + 1)];
+            Cx<float>* on = (Cx<float>*)a.out + ((long long)tl * a.K + a.k.nuc + 2 * flush_g1) * a.V3 + x0 + s;
+            on[0] = sf[s * kRow32 + nuc_slot(2 * flush_g1)];
+            on[a.V3] = sf[s * kRow32 + nuc_slot(2 * flush_g1 + 1)];
           }
         }
       }
