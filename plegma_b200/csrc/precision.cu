@@ -179,19 +179,28 @@ p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int
   // projection GEMM candidates (N-tile width NT <= project_split_max_nt()
   // components, a multiple of 8; number of N-tiles, site splits, k-steps per
   // split): the fewest N-tiles at ~2 waves first, then up to two more N-tiles
-  // at 1, 2 and 4 waves
+  // at 1, 2 and 4 waves, and for each N-tile count the two smallest split
+  // counts whose last wave is at least 95 % full (the CTAs, one per SM, all
+  // take about as long, so a launch lasts whole waves: at 32 slices of 4
+  // N-tiles, 2, 3 or 5 splits fill 86 % of their last wave, 8 splits 99 %)
   std::vector<std::vector<int>> cands;
   const int maxnt = p2::project_split_max_nt();
   for (int ntile = (K + maxnt - 1) / maxnt, extra = 0; extra < 3; ntile++, extra++) {
     const int NT = ((K + ntile - 1) / ntile + 7) / 8 * 8;
     if ((ntile - 1) * NT >= K) continue;  // an empty N-tile
-    for (int waves : {2, 1, 4}) {
-      const int per = ntile * nmtile * n;
-      int nsplit = std::min(std::max(1, (waves * c->nsm + per - 1) / per), nkstep);
+    const int per = ntile * nmtile * n;
+    auto add = [&](int nsplit) {
       const int ks_per = (nkstep + nsplit - 1) / nsplit;
       nsplit = (nkstep + ks_per - 1) / ks_per;
       std::vector<int> v{NT, ntile, nsplit, ks_per};
       if (std::find(cands.begin(), cands.end(), v) == cands.end()) cands.push_back(v);
+      return nsplit;
+    };
+    for (int waves : {2, 1, 4}) add(std::min(std::max(1, (waves * c->nsm + per - 1) / per), nkstep));
+    for (int ns = 1, found = 0; ns <= std::min(nkstep, 64) && found < 2; ns++) {
+      const double w = (double)per * ns / c->nsm;
+      if (w < 1.0 || w > 16.0 || w / std::ceil(w) < 0.95) continue;
+      if (add(ns) == ns) found++;
     }
   }
   size_t maxpart = 0;

@@ -441,6 +441,8 @@ __global__ void k_split_reduce(const SplitReduceArgs a) {
     const int rc = mr[0], rs = mr[1], sg = mr[2];
     const int col = (k / a.NT) * 2 * a.NT + 2 * (k % a.NT);
     double cr = 0, ci = 0, sr = 0, si = 0;
+    // fixed order over the splits; unrolled so that several splits' loads are in flight
+#pragma unroll 4
     for (int sp = 0; sp < a.nsplit; sp++) {
       const float* base = a.part + ((long long)tl * a.nsplit + sp) * a.nmtile * 128 * (long long)a.ncols;
       const float* pc = base + (long long)rc * a.ncols + col;
