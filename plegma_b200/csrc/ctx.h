@@ -100,6 +100,7 @@ struct p2_ctx {
   // split form: phase tiles, per-slice exponents, component maxima, tables, partials, error flag
   p2host::DevBuf phaseA, expb, cmaxb, momrow, kexp, fpart, rowtab, errflag;
   std::vector<int> split_moms_key;  // momentum list the phase tiles and rows were built for
+  int split_nrep = 0;                // representatives (+-h pairs) of that list
   unsigned split_what_key = 0;      // contraction set of the component exponents
   int project_split_smem_max = 0;  // opt-in shared memory per block of the device
   int wait_test = 0;               // p2_debug_wait_timeout armed for the next tensor-core projection

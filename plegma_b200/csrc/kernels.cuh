@@ -140,6 +140,9 @@ struct SplitReduceArgs {
   int ntau, nsplit, nmtile, ncols, NT;
   int nmom, K;
   const int* mom_row;  // [nmom][6]: cos row, sin row (-1 for h = 0), sign (+1: p = h, -1: p = -h), p
+  int nrep;             // representatives h; the momenta of h are rep_moms[rep_start[h] .. rep_start[h + 1])
+  const int* rep_start;
+  const int* rep_moms;
   int L[3];            // global spatial extents (source phase exp(i p.x0))
   const int* cmax;     // [ntau][K]
   const int* exps;     // [ntau][2]

@@ -62,6 +62,7 @@ struct PhaseRows {
   std::vector<int> row_h;    // per row: representative index
   std::vector<int> row_sin;  // per row: 0 cos, 1 sin
   std::vector<int> mom_row;  // per momentum: cos row, sin row, sign
+  std::vector<int> mom_rep;  // per momentum: its representative
 };
 
 PhaseRows phase_rows(const std::vector<int>& moms) {
@@ -97,6 +98,7 @@ PhaseRows phase_rows(const std::vector<int>& moms) {
     pr.mom_row.push_back(cos_row[idx]);
     pr.mom_row.push_back(sin_row[idx]);
     pr.mom_row.push_back(sg);
+    pr.mom_rep.push_back(idx);
   }
   return pr;
 }
@@ -140,12 +142,23 @@ p2_status split_prepare_tables(p2_ctx* c, const Plan& pl, unsigned what, int& nm
       ProfScope ps(c, "build_phase_tiles");
       P2_TRY(c, p2::launch_build_phases(b, c->stream), "phase tiles");
     }
-    // [nmom][6]: cos row, sin row, sign, p
+    // [nmom][6]: cos row, sin row, sign, p; then the momenta of each
+    // representative (+h and -h share its rows): [nrep + 1] starts, [nmom] indices
     std::vector<int> mr;
     for (int p = 0; p < pl.nmom; p++) {
       for (int q = 0; q < 3; q++) mr.push_back(pr.mom_row[3 * p + q]);
       for (int q = 0; q < 3; q++) mr.push_back(pl.moms[3 * p + q]);
     }
+    mr.push_back(0);
+    for (int r = 0; r < nh; r++) {
+      int cnt = 0;
+      for (int p = 0; p < pl.nmom; p++) cnt += pr.mom_rep[p] == r;
+      mr.push_back(mr.back() + cnt);
+    }
+    for (int r = 0; r < nh; r++)
+      for (int p = 0; p < pl.nmom; p++)
+        if (pr.mom_rep[p] == r) mr.push_back(p);
+    c->split_nrep = nh;
     if ((st = upload_async(c, c->momrow, mr.data(), mr.size() * sizeof(int), "momentum rows")) != P2_OK) return st;
     c->split_moms_key = pl.moms;
   }
@@ -258,6 +271,9 @@ p2_status split_project(p2_ctx* c, const Plan& pl, int K, int n, int nmtile, int
   rd.nmom = pl.nmom;
   rd.K = K;
   rd.mom_row = (const int*)c->momrow.p;
+  rd.nrep = c->split_nrep;
+  rd.rep_start = rd.mom_row + 6 * pl.nmom;
+  rd.rep_moms = rd.rep_start + c->split_nrep + 1;
   for (int d = 0; d < 3; d++) rd.L[d] = c->g.L[d];
   rd.cmax = (const int*)c->cmaxb.p;
   rd.exps = exps;

@@ -435,14 +435,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_project_split(const SplitGemmAr
   if (warp == 0) tc::tmem_dealloc(tmem, TCOLS);
 }
 
+// One thread per (slice, representative h, component): the cos and sin rows'
+// partials of h are summed over the site splits once, in a fixed order, and
+// give every momentum of h (+h and -h) its value.
 __global__ void k_split_reduce(const SplitReduceArgs a) {
-  const long long n = (long long)a.ntau * a.nmom * a.K;
+  const long long n = (long long)a.ntau * a.nrep * a.K;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int k = (int)(i % a.K);
-    const int p = (int)((i / a.K) % a.nmom);
-    const int tl = (int)(i / ((long long)a.K * a.nmom));
-    const int* mr = a.mom_row + 6 * p;
-    const int rc = mr[0], rs = mr[1], sg = mr[2];
+    const int h = (int)((i / a.K) % a.nrep);
+    const int tl = (int)(i / ((long long)a.K * a.nrep));
+    const int j0 = a.rep_start[h], j1 = a.rep_start[h + 1];
+    if (j0 == j1) continue;
+    const int* mr0 = a.mom_row + 6 * a.rep_moms[j0];
+    const int rc = mr0[0], rs = mr0[1];
     const int col = (k / a.NT) * 2 * a.NT + 2 * (k % a.NT);
     double cr = 0, ci = 0, sr = 0, si = 0;
     // fixed order over the splits; unrolled so that several splits' loads are in flight
@@ -465,24 +470,29 @@ __global__ void k_split_reduce(const SplitReduceArgs a) {
     const int pw = a.kexp[2 * k] * (a.exps[2 * tl] + sd.eh[0]) + a.kexp[2 * k + 1] * (a.exps[2 * tl + 1] + sd.eh[1]) -
                    (14 - e);
     const double f = ldexp(1.0, pw);
-    // S(p) = sum_x c e^{-i p.x}; the source phase: C(p) = e^{i p.x0} S(p), with
-    // p.x0 / L reduced exactly in integers per dimension
-    Cx<double> v = cmul(cx<double>((cr + sg * si) * f, (ci - sg * sr) * f), source_phase(mr + 3, sd.x0, a.L));
-    if (a.kphase) {
-      const int q = a.kphase[k];
-      if (q & 1) v = cx<double>(-v.y, v.x);
-      if (q & 2) v = cx<double>(-v.x, -v.y);
-    }
-    if (a.nblocks == 0) ((Cx<double>*)a.out)[(long long)sd.tau * a.oT + (long long)k * a.oK + p] = v;
-    for (int b = 0; b < a.nblocks; b++) {
-      const ScatterBlock& B = a.blk[b];
-      const int rel = k - B.k0;
-      if (rel >= 0 && rel < B.groups * B.datasets * B.comps) {
-        const int comp = rel % B.comps;
-        const int gd = rel / B.comps;
-        const long long o = B.base * sd.totalT * a.nmom +
-                            (((long long)gd * sd.totalT + sd.tau) * a.nmom + p) * B.comps + comp;
-        ((Cx<double>*)sd.out)[o] = v;
+    for (int j = j0; j < j1; j++) {
+      const int p = a.rep_moms[j];
+      const int* mr = a.mom_row + 6 * p;
+      const int sg = mr[2];
+      // S(p) = sum_x c e^{-i p.x}; the source phase: C(p) = e^{i p.x0} S(p), with
+      // p.x0 / L reduced exactly in integers per dimension
+      Cx<double> v = cmul(cx<double>((cr + sg * si) * f, (ci - sg * sr) * f), source_phase(mr + 3, sd.x0, a.L));
+      if (a.kphase) {
+        const int q = a.kphase[k];
+        if (q & 1) v = cx<double>(-v.y, v.x);
+        if (q & 2) v = cx<double>(-v.x, -v.y);
+      }
+      if (a.nblocks == 0) ((Cx<double>*)a.out)[(long long)sd.tau * a.oT + (long long)k * a.oK + p] = v;
+      for (int b = 0; b < a.nblocks; b++) {
+        const ScatterBlock& B = a.blk[b];
+        const int rel = k - B.k0;
+        if (rel >= 0 && rel < B.groups * B.datasets * B.comps) {
+          const int comp = rel % B.comps;
+          const int gd = rel / B.comps;
+          const long long o = B.base * sd.totalT * a.nmom +
+                              (((long long)gd * sd.totalT + sd.tau) * a.nmom + p) * B.comps + comp;
+          ((Cx<double>*)sd.out)[o] = v;
+        }
       }
     }
   }
@@ -653,7 +663,7 @@ cudaError_t launch_meson_gamma(const MesonGammaArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_split_reduce(const SplitReduceArgs& a, cudaStream_t s) {
-  const long long n = (long long)a.ntau * a.nmom * a.K;
+  const long long n = (long long)a.ntau * a.nrep * a.K;
   int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
   if (blocks < 1) blocks = 1;
   k_split_reduce<<<blocks, 256, 0, s>>>(a);
